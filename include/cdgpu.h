@@ -1,0 +1,194 @@
+/*
+ * cdgpu.h -- C ABI of libcdgpu, the B200 (sm_100a) implementation of ParMooN's
+ * scalar convection-diffusion hot path: Galerkin/SUPG assembly of Q1/Q2
+ * quadrilaterals and hexahedra into the CSR TSquareMatrix, and the
+ * geometric-multigrid-preconditioned FGMRES / fixed-point solve.
+ *
+ * Plain C types only.  Every call returns a status code (CDGPU_OK = 0); the
+ * reference instead prints a message and calls exit(4711), which a host shim
+ * maps back to (see cdgpu_status_string).  Pointers named h_* are host memory,
+ * d_* device memory of the context's device.  Calls on one context are
+ * serialised on the context's CUDA stream; a context must not be used by two
+ * host threads at once.
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the ParMooN_CMG tree).
+ */
+#ifndef CDGPU_H
+#define CDGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum cdgpu_status
+{
+  CDGPU_OK = 0,
+  CDGPU_ERR_INVALID = 1,       /* bad argument or id */
+  CDGPU_ERR_OOM = 2,           /* device allocation failed */
+  CDGPU_ERR_CUDA = 3,          /* a CUDA call failed (see cdgpu_last_error) */
+  CDGPU_ERR_NOT_CONVERGED = 4, /* maximal iterations reached (reference: "not converged" message) */
+  CDGPU_ERR_DIVERGED = 5,      /* residual > SC_DIV_FACTOR * initial (reference: exit(4711)) */
+  CDGPU_ERR_UNSUPPORTED = 6,   /* input outside the implemented scope (hanging nodes, ...) */
+  CDGPU_ERR_PATTERN = 7,       /* a cell coupling is missing from the given CSR pattern */
+  CDGPU_ERR_NO_DEVICE = 8      /* no CUDA device */
+};
+
+/* discretisation types, include/General/Constants.h:188-190 */
+#define CDGPU_GALERKIN 1
+#define CDGPU_SUPG 2
+
+/* coefficient kinds: how BilinearCoeffs (Examples/CD_2D, CD_3D) is evaluated */
+#define CDGPU_COEFF_CONSTANT 0 /* eps, b, c, f constant in space */
+#define CDGPU_COEFF_SINE 1     /* Examples/CD_2D/SineLaplace.h: f = 2 pi^2 eps sin(pi x) sin(pi y) */
+#define CDGPU_COEFF_ROTATING 2 /* b = (0.5 - y, x - 0.5), eps, c, f constant (TCD2D config) */
+#define CDGPU_COEFF_TABLE 3    /* host-evaluated record per cell and quadrature point */
+
+typedef struct cdgpu_coeffs
+{
+  int kind;        /* CDGPU_COEFF_* */
+  int poly_degree; /* INTERNAL_POLYNOMIAL_DEGREE used by the SUPG parameter (reference default 1) */
+  double eps;      /* diffusion, coeff[0] */
+  double b1, b2, b3; /* convection, coeff[1..2] (2D) / [1..3] (3D) */
+  double c;        /* reaction */
+  double f;        /* source */
+  double delta0;   /* DELTA0 (src/General/Database.C:456, default 1) */
+} cdgpu_coeffs;
+
+/* multigrid / Krylov parameters, named after the reference's ParamDB keys
+ * (defaults src/General/Database.C:639-760) */
+typedef struct cdgpu_solver_params
+{
+  int solver;          /* SC_SOLVER_SCALAR: 16 FGMRES (flexible), 11 fixed point */
+  int restart;         /* SC_GMRES_RESTART */
+  int maxit;           /* SC_LIN_MAXIT_SCALAR */
+  int minit;           /* SC_MINIT */
+  int smoother;        /* SC_SMOOTHER_SCALAR: 1 damped Jacobi (only value implemented on the GPU) */
+  int coarse_smoother; /* SC_COARSE_SMOOTHER_SCALAR: 1 Jacobi, 3 SSOR, 17 exact (dense FP64) */
+  int pre, post;       /* SC_PRE_SMOOTH_SCALAR, SC_POST_SMOOTH_SCALAR */
+  int coarse_maxit;    /* SC_COARSE_MAXIT_SCALAR */
+  int cycle;           /* SC_MG_CYCLE_SCALAR: 1 V, 2 W, 0 F */
+  int slc;             /* SC_STEP_LENGTH_CONTROL_ALL_SCALAR (must be 0 on the GPU) */
+  int precision;       /* 0: FP64 multigrid (drop-in); 1: FP32 multigrid inside FP64 FGMRES */
+  double red_factor;   /* SC_LIN_RED_FACTOR_SCALAR */
+  double res_norm_min; /* SC_LIN_RES_NORM_MIN_SCALAR */
+  double div_factor;   /* SC_DIV_FACTOR */
+  double omega;        /* SC_SMOOTH_DAMP_FACTOR_SCALAR */
+  double coarse_red;   /* SC_COARSE_RED_FACTOR_SCALAR */
+  double gmg_damp;     /* SC_GMG_DAMP_FACTOR_SCALAR */
+} cdgpu_solver_params;
+
+typedef struct cdgpu_solve_info
+{
+  int iterations;        /* the value TFgmresIte::Iterate / TFixedPointIte::Iterate returns */
+  int status;            /* CDGPU_OK, CDGPU_ERR_NOT_CONVERGED or CDGPU_ERR_DIVERGED */
+  double initial_residual;
+  double final_residual; /* |s_{i+1}| (FGMRES) or ||f - A x|| (fixed point) at exit */
+} cdgpu_solve_info;
+
+typedef struct cdgpu_ctx cdgpu_ctx;
+
+/* --- context ------------------------------------------------------------- */
+/* No reference counterpart (the reference is a process-wide CPU library).   */
+int cdgpu_create(cdgpu_ctx **ctx, int device);
+void cdgpu_destroy(cdgpu_ctx *ctx);
+const char *cdgpu_status_string(int status);
+const char *cdgpu_last_error(const cdgpu_ctx *ctx);
+/* the cudaStream_t all work of this context is issued on, as an integer handle */
+unsigned long long cdgpu_stream(const cdgpu_ctx *ctx);
+/* number of kernels this context has launched so far */
+long long cdgpu_kernel_launches(const cdgpu_ctx *ctx);
+
+/* --- finite element space -------------------------------------------------
+ * Replaces the data TFESpace2D/TFESpace3D hands to the assembler
+ * (include/FE/FESpace.h:135-197: GetGlobalNumbers, GetBeginIndex,
+ * GetActiveBound, GetHangingBound, GetN_Dirichlet) plus the cell vertices
+ * (TBaseCell::GetVertex, include/Geometry/BaseCell.h:165).
+ * h_vert: n_cells x (4|8) x dim doubles, cell vertices in the reference's
+ * counter-clockwise order; h_global_numbers / h_begin_index as in TFESpace;
+ * DOFs ordered [active | Dirichlet].  Hanging nodes are not supported
+ * (hanging_bound must equal n_active). */
+int cdgpu_upload_space(cdgpu_ctx *ctx, int dim, int order, int n_cells, const double *h_vert,
+                       const int *h_global_numbers, const int *h_begin_index, int n_dof,
+                       int n_active, int hanging_bound, int *space_id);
+
+/* --- matrix structure ------------------------------------------------------
+ * Replaces TSquareStructure2D/3D(TFESpace*) + TSquareStructure::Sort()
+ * (src/FE/SquareStructure3D.C:32, SquareStructure2D.C:46, SquareStructure.C:65):
+ * builds the CSR pattern from the space's DOF map (bit-identical to the
+ * reference's), or takes the host's own RowPtr/KCol.  *nnz receives the count. */
+int cdgpu_build_pattern(cdgpu_ctx *ctx, int space_id, int *nnz);
+int cdgpu_upload_pattern(cdgpu_ctx *ctx, int space_id, const int *h_row_ptr, const int *h_kcol,
+                         int nnz);
+int cdgpu_get_pattern(cdgpu_ctx *ctx, int space_id, int *h_row_ptr, int *h_kcol);
+
+/* --- coefficients ----------------------------------------------------------
+ * Replaces the CoeffFct2D/CoeffFct3D callback (include/General/Constants.h:120-125)
+ * bound by TDiscreteForm2D/3D.  h_table (kind CDGPU_COEFF_TABLE only):
+ * n_cells x n_quad x 6 doubles (eps, b1, b2, b3, c, f) at the assembly's
+ * quadrature points, see cdgpu_quadrature_points. */
+int cdgpu_set_coeffs(cdgpu_ctx *ctx, int space_id, const cdgpu_coeffs *coeffs,
+                     const double *h_table);
+/* quadrature points (physical coordinates, n_cells x n_quad x dim) at which a
+ * CDGPU_COEFF_TABLE must be evaluated; *n_quad receives the points per cell. */
+int cdgpu_quadrature_points(cdgpu_ctx *ctx, int space_id, double *h_xyz, int *n_quad);
+
+/* --- assembly ---------------------------------------------------------------
+ * Replaces TSystemCD3D::Assemble / TAssembleMat3D::Reset + Assemble3D
+ * (src/System/SystemCD3D.C:314-339, src/System/AssembleMat3D.C:230-505) and
+ * TSystemCD2D::Assemble / Assemble2D (src/System/SystemCD2D.C:125-179,
+ * src/FE/Assemble2D.C:33-1206): local Galerkin (ConvDiff2D.C:32, ConvDiff3D.C:61)
+ * or SUPG (ConvDiff2D.C:96, ConvDiff3D.C:124) forms, scattered into the CSR
+ * entries; Dirichlet rows become identity rows whose right-hand side is the
+ * boundary value.  The matrix and right-hand side stay on the device;
+ * h_entries / h_rhs (nullable) receive copies like TSquareMatrix::GetEntries().
+ * h_dirichlet: values of DOFs [n_active, n_dof) (BoundValue at the nodes), NULL = 0. */
+int cdgpu_assemble(cdgpu_ctx *ctx, int space_id, int disctype, const double *h_dirichlet,
+                   double *h_entries, double *h_rhs);
+/* Neumann boundary data: adds sum_q hE w_q g_q phi_k(x_q) to active rows, like the
+ * NEUMANN branch of Assemble2D (src/FE/Assemble2D.C:797-827).  Per edge: its cell,
+ * local edge m (vertices m, m+1), and g at the (order+1) Gauss points of the edge in
+ * ascending order from vertex m.  h_rhs (nullable) receives the updated right-hand side. */
+int cdgpu_add_neumann(cdgpu_ctx *ctx, int space_id, int n_edges, const int *h_cell,
+                      const int *h_local_edge, const double *h_g, double *h_rhs);
+
+/* --- matrix-vector products -------------------------------------------------
+ * Replace MatVect / MatVect_Scalar and ScalarDefect / Defect_Scalar
+ * (src/FE/Blas2.C:11-99) on the assembled matrix of a space. */
+int cdgpu_spmv(cdgpu_ctx *ctx, int space_id, const double *h_x, double *h_y);
+int cdgpu_defect(cdgpu_ctx *ctx, int space_id, const double *h_x, const double *h_f, double *h_d,
+                 double *res);
+int cdgpu_spmv_device(cdgpu_ctx *ctx, int space_id, const double *d_x, double *d_y);
+
+/* --- multigrid hierarchy ------------------------------------------------------
+ * Replaces TMultiGrid3D/TMultiGrid2D + AddLevel(TMGLevel) (src/System/SystemCD3D.C:
+ * 147-151, 295-308) and the cell-wise transfer operators Prolongate /
+ * DefectRestriction (src/FE/MGComponents3D.C:182-988, MGComponents2D.C:118-1022),
+ * which are built here once as sparse matrices.  space_ids: coarsest first;
+ * h_parent[l] (l >= 1): for each cell of level l, its parent cell on level l-1
+ * (TBaseCell::GetParent); h_parent[0] is ignored. */
+int cdgpu_hierarchy(cdgpu_ctx *ctx, int n_levels, const int *space_ids, const int *const *h_parent,
+                    int *mg_id);
+
+/* --- solve -----------------------------------------------------------------
+ * Replaces TSystemCD3D::Solve (GMG branch, src/System/SystemCD3D.C:342-368):
+ * TFgmresIte (src/FE/FgmresIte.C:219-582) or TFixedPointIte (FixedPointIte.C:150)
+ * preconditioned by one TMultiGridScaIte cycle (MultiGridScaIte.C:63-104) of
+ * TMultiGrid3D::Cycle (src/FE/MultiGrid3D.C:423-669).  Uses the finest level's
+ * assembled matrix.  h_sol: initial guess in, solution out. */
+int cdgpu_solve(cdgpu_ctx *ctx, int mg_id, const cdgpu_solver_params *params, const double *h_rhs,
+                double *h_sol, cdgpu_solve_info *info);
+/* same with device vectors (length n_dof of the finest level) */
+int cdgpu_solve_device(cdgpu_ctx *ctx, int mg_id, const cdgpu_solver_params *params,
+                       const double *d_rhs, double *d_sol, cdgpu_solve_info *info);
+/* assemble every level of a hierarchy (TSystemCD3D::Assemble loops over all levels) and
+ * copy the finest right-hand side's Dirichlet part into d_sol like SystemCD3D.C:330 */
+int cdgpu_assemble_hierarchy(cdgpu_ctx *ctx, int mg_id, int disctype);
+/* device pointer of the assembled right-hand side of a space */
+int cdgpu_rhs_device(cdgpu_ctx *ctx, int space_id, double **d_rhs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CDGPU_H */

@@ -1,0 +1,667 @@
+// Assembly kernels of libcdgpu (sm_100a).
+//
+// The reference assembles cell by cell and adds every local entry into the CSR
+// row with a linear search (TMatrix::add -> TStructure::index_of_entry,
+// src/FE/Matrix.C:111, src/FE/Structure.C:98; src/System/AssembleMat3D.C:765-787).
+// Here the matrix is assembled row by row instead: a group of threads owns one
+// CSR row, walks the cells containing the row's DOF in ascending cell order (the
+// same order in which the reference's cell loop adds into that row), finds each
+// column's slot by binary search in the row's own column list held in shared
+// memory, and accumulates in shared memory.  Every entry is written exactly once
+// with coalesced stores, there are no atomics and no colouring, and the sum order
+// per entry is the reference's.  Local values come from one of two producers:
+//   * affine fast path: for parallelogram / parallelepiped cells with constant
+//     coefficients the local matrix is sum_t coef[cell][t] * R_t over reference
+//     tensors R_t (see reference_tensors in setup.cpp); coef is computed per cell
+//     (cell_coef_kernel) and the row kernel evaluates local entries on the fly;
+//   * quadrature path: local matrices by Gauss quadrature with the reference's
+//     per-point formulas (local_quad_kernel), stored and then gathered.
+#include <cooperative_groups.h>
+
+#include <cmath>
+
+#include "internal.h"
+
+namespace cg = cooperative_groups;
+
+struct Coef
+{
+  int kind, poly_degree;
+  double eps, b1, b2, b3, c, f, delta0;
+};
+
+static Coef to_coef(const cdgpu_coeffs &c)
+{
+  return Coef{c.kind, c.poly_degree > 0 ? c.poly_degree : 1, c.eps, c.b1, c.b2, c.b3,
+              c.c, c.f, c.delta0};
+}
+
+// SDFEM_TYPE 2 parameter (src/FE/ConvDiff.C:490-582, cases 1/2) with CELL_MEASURE 0
+__device__ __forceinline__ double sdfem_delta(double hK, double eps, double b1, double b2,
+                                              double b3, double delta0, int polydeg)
+{
+  if (fabs(eps) < 1e-20) eps = 1e-20;
+  double nb = sqrt(b1 * b1 + b2 * b2 + b3 * b3);
+  double nu = 1.0 / polydeg, delta = 0.0;
+  if (nb > 0)
+  {
+    double alpha = nu * nb * hK / (2 * eps);
+    delta = nu * hK * (1 / tanh(alpha) - 1 / alpha) / (2 * nb);
+  }
+  return delta * delta0;
+}
+
+__device__ __forceinline__ void coef_at(const Coef &co, const double *tab, const double *x,
+                                        double *k)
+{
+  k[0] = co.eps; k[1] = co.b1; k[2] = co.b2; k[3] = co.b3; k[4] = co.c; k[5] = co.f;
+  if (co.kind == CDGPU_COEFF_SINE)
+  {
+    k[1] = k[2] = k[3] = k[4] = 0.0;
+    k[5] = 2 * M_PI * M_PI * co.eps * sin(M_PI * x[0]) * sin(M_PI * x[1]);
+  }
+  else if (co.kind == CDGPU_COEFF_ROTATING)
+  {
+    k[1] = -x[1] + 0.5;
+    k[2] = x[0] - 0.5;
+  }
+  else if (co.kind == CDGPU_COEFF_TABLE && tab)
+  {
+    for (int i = 0; i < 6; i++) k[i] = tab[i];
+  }
+}
+
+__device__ __forceinline__ double d_invert(int dim, const double *J, double *Ji)
+{
+  if (dim == 2)
+  {
+    double det = J[0] * J[3] - J[1] * J[2];
+    Ji[0] = J[3] / det; Ji[1] = -J[1] / det; Ji[2] = -J[2] / det; Ji[3] = J[0] / det;
+    return det;
+  }
+  double c00 = J[4] * J[8] - J[5] * J[7], c01 = J[5] * J[6] - J[3] * J[8], c02 = J[3] * J[7] - J[4] * J[6];
+  double det = J[0] * c00 + J[1] * c01 + J[2] * c02;
+  Ji[0] = c00 / det; Ji[1] = (J[2] * J[7] - J[1] * J[8]) / det; Ji[2] = (J[1] * J[5] - J[2] * J[4]) / det;
+  Ji[3] = c01 / det; Ji[4] = (J[0] * J[8] - J[2] * J[6]) / det; Ji[5] = (J[2] * J[3] - J[0] * J[5]) / det;
+  Ji[6] = c02 / det; Ji[7] = (J[1] * J[6] - J[0] * J[7]) / det; Ji[8] = (J[0] * J[4] - J[1] * J[3]) / det;
+  return det;
+}
+
+__device__ __forceinline__ double d_diameter(int dim, const double *V)
+{
+  double best = 0;
+  if (dim == 2)
+  {
+    for (int e = 0; e < 2; e++)
+    {
+      int a = e, b = e + 2;
+      double dx = V[2 * a] - V[2 * b], dy = V[2 * a + 1] - V[2 * b + 1];
+      best = fmax(best, dx * dx + dy * dy);
+    }
+  }
+  else
+  {
+    const int p0[4] = {0, 1, 2, 3}, p1[4] = {6, 7, 4, 5};
+    for (int e = 0; e < 4; e++)
+    {
+      double s = 0;
+      for (int a = 0; a < 3; a++)
+      {
+        double d = V[3 * p0[e] + a] - V[3 * p1[e] + a];
+        s += d * d;
+      }
+      best = fmax(best, s);
+    }
+  }
+  return sqrt(best);
+}
+
+// ---------------------------------------------------------------------------
+// affine fast path: per-cell coefficients of the reference tensors
+// ---------------------------------------------------------------------------
+struct CellCoefArgs
+{
+  int dim, nv, n_cells, disctype, T, Tr;
+  Coef co;
+  const double *coords;
+  double *out; // n_cells x (T + Tr)
+};
+
+__global__ void cell_coef_kernel(CellCoefArgs a)
+{
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.n_cells) return;
+  const int dim = a.dim;
+  double V[24];
+  for (int k = 0; k < a.nv * dim; k++) V[k] = a.coords[(size_t)c * a.nv * dim + k];
+  double J[9], Ji[9];
+  for (int r = 0; r < dim; r++)
+  {
+    J[r * dim + 0] = (V[1 * dim + r] - V[r]) * 0.5;
+    J[r * dim + 1] = (V[3 * dim + r] - V[r]) * 0.5;
+    if (dim == 3) J[r * dim + 2] = (V[4 * dim + r] - V[r]) * 0.5;
+  }
+  double w = fabs(d_invert(dim, J, Ji));
+  double b[3] = {a.co.b1, a.co.b2, dim == 3 ? a.co.b3 : 0.0};
+  double G[9], beta[3];
+  for (int p = 0; p < dim; p++)
+  {
+    double s = 0;
+    for (int q = 0; q < dim; q++) s += Ji[p * dim + q] * b[q];
+    beta[p] = s;
+    for (int r = 0; r < dim; r++)
+    {
+      double g = 0;
+      for (int q = 0; q < dim; q++) g += Ji[p * dim + q] * Ji[r * dim + q];
+      G[p * dim + r] = g;
+    }
+  }
+  double eps = a.co.eps, cr = a.co.c, f = a.co.f;
+  bool supg = a.disctype == CDGPU_SUPG;
+  double delta = supg ? sdfem_delta(d_diameter(dim, V), eps, b[0], b[1], b[2], a.co.delta0,
+                                    a.co.poly_degree)
+                      : 0.0;
+  double K[9];
+  for (int p = 0; p < dim * dim; p++) K[p] = eps * G[p];
+  if (supg)
+    for (int p = 0; p < dim; p++)
+      for (int r = 0; r < dim; r++) K[p * dim + r] += delta * beta[p] * beta[r];
+  double *o = a.out + (size_t)c * (a.T + a.Tr);
+  if (dim == 2)
+  {
+    o[0] = w * K[0]; o[1] = w * K[3]; o[2] = w * K[1];
+    o[3] = w * beta[0]; o[4] = w * beta[1]; o[5] = w * cr;
+    if (supg)
+    {
+      o[6] = w * delta * cr * beta[0];
+      o[7] = w * delta * cr * beta[1];
+      double s = -w * delta * eps;
+      o[8] = s * G[0] * beta[0]; o[9] = s * G[0] * beta[1];
+      o[10] = s * G[3] * beta[0]; o[11] = s * G[3] * beta[1];
+      o[12] = s * G[1] * beta[0]; o[13] = s * G[1] * beta[1];
+    }
+  }
+  else
+  {
+    o[0] = w * K[0]; o[1] = w * K[4]; o[2] = w * K[8];
+    o[3] = w * K[1]; o[4] = w * K[2]; o[5] = w * K[5];
+    o[6] = w * beta[0]; o[7] = w * beta[1]; o[8] = w * beta[2]; o[9] = w * cr;
+    if (supg)
+      for (int p = 0; p < 3; p++) o[10 + p] = w * delta * cr * beta[p];
+  }
+  double *orr = o + a.T;
+  orr[0] = w * f;
+  if (supg)
+    for (int p = 0; p < dim; p++) orr[1 + p] = w * f * delta * beta[p];
+}
+
+// ---------------------------------------------------------------------------
+// quadrature path: one CTA per cell, the reference's per-point local forms
+// (src/FE/ConvDiff2D.C:32-162, src/FE/ConvDiff3D.C:61-190) summed over the Gauss points
+// in the reference's order.  Writes nbf*nbf matrix entries then nbf rhs entries.
+// ---------------------------------------------------------------------------
+struct LocalArgs
+{
+  int dim, nv, nbf, nq, n_cells, disctype, affine_all;
+  Coef co;
+  const double *coords, *tab; // tab: n_cells x nq x 6 (kind TABLE)
+  const double *qx, *qw, *phi, *dphi, *hphi;
+  double *out;
+};
+
+__global__ void local_quad_kernel(LocalArgs a)
+{
+  extern __shared__ double sm[];
+  const int dim = a.dim, nbf = a.nbf, nq = a.nq;
+  double *g = sm;                      // nq x nbf x dim physical gradients
+  double *lap = g + nq * nbf * dim;    // nq x nbf physical Laplacians (2D SUPG)
+  double *mult = lap + nq * nbf;       // nq
+  double *kq = mult + nq;              // nq x 6 coefficients
+  double *dl = kq + nq * 6;            // nq SUPG parameters
+  double *Jis = dl + nq;               // nq x dim*dim
+  __shared__ double V[24];
+  int c = blockIdx.x;
+  for (int k = threadIdx.x; k < a.nv * dim; k += blockDim.x) V[k] = a.coords[(size_t)c * a.nv * dim + k];
+  __syncthreads();
+  for (int q = threadIdx.x; q < nq; q += blockDim.x)
+  {
+    const double *xi = a.qx + q * dim;
+    double x[3] = {0, 0, 0}, J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Ji[9];
+    bool affine = a.affine_all;
+    if (affine)
+    {
+      for (int r = 0; r < dim; r++)
+      {
+        double c1 = (V[1 * dim + r] - V[r]) * 0.5, c2 = (V[3 * dim + r] - V[r]) * 0.5;
+        if (dim == 2)
+        {
+          x[r] = (V[1 * dim + r] + V[3 * dim + r]) * 0.5 + c1 * xi[0] + c2 * xi[1];
+          J[r * 2] = c1; J[r * 2 + 1] = c2;
+        }
+        else
+        {
+          double c3 = (V[4 * dim + r] - V[r]) * 0.5;
+          x[r] = (V[1 * dim + r] + V[3 * dim + r] + V[4 * dim + r] - V[r]) * 0.5 + c1 * xi[0] +
+                 c2 * xi[1] + c3 * xi[2];
+          J[r * 3] = c1; J[r * 3 + 1] = c2; J[r * 3 + 2] = c3;
+        }
+      }
+    }
+    else
+    {
+      const double r2[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
+      for (int v = 0; v < a.nv; v++)
+      {
+        double rv[3];
+        if (dim == 2) { rv[0] = r2[v][0]; rv[1] = r2[v][1]; }
+        else { rv[0] = r2[v & 3][0]; rv[1] = r2[v & 3][1]; rv[2] = v < 4 ? -1.0 : 1.0; }
+        double f[3], N = 1;
+        for (int b = 0; b < dim; b++) { f[b] = 0.5 * (1 + rv[b] * xi[b]); N *= f[b]; }
+        for (int b = 0; b < dim; b++)
+        {
+          double dN = 0.5 * rv[b];
+          for (int e = 0; e < dim; e++)
+            if (e != b) dN *= f[e];
+          for (int r = 0; r < dim; r++) J[r * dim + b] += dN * V[v * dim + r];
+        }
+        for (int r = 0; r < dim; r++) x[r] += N * V[v * dim + r];
+      }
+    }
+    double det = d_invert(dim, J, Ji);
+    mult[q] = a.qw[q] * fabs(det);
+    for (int k = 0; k < dim * dim; k++) Jis[q * dim * dim + k] = Ji[k];
+    double k6[6];
+    coef_at(a.co, a.tab ? a.tab + ((size_t)c * nq + q) * 6 : nullptr, x, k6);
+    for (int k = 0; k < 6; k++) kq[q * 6 + k] = k6[k];
+    dl[q] = a.disctype == CDGPU_SUPG
+                ? sdfem_delta(d_diameter(dim, V), k6[0], k6[1], k6[2], dim == 3 ? k6[3] : 0.0,
+                              a.co.delta0, a.co.poly_degree)
+                : 0.0;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nq * nbf; t += blockDim.x)
+  {
+    int q = t / nbf, b = t % nbf;
+    const double *Ji = Jis + q * dim * dim;
+    const double *dp = a.dphi + (size_t)(q * nbf + b) * dim;
+    for (int r = 0; r < dim; r++)
+    {
+      double s = 0;
+      for (int e = 0; e < dim; e++) s += Ji[e * dim + r] * dp[e];
+      g[(q * nbf + b) * dim + r] = s;
+    }
+    double l = 0;
+    if (dim == 2 && a.disctype == CDGPU_SUPG)
+    {
+      const double *hp = a.hphi + (size_t)(q * nbf + b) * 4;
+      for (int r = 0; r < 2; r++)
+        for (int e = 0; e < 2; e++)
+          for (int f = 0; f < 2; f++) l += Ji[e * 2 + r] * Ji[f * 2 + r] * hp[e * 2 + f];
+    }
+    lap[q * nbf + b] = l;
+  }
+  __syncthreads();
+  double *out = a.out + (size_t)c * (nbf * nbf + nbf);
+  for (int t = threadIdx.x; t < nbf * nbf + nbf; t += blockDim.x)
+  {
+    bool is_rhs = t >= nbf * nbf;
+    int i = is_rhs ? t - nbf * nbf : t / nbf, j = is_rhs ? 0 : t % nbf;
+    double acc = 0;
+    for (int q = 0; q < nq; q++)
+    {
+      const double *k6 = kq + q * 6;
+      double c0 = k6[0], c1 = k6[1], c2 = k6[2], c3 = dim == 3 ? k6[3] : 0.0, cr = k6[4], f = k6[5];
+      const double *gi = g + (q * nbf + i) * dim;
+      double phi_i = a.phi[q * nbf + i];
+      double bgradv = c1 * gi[0] + c2 * gi[1] + (dim == 3 ? c3 * gi[2] : 0.0);
+      double delta = dl[q];
+      if (is_rhs)
+      {
+        acc += a.disctype == CDGPU_SUPG ? mult[q] * (phi_i + delta * bgradv) * f : mult[q] * phi_i * f;
+        continue;
+      }
+      const double *gj = g + (q * nbf + j) * dim;
+      double phi_j = a.phi[q * nbf + j];
+      double val = c0 * (gi[0] * gj[0] + gi[1] * gj[1] + (dim == 3 ? gi[2] * gj[2] : 0.0));
+      double bg = c1 * gj[0] + c2 * gj[1] + (dim == 3 ? c3 * gj[2] : 0.0);
+      val += bg * phi_i;
+      val += cr * phi_j * phi_i;
+      if (a.disctype == CDGPU_SUPG)
+      {
+        if (dim == 2)
+          val += delta * (-c0 * lap[q * nbf + j] + bg + cr * phi_j) * bgradv;
+        else
+          val += delta * (bg + cr * phi_j) * bgradv;
+      }
+      val *= mult[q];
+      acc += val;
+    }
+    out[t] = acc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// row gather: one group of GS threads per CSR row
+// ---------------------------------------------------------------------------
+struct GatherArgs
+{
+  int n_dof, n_active, nbf, T, Tr, mode; // mode 0 affine tensors, 1 stored local matrices
+  const int *row_ptr, *kcol, *inc_ptr, *inc, *gn;
+  const double *cellcoef, *local, *R, *r, *dir;
+  double *a, *rhs, *diag;
+  float *a32, *diag32;
+  int *err;
+};
+
+template <int GS, int MAXROW>
+__global__ void __launch_bounds__(256) row_gather_kernel(GatherArgs p)
+{
+  extern __shared__ double smem[];
+  const int nbf = p.nbf, T = p.T, Tr = p.Tr;
+  double *Rs = smem;                                       // nbf*nbf*T (mode 0)
+  double *rs = Rs + (p.mode == 0 ? nbf * nbf * T : 0);     // nbf*Tr (mode 0)
+  double *accs = rs + (p.mode == 0 ? nbf * Tr : 0);        // groups x MAXROW
+  int *cols = (int *)(accs + (blockDim.x / GS) * MAXROW);  // groups x MAXROW
+  if (p.mode == 0)
+  {
+    for (int t = threadIdx.x; t < nbf * nbf * T; t += blockDim.x) Rs[t] = p.R[t];
+    for (int t = threadIdx.x; t < nbf * Tr; t += blockDim.x) rs[t] = p.r[t];
+  }
+  __syncthreads();
+  auto tile = cg::tiled_partition<GS>(cg::this_thread_block());
+  const int lane = tile.thread_rank(), grp = threadIdx.x / GS;
+  double *acc = accs + grp * MAXROW;
+  int *cl = cols + grp * MAXROW;
+  const int ngroups = gridDim.x * (blockDim.x / GS);
+  for (int r = blockIdx.x * (blockDim.x / GS) + grp; r < p.n_dof; r += ngroups)
+  {
+    const int base = p.row_ptr[r], len = p.row_ptr[r + 1] - base;
+    if (r >= p.n_active)
+    {
+      // Dirichlet row: identity row (Assemble2D.C:512, AssembleMat3D.C:811-816)
+      for (int s = lane; s < len; s += GS)
+      {
+        bool d = p.kcol[base + s] == r;
+        p.a[base + s] = d ? 1.0 : 0.0;
+        if (p.a32) p.a32[base + s] = d ? 1.0f : 0.0f;
+      }
+      if (lane == 0)
+      {
+        p.rhs[r] = p.dir ? p.dir[r - p.n_active] : 0.0;
+        p.diag[r] = 1.0;
+        if (p.diag32) p.diag32[r] = 1.0f;
+      }
+      continue;
+    }
+    if (len > MAXROW)
+    {
+      if (lane == 0) atomicExch(p.err, 2);
+      continue;
+    }
+    for (int s = lane; s < len; s += GS) { cl[s] = p.kcol[base + s]; acc[s] = 0.0; }
+    tile.sync();
+    double racc = 0.0;
+    for (int t = p.inc_ptr[r]; t < p.inc_ptr[r + 1]; t++)
+    {
+      const int e = p.inc[t], K = e / nbf, i = e - K * nbf;
+      double cf[CD_MAXT];
+      if (p.mode == 0)
+      {
+#pragma unroll
+        for (int u = 0; u < CD_MAXT; u++) cf[u] = u < T ? __ldg(p.cellcoef + (size_t)K * (T + Tr) + u) : 0.0;
+      }
+      for (int j = lane; j < nbf; j += GS)
+      {
+        const int col = __ldg(p.gn + (size_t)K * nbf + j);
+        int lo = 0, hi = len - 1, slot = -1;
+        while (lo <= hi)
+        {
+          int mid = (lo + hi) >> 1, v = cl[mid];
+          if (v == col) { slot = mid; break; }
+          if (v < col) lo = mid + 1; else hi = mid - 1;
+        }
+        if (slot < 0) { atomicExch(p.err, 1); continue; }
+        double v;
+        if (p.mode == 0)
+        {
+          const double *Rij = Rs + (i * nbf + j) * T;
+          v = 0.0;
+#pragma unroll
+          for (int u = 0; u < CD_MAXT; u++)
+            if (u < T) v += cf[u] * Rij[u];
+        }
+        else
+          v = __ldg(p.local + (size_t)K * (nbf * nbf + nbf) + i * nbf + j);
+        acc[slot] += v;
+      }
+      if (lane == 0)
+      {
+        double F;
+        if (p.mode == 0)
+        {
+          F = 0.0;
+          const double *rc = p.cellcoef + (size_t)K * (T + Tr) + T;
+          for (int u = 0; u < Tr; u++) F += __ldg(rc + u) * rs[i * Tr + u];
+        }
+        else
+          F = __ldg(p.local + (size_t)K * (nbf * nbf + nbf) + nbf * nbf + i);
+        racc += F;
+      }
+      tile.sync();
+    }
+    for (int s = lane; s < len; s += GS)
+    {
+      double v = acc[s];
+      p.a[base + s] = v;
+      if (p.a32) p.a32[base + s] = (float)v;
+      if (cl[s] == r)
+      {
+        p.diag[r] = v;
+        if (p.diag32) p.diag32[r] = (float)v;
+      }
+    }
+    if (lane == 0) p.rhs[r] = racc;
+    tile.sync();
+  }
+}
+
+template <int GS, int MAXROW>
+static int launch_gather(cdgpu_ctx *ctx, const GatherArgs &g, int n_dof)
+{
+  int groups = 256 / GS;
+  size_t sm = (size_t)(g.mode == 0 ? g.nbf * g.nbf * g.T + g.nbf * g.Tr : 0) * sizeof(double) +
+              (size_t)groups * MAXROW * (sizeof(double) + sizeof(int));
+  CD_CUDA(ctx, cudaFuncSetAttribute(row_gather_kernel<GS, MAXROW>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  int blocks_per_sm = 0;
+  CD_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm,
+                                                             row_gather_kernel<GS, MAXROW>, 256, sm));
+  if (blocks_per_sm < 1) blocks_per_sm = 1;
+  long need = (n_dof + groups - 1) / groups;
+  long grid = std::min<long>(need, (long)ctx->sm_count * blocks_per_sm);
+  if (grid < 1) grid = 1;
+  row_gather_kernel<GS, MAXROW><<<(int)grid, 256, sm, ctx->stream>>>(g);
+  CD_LAUNCHED(ctx);
+  return CDGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// driver
+// ---------------------------------------------------------------------------
+int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir)
+{
+  if (s.nnz < 0) return fail(ctx, CDGPU_ERR_INVALID, "assemble: no pattern (call cdgpu_build_pattern)");
+  if (!s.co_set) return fail(ctx, CDGPU_ERR_INVALID, "assemble: coefficients not set");
+  if (disctype != CDGPU_GALERKIN && disctype != CDGPU_SUPG)
+    return fail(ctx, CDGPU_ERR_UNSUPPORTED, "assemble: DISCTYPE must be GALERKIN (1) or SUPG (2)");
+  int rc;
+  if (!s.d_a)
+  {
+    if ((rc = dev_alloc(ctx, &s.d_a, s.nnz)) || (rc = dev_alloc(ctx, &s.d_a32, s.nnz)) ||
+        (rc = dev_alloc(ctx, &s.d_rhs, s.n_dof)) || (rc = dev_alloc(ctx, &s.d_diag, s.n_dof)) ||
+        (rc = dev_alloc(ctx, &s.d_diag32, s.n_dof)))
+      return rc;
+  }
+  int n_dir = s.n_dof - s.n_active;
+  const double *d_dir = nullptr;
+  if (h_dir && n_dir > 0)
+  {
+    if ((rc = dev_alloc(ctx, &s.d_dir, n_dir))) return rc;
+    CD_CUDA(ctx, cudaMemcpyAsync(s.d_dir, h_dir, sizeof(double) * n_dir, cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    d_dir = s.d_dir;
+  }
+  RefElement re;
+  make_ref_element(s.dim, s.order, re);
+  bool fast = s.all_affine && s.co.kind == CDGPU_COEFF_CONSTANT;
+  int T = n_tensors(s.dim, disctype), Tr = n_rhs_tensors(s.dim, disctype);
+  Coef co = to_coef(s.co);
+  if (fast)
+  {
+    if (s.ref_disctype != disctype)
+    {
+      std::vector<double> R, r;
+      reference_tensors(re, disctype, R, r);
+      std::vector<double> both(R);
+      both.insert(both.end(), r.begin(), r.end());
+      if ((rc = dev_alloc(ctx, &s.d_ref, both.size()))) return rc;
+      CD_CUDA(ctx, cudaMemcpy(s.d_ref, both.data(), both.size() * sizeof(double), cudaMemcpyHostToDevice));
+      s.ref_disctype = disctype;
+    }
+    if (!s.d_cellcoef && (rc = dev_alloc(ctx, &s.d_cellcoef, (size_t)s.n_cells * (CD_MAXT + 4))))
+      return rc;
+    CellCoefArgs a{s.dim, s.nv, s.n_cells, disctype, T, Tr, co, s.d_coords, s.d_cellcoef};
+    cell_coef_kernel<<<(s.n_cells + 127) / 128, 128, 0, ctx->stream>>>(a);
+    CD_LAUNCHED(ctx);
+  }
+  else
+  {
+    static thread_local std::vector<double> dummy;
+    double *d_tab = nullptr;
+    std::vector<double> packed;
+    // reference tables for the quadrature path
+    packed.insert(packed.end(), re.qx.begin(), re.qx.end());
+    packed.insert(packed.end(), re.qw.begin(), re.qw.end());
+    packed.insert(packed.end(), re.phi.begin(), re.phi.end());
+    packed.insert(packed.end(), re.dphi.begin(), re.dphi.end());
+    packed.insert(packed.end(), re.hphi.begin(), re.hphi.end());
+    if ((rc = dev_alloc(ctx, &s.d_ref, packed.size()))) return rc;
+    s.ref_disctype = -1;
+    CD_CUDA(ctx, cudaMemcpyAsync(s.d_ref, packed.data(), packed.size() * sizeof(double),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+    CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (s.co.kind == CDGPU_COEFF_TABLE)
+    {
+      if (!s.d_tab) return fail(ctx, CDGPU_ERR_INVALID, "assemble: coefficient table missing");
+      d_tab = s.d_tab;
+    }
+    if (!s.d_local && (rc = dev_alloc(ctx, &s.d_local, (size_t)s.n_cells * (s.nbf * s.nbf + s.nbf))))
+      return rc;
+    const double *base = s.d_ref;
+    LocalArgs a;
+    a.dim = s.dim; a.nv = s.nv; a.nbf = s.nbf; a.nq = re.nq; a.n_cells = s.n_cells;
+    a.disctype = disctype; a.affine_all = s.all_affine; a.co = co; a.coords = s.d_coords; a.tab = d_tab;
+    a.qx = base; a.qw = a.qx + re.qx.size(); a.phi = a.qw + re.qw.size();
+    a.dphi = a.phi + re.phi.size(); a.hphi = a.dphi + re.dphi.size(); a.out = s.d_local;
+    size_t sm = sizeof(double) * ((size_t)re.nq * s.nbf * s.dim + (size_t)re.nq * s.nbf + re.nq * 8 +
+                                  (size_t)re.nq * s.dim * s.dim);
+    CD_CUDA(ctx, cudaFuncSetAttribute(local_quad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    local_quad_kernel<<<s.n_cells, 256, sm, ctx->stream>>>(a);
+    CD_LAUNCHED(ctx);
+    (void)dummy;
+  }
+  int *d_err = nullptr;
+  if ((rc = dev_alloc(ctx, &d_err, 1))) return rc;
+  CD_CUDA(ctx, cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
+  GatherArgs g;
+  g.n_dof = s.n_dof; g.n_active = s.n_active; g.nbf = s.nbf; g.T = T; g.Tr = Tr; g.mode = fast ? 0 : 1;
+  g.row_ptr = s.d_row_ptr; g.kcol = s.d_kcol; g.inc_ptr = s.d_inc_ptr; g.inc = s.d_inc; g.gn = s.d_gn;
+  g.cellcoef = s.d_cellcoef; g.local = s.d_local; g.R = s.d_ref;
+  g.r = s.d_ref + (size_t)s.nbf * s.nbf * T; g.dir = d_dir;
+  g.a = s.d_a; g.rhs = s.d_rhs; g.diag = s.d_diag; g.a32 = s.d_a32; g.diag32 = s.d_diag32; g.err = d_err;
+  if (s.dim == 2 && s.order == 1) rc = launch_gather<4, 16>(ctx, g, s.n_dof);
+  else if (s.dim == 2) rc = launch_gather<16, 32>(ctx, g, s.n_dof);
+  else if (s.order == 1) rc = launch_gather<8, 32>(ctx, g, s.n_dof);
+  else rc = launch_gather<32, CD_MAXROW>(ctx, g, s.n_dof);
+  if (rc) { cudaFree(d_err); return rc; }
+  int h_err = 0;
+  cudaError_t e = cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d_err);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "assemble");
+  if (h_err == 1) return fail(ctx, CDGPU_ERR_PATTERN, "assemble: a cell coupling is missing from the CSR pattern");
+  if (h_err == 2) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "assemble: CSR row longer than the kernel's row buffer");
+  s.assembled = true;
+  s.assembly_version++;
+  return CDGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Neumann data (Assemble2D.C:797-827): one CTA, edges in order, so every DOF's sum
+// runs in the same order on every call.
+// ---------------------------------------------------------------------------
+__global__ void neumann_kernel(int order, int nbf, int n_edges, const double *coords,
+                               const int *gn, int n_active, const int *cell, const int *edge,
+                               const double *g, double *rhs)
+{
+  const double r2[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
+  int nl = order + 1;
+  double z[4], w[4];
+  if (nl == 2) { z[0] = -1.0 / sqrt(3.0); z[1] = -z[0]; w[0] = w[1] = 1.0; }
+  else { z[0] = -sqrt(0.6); z[1] = 0; z[2] = sqrt(0.6); w[0] = w[2] = 5.0 / 9.0; w[1] = 8.0 / 9.0; }
+  for (int e = 0; e < n_edges; e++)
+  {
+    int c = cell[e], m = edge[e], m1 = (m + 1) % 4;
+    const double *V = coords + (size_t)c * 8;
+    double hE = sqrt((V[2 * m1] - V[2 * m]) * (V[2 * m1] - V[2 * m]) +
+                     (V[2 * m1 + 1] - V[2 * m + 1]) * (V[2 * m1 + 1] - V[2 * m + 1])) / 2;
+    int k = threadIdx.x;
+    if (k < nbf)
+    {
+      int kx = k % (order + 1), ky = k / (order + 1);
+      double add = 0;
+      for (int l = 0; l < nl; l++)
+      {
+        double s = 0.5 * (z[l] + 1);
+        double xi = r2[m][0] + (r2[m1][0] - r2[m][0]) * s, eta = r2[m][1] + (r2[m1][1] - r2[m][1]) * s;
+        double vx, vy;
+        if (order == 1) { vx = kx ? 0.5 * (1 + xi) : 0.5 * (1 - xi); vy = ky ? 0.5 * (1 + eta) : 0.5 * (1 - eta); }
+        else
+        {
+          vx = kx == 0 ? 0.5 * xi * (xi - 1) : kx == 1 ? 1 - xi * xi : 0.5 * xi * (xi + 1);
+          vy = ky == 0 ? 0.5 * eta * (eta - 1) : ky == 1 ? 1 - eta * eta : 0.5 * eta * (eta + 1);
+        }
+        add += g[e * nl + l] * hE * w[l] * vx * vy;
+      }
+      int d = gn[(size_t)c * nbf + k];
+      if (d < n_active) rhs[d] += add;
+    }
+    __syncthreads();
+  }
+}
+
+int add_neumann(cdgpu_ctx *ctx, Space &s, int n_edges, const int *cell, const int *edge,
+                const double *g)
+{
+  if (s.dim != 2) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "Neumann data: 2D only");
+  if (!s.assembled) return fail(ctx, CDGPU_ERR_INVALID, "Neumann data: assemble first");
+  if (n_edges <= 0) return CDGPU_OK;
+  int nl = s.order + 1, rc;
+  int *d_cell = nullptr, *d_edge = nullptr;
+  double *d_g = nullptr;
+  if ((rc = dev_alloc(ctx, &d_cell, n_edges)) || (rc = dev_alloc(ctx, &d_edge, n_edges)) ||
+      (rc = dev_alloc(ctx, &d_g, (size_t)n_edges * nl)))
+    return rc;
+  for (int e = 0; e < n_edges; e++)
+    if (cell[e] < 0 || cell[e] >= s.n_cells || edge[e] < 0 || edge[e] > 3)
+      return fail(ctx, CDGPU_ERR_INVALID, "Neumann data: bad cell or edge index");
+  CD_CUDA(ctx, cudaMemcpyAsync(d_cell, cell, sizeof(int) * n_edges, cudaMemcpyHostToDevice, ctx->stream));
+  CD_CUDA(ctx, cudaMemcpyAsync(d_edge, edge, sizeof(int) * n_edges, cudaMemcpyHostToDevice, ctx->stream));
+  CD_CUDA(ctx, cudaMemcpyAsync(d_g, g, sizeof(double) * n_edges * nl, cudaMemcpyHostToDevice, ctx->stream));
+  neumann_kernel<<<1, 32, 0, ctx->stream>>>(s.order, s.nbf, n_edges, s.d_coords, s.d_gn, s.n_active,
+                                            d_cell, d_edge, d_g, s.d_rhs);
+  CD_LAUNCHED(ctx);
+  CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  cudaFree(d_cell); cudaFree(d_edge); cudaFree(d_g);
+  return CDGPU_OK;
+}

@@ -1,0 +1,161 @@
+// Internal declarations of libcdgpu (not part of the public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/cdgpu.h"
+
+#define CD_MAXBF 27   // Q2 hexahedron
+#define CD_MAXQ 64    // Gauss4 on hexahedra
+#define CD_MAXT 14    // reference tensors of the affine fast path
+#define CD_MAXROW 128 // longest CSR row of a conforming Q2 hexahedral mesh is 125
+
+// ---------------------------------------------------------------------------
+// reference element: tensor-product Lagrange basis, Gauss rules, reference tensors
+// ---------------------------------------------------------------------------
+struct RefElement
+{
+  int dim = 0, order = 0, nbf = 0, nq = 0, nv = 0;
+  std::vector<double> qx, qw;          // nq x dim, nq
+  std::vector<double> phi, dphi, hphi; // nq x nbf, nq x nbf x dim, nq x nbf x dim x dim
+};
+void make_ref_element(int dim, int order, RefElement &re);
+void basis_eval(int dim, int order, const double *xi, double *val, double *grad);
+int n_tensors(int dim, int disctype);
+int n_rhs_tensors(int dim, int disctype);
+// R[(i*nbf + j)*T + t] and r[i*Tr + t]
+void reference_tensors(const RefElement &re, int disctype, std::vector<double> &R,
+                       std::vector<double> &r);
+
+// ---------------------------------------------------------------------------
+// finite element space with its matrix
+// ---------------------------------------------------------------------------
+struct Space
+{
+  int dim = 0, order = 0, nbf = 0, nv = 0, n_cells = 0, n_dof = 0, n_active = 0;
+  std::vector<double> h_coords;
+  std::vector<int> h_gn;
+  bool all_affine = true;
+  double *d_coords = nullptr;
+  int *d_gn = nullptr;
+  // CSR pattern (bit-identical to TSquareStructure + Sort)
+  long nnz = -1;
+  std::vector<int> h_row_ptr, h_kcol;
+  int *d_row_ptr = nullptr, *d_kcol = nullptr;
+  int *d_dir_start = nullptr; // first slot of each row whose column is a Dirichlet DOF
+  // DOF -> (cell, local index) incidence, ascending cell per DOF
+  int *d_inc_ptr = nullptr, *d_inc = nullptr;
+  // values
+  double *d_a = nullptr, *d_rhs = nullptr, *d_diag = nullptr;
+  float *d_a32 = nullptr, *d_diag32 = nullptr;
+  bool assembled = false;
+  long assembly_version = 0;
+  // coefficients
+  cdgpu_coeffs co{};
+  bool co_set = false;
+  double *d_tab = nullptr;
+  // assembly scratch
+  double *d_cellcoef = nullptr; // affine path: n_cells x (T + Tr)
+  double *d_local = nullptr;    // quadrature path: n_cells x (nbf*nbf + nbf)
+  double *d_dir = nullptr;      // Dirichlet values
+  double *d_ref = nullptr;      // reference tensors (affine path)
+  int ref_disctype = -1;
+  int n_tab = 0;
+};
+
+// ---------------------------------------------------------------------------
+// multigrid hierarchy
+// ---------------------------------------------------------------------------
+template <typename T> struct LevelVec
+{
+  T *sol = nullptr, *alt = nullptr, *rhs = nullptr, *def = nullptr;
+};
+
+struct Level
+{
+  Space *sp = nullptr;
+  // prolongation from the next coarser level (rows = this level's DOFs) and its transpose
+  int *d_p_row = nullptr, *d_p_col = nullptr, *d_r_row = nullptr, *d_r_col = nullptr;
+  double *d_p_val = nullptr, *d_r_val = nullptr;
+  float *d_p_val32 = nullptr, *d_r_val32 = nullptr;
+  long p_nnz = 0;
+  LevelVec<double> v64;
+  LevelVec<float> v32;
+};
+
+struct Hierarchy
+{
+  std::vector<Level> lev;
+  double *d_cinv = nullptr; // explicit inverse of the coarsest matrix (exact coarse solve)
+  long cinv_version = -1;
+  // FGMRES workspace
+  int m = 0;
+  double *d_V = nullptr, *d_Z = nullptr, *d_w = nullptr, *d_ctl = nullptr, *d_partial = nullptr;
+  double *h_ctl = nullptr; // pinned mirror of the control block
+  int partial_blocks = 0;
+  double *d_x = nullptr, *d_b = nullptr; // host-API staging vectors
+};
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct cdgpu_ctx
+{
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  long long launches = 0;
+  std::vector<Space *> spaces;
+  std::vector<Hierarchy *> mgs;
+};
+
+// error helpers: set ctx->err and return a status
+int fail(cdgpu_ctx *ctx, int status, const std::string &msg);
+int cuda_fail(cdgpu_ctx *ctx, cudaError_t e, const char *what);
+#define CD_CUDA(ctx, call)                                   \
+  do {                                                       \
+    cudaError_t e_ = (call);                                 \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+#define CD_LAUNCHED(ctx)                                                  \
+  do {                                                                    \
+    (ctx)->launches++;                                                    \
+    cudaError_t e_ = cudaGetLastError();                                  \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, "kernel launch");   \
+  } while (0)
+
+template <typename T> int dev_alloc(cdgpu_ctx *ctx, T **p, size_t n)
+{
+  if (*p) { cudaFree(*p); *p = nullptr; }
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+  if (e != cudaSuccess) { *p = nullptr; cudaGetLastError(); return fail(ctx, CDGPU_ERR_OOM, "cudaMalloc failed"); }
+  return CDGPU_OK;
+}
+
+// host-side setup algorithms (setup.cpp)
+void build_pattern(const Space &s, std::vector<int> &row_ptr, std::vector<int> &kcol);
+void build_incidence(const Space &s, std::vector<int> &ptr, std::vector<int> &inc);
+bool cell_is_affine(int dim, const double *V);
+void ref_map(int dim, bool affine, const double *V, const double *xi, double *x, double *J);
+double invert(int dim, const double *J, double *Ji);
+double cell_diameter(int dim, const double *V);
+void build_prolongation(const Space &coarse, const Space &fine, const int *parent,
+                        std::vector<int> &row, std::vector<int> &col, std::vector<double> &val);
+bool dense_inverse(int n, std::vector<double> &a); // in place, row-major; false if singular
+
+// device entry points (assemble.cu / solve.cu)
+int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir);
+int add_neumann(cdgpu_ctx *ctx, Space &s, int n_edges, const int *cell, const int *edge,
+                const double *g);
+int spmv64(cdgpu_ctx *ctx, const Space &s, const double *x, double *y);
+int defect64(cdgpu_ctx *ctx, const Space &s, const double *x, const double *f, double *d,
+             double *res);
+int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m);
+int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *d_rhs,
+              double *d_sol, cdgpu_solve_info *info);

@@ -1,0 +1,960 @@
+// Solver kernels and drivers of libcdgpu (sm_100a): CSR SpMV / defect, damped
+// Jacobi, transfer operators, coarse solves, and the multigrid-preconditioned
+// FGMRES and fixed-point iterations.
+//
+// The V-cycle follows TMultiGrid3D::Cycle (src/FE/MultiGrid3D.C:423-669) state for
+// state: pre-smoothing, defect, restriction with CorrectDefect and Reset of the
+// coarse solution, recursion, prolongation with CorrectNodes, Update with
+// SC_GMG_DAMP_FACTOR_SCALAR, post-smoothing.  The three defects the reference
+// computes only to print residuals (before pre-smoothing, after the update, after
+// post-smoothing) change no state and are not computed.  Jacobi sweeps write into a
+// second buffer and swap pointers instead of copying sol into aux first
+// (MGLevel3D.C:455), which gives the same values.  A level whose solution is known
+// to be zero (after Reset) starts with a sweep that reads no matrix row.
+//
+// FGMRES follows TFgmresIte::Iterate (src/FE/FgmresIte.C:236-582): same restart,
+// stopping and divergence rules, the same Givens rotations computed on the host in
+// FP64; the Arnoldi orthogonalisation is classical Gram-Schmidt applied twice
+// (two fused passes over the basis) instead of modified Gram-Schmidt (one kernel
+// launch per basis vector).  Both are accurate to working precision; iterates
+// differ from the reference's by rounding only.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "internal.h"
+
+namespace cg = cooperative_groups;
+
+static const int kBlock = 256;
+
+// ---------------------------------------------------------------------------
+// CSR kernels: one group of GS threads per row, grid-stride over rows
+// ---------------------------------------------------------------------------
+template <int GS, typename T> __device__ __forceinline__ T group_sum(T v)
+{
+#pragma unroll
+  for (int o = GS / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, GS);
+  return v;
+}
+
+template <typename T, int GS>
+__global__ void __launch_bounds__(kBlock) spmv_kernel(int n, const int *__restrict__ rp,
+                                                      const int *__restrict__ kc,
+                                                      const T *__restrict__ a,
+                                                      const T *__restrict__ x, T *__restrict__ y)
+{
+  const int lane = threadIdx.x % GS;
+  const int ng = gridDim.x * (blockDim.x / GS);
+  for (int r = blockIdx.x * (blockDim.x / GS) + threadIdx.x / GS; r < n; r += ng)
+  {
+    const int b = rp[r], e = rp[r + 1];
+    T s = 0;
+    for (int j = b + lane; j < e; j += GS) s += a[j] * __ldg(x + kc[j]);
+    s = group_sum<GS>(s);
+    if (lane == 0) y[r] = s;
+  }
+}
+
+// d = f - A x, and per-block partial sums of d^2 (fixed order -> deterministic)
+template <typename T, int GS>
+__global__ void __launch_bounds__(kBlock) defect_kernel(int n, const int *__restrict__ rp,
+                                                        const int *__restrict__ kc,
+                                                        const T *__restrict__ a,
+                                                        const T *__restrict__ x,
+                                                        const T *__restrict__ f, T *__restrict__ d,
+                                                        double *__restrict__ partial)
+{
+  __shared__ double red[kBlock / GS];
+  const int lane = threadIdx.x % GS, grp = threadIdx.x / GS;
+  const int ng = gridDim.x * (blockDim.x / GS);
+  double acc = 0;
+  for (int r = blockIdx.x * (blockDim.x / GS) + grp; r < n; r += ng)
+  {
+    const int b = rp[r], e = rp[r + 1];
+    T s = 0;
+    for (int j = b + lane; j < e; j += GS) s += a[j] * __ldg(x + kc[j]);
+    s = group_sum<GS>(s);
+    if (lane == 0)
+    {
+      T v = f[r] - s;
+      d[r] = v;
+      acc += (double)v * (double)v;
+    }
+  }
+  if (partial)
+  {
+    if (lane == 0) red[grp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+      double t = 0;
+      for (int g = 0; g < kBlock / GS; g++) t += red[g];
+      partial[blockIdx.x] = t;
+    }
+  }
+}
+
+// damped Jacobi sweep (MGLevel3D.C:443-537 / MGLevel2D.C:318-368) from x_in into x_out
+template <typename T, int GS>
+__global__ void __launch_bounds__(kBlock) jacobi_kernel(int n, int n_active,
+                                                        const int *__restrict__ rp,
+                                                        const int *__restrict__ kc,
+                                                        const T *__restrict__ a,
+                                                        const T *__restrict__ diag,
+                                                        const T *__restrict__ x,
+                                                        const T *__restrict__ f,
+                                                        T *__restrict__ xo, T omega)
+{
+  const int lane = threadIdx.x % GS;
+  const int ng = gridDim.x * (blockDim.x / GS);
+  for (int r = blockIdx.x * (blockDim.x / GS) + threadIdx.x / GS; r < n; r += ng)
+  {
+    if (r >= n_active)
+    {
+      if (lane == 0) xo[r] = f[r];
+      continue;
+    }
+    const int b = rp[r], e = rp[r + 1];
+    T s = 0;
+    for (int j = b + lane; j < e; j += GS)
+    {
+      int c = kc[j];
+      if (c != r) s += a[j] * __ldg(x + c);
+    }
+    s = group_sum<GS>(s);
+    if (lane == 0)
+    {
+      T t = x[r];
+      xo[r] = (T(1) - omega) * t + omega * (f[r] - s) / diag[r];
+    }
+  }
+}
+
+// first sweep when the active part of x is zero: only Dirichlet columns (numbered last,
+// so at the end of every sorted row, from dir_start[r]) can contribute
+template <typename T>
+__global__ void jacobi_first_kernel(int n, int n_active, const int *__restrict__ rp,
+                                    const int *__restrict__ kc, const int *__restrict__ dir_start,
+                                    const T *__restrict__ a, const T *__restrict__ diag,
+                                    const T *__restrict__ x, const T *__restrict__ f,
+                                    T *__restrict__ xo, T omega, int x_all_zero)
+{
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  if (r >= n_active) { xo[r] = f[r]; return; }
+  T s = f[r];
+  if (!x_all_zero)
+    for (int j = dir_start[r]; j < rp[r + 1]; j++) s -= a[j] * x[kc[j]];
+  xo[r] = omega * s / diag[r];
+}
+
+// coarse right-hand side = R d, zero on non-active rows (CorrectDefect, MGLevel3D.C:588),
+// coarse solution reset to zero (MGLevel3D.C:557)
+template <typename T, int GS>
+__global__ void __launch_bounds__(kBlock) restrict_kernel(int nc, int nc_active,
+                                                          const int *__restrict__ rr,
+                                                          const int *__restrict__ rc,
+                                                          const T *__restrict__ rv,
+                                                          const T *__restrict__ d,
+                                                          T *__restrict__ crhs, T *__restrict__ csol)
+{
+  const int lane = threadIdx.x % GS;
+  const int ng = gridDim.x * (blockDim.x / GS);
+  for (int r = blockIdx.x * (blockDim.x / GS) + threadIdx.x / GS; r < nc; r += ng)
+  {
+    T s = 0;
+    if (r < nc_active)
+      for (int j = rr[r] + lane; j < rr[r + 1]; j += GS) s += rv[j] * __ldg(d + rc[j]);
+    s = group_sum<GS>(s);
+    if (lane == 0) { crhs[r] = s; csol[r] = 0; }
+  }
+}
+
+// sol += damp * (P xc) on active rows; the correction of Dirichlet rows is zeroed
+// (CorrectNodes, MGLevel3D.C:562) so they are left unchanged (Update, MGLevel3D.C:539)
+template <typename T, int GS>
+__global__ void __launch_bounds__(kBlock) prolong_kernel(int nf, int nf_active,
+                                                         const int *__restrict__ pr,
+                                                         const int *__restrict__ pc,
+                                                         const T *__restrict__ pv,
+                                                         const T *__restrict__ xc,
+                                                         T *__restrict__ sol, T damp)
+{
+  const int lane = threadIdx.x % GS;
+  const int ng = gridDim.x * (blockDim.x / GS);
+  for (int r = blockIdx.x * (blockDim.x / GS) + threadIdx.x / GS; r < nf_active; r += ng)
+  {
+    T s = 0;
+    for (int j = pr[r] + lane; j < pr[r + 1]; j += GS) s += pv[j] * __ldg(xc + pc[j]);
+    s = group_sum<GS>(s);
+    if (lane == 0) sol[r] += damp * s;
+  }
+}
+
+// exact coarse solve with the explicit FP64 inverse of the whole coarse matrix
+// (Dirichlet identity rows included, like SolveExact, MGLevel3D.C:839)
+template <typename T>
+__global__ void coarse_exact_kernel(int n, const double *__restrict__ cinv, const T *__restrict__ rhs,
+                                    T *__restrict__ sol)
+{
+  extern __shared__ double b[];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) b[i] = (double)rhs[i];
+  __syncthreads();
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nw = blockDim.x / 32;
+  for (int r = warp; r < n; r += nw)
+  {
+    double s = 0;
+    for (int j = lane; j < n; j += 32) s += cinv[(size_t)r * n + j] * b[j];
+    s = group_sum<32>(s);
+    if (lane == 0) sol[r] = (T)s;
+  }
+}
+
+// coarse smoother loop (MultiGrid3D.C:199-311): iterate the coarse smoother until the
+// defect norm drops by SC_COARSE_RED_FACTOR_SCALAR or SC_COARSE_MAXIT_SCALAR sweeps,
+// in one CTA; mode 1 Jacobi, 2 SOR, 3 SSOR (MGLevel3D.C:254-537)
+template <typename T>
+__global__ void coarse_smooth_kernel(int n, int n_active, const int *__restrict__ rp,
+                                     const int *__restrict__ kc, const T *__restrict__ a,
+                                     const T *__restrict__ f, T *__restrict__ sol, double omega,
+                                     int mode, int maxit, double red_factor)
+{
+  extern __shared__ double sh[];
+  double *x = sh, *aux = sh + n;
+  __shared__ double red[32];
+  __shared__ double res_s;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = (double)sol[i];
+  __syncthreads();
+  auto defect_norm = [&]() {
+    double acc = 0;
+    for (int r = threadIdx.x; r < n; r += blockDim.x)
+    {
+      double s = (double)f[r];
+      for (int j = rp[r]; j < rp[r + 1]; j++) s -= (double)a[j] * x[kc[j]];
+      acc += s * s;
+    }
+    acc = group_sum<32>(acc);
+    if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+      double t = 0;
+      for (int w = 0; w < (int)blockDim.x / 32; w++) t += red[w];
+      res_s = sqrt(t);
+    }
+    __syncthreads();
+    return res_s;
+  };
+  double res = defect_norm();
+  double target = red_factor * res;
+  int it = 0;
+  while (res > target && it < maxit)
+  {
+    // Dirichlet rows take the right-hand side
+    for (int i = n_active + threadIdx.x; i < n; i += blockDim.x) x[i] = (double)f[i];
+    __syncthreads();
+    if (mode == 1)
+    {
+      for (int i = threadIdx.x; i < n; i += blockDim.x) aux[i] = x[i];
+      __syncthreads();
+      for (int r = threadIdx.x; r < n_active; r += blockDim.x)
+      {
+        double s = (double)f[r], dg = 1;
+        for (int j = rp[r]; j < rp[r + 1]; j++)
+        {
+          int c = kc[j];
+          if (c == r) dg = (double)a[j]; else s -= (double)a[j] * aux[c];
+        }
+        x[r] = (1 - omega) * aux[r] + omega * s / dg;
+      }
+      __syncthreads();
+    }
+    else
+    {
+      if (threadIdx.x < 32)
+      {
+        const int lane = threadIdx.x;
+        for (int pass = 0; pass < (mode == 3 ? 2 : 1); pass++)
+          for (int ii = 0; ii < n_active; ii++)
+          {
+            int r = pass == 0 ? ii : n_active - 1 - ii;
+            double s = 0, dg = 0;
+            for (int j = rp[r] + lane; j < rp[r + 1]; j += 32)
+            {
+              int c = kc[j];
+              if (c == r) dg = (double)a[j]; else s += (double)a[j] * x[c];
+            }
+            s = group_sum<32>(s);
+            dg = group_sum<32>(dg);
+            if (lane == 0)
+            {
+              double t = x[r];
+              x[r] = omega * (((double)f[r] - s) / dg - t) + t;
+            }
+            __syncwarp();
+          }
+      }
+      __syncthreads();
+    }
+    res = defect_norm();
+    it++;
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sol[i] = (T)x[i];
+}
+
+// ---------------------------------------------------------------------------
+// dense vector kernels for FGMRES (FP64)
+// ---------------------------------------------------------------------------
+// per-block partial dot products of w with k basis vectors Y[0..k) (row stride n)
+// optionally after w -= Y coef (fused), and/or partial ||w||^2 (slot k)
+__global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, int k, const double *__restrict__ Y,
+                                                         double *__restrict__ w,
+                                                         const double *__restrict__ coef,
+                                                         int do_dots, double *__restrict__ partial)
+{
+  __shared__ double red[kBlock / 32][33];
+  double acc[33];
+#pragma unroll
+  for (int j = 0; j < 33; j++) acc[j] = 0;
+  double cf[32];
+  if (coef)
+    for (int j = 0; j < k; j++) cf[j] = coef[j];
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+  {
+    double wi = w[i];
+    if (coef)
+    {
+      for (int j = 0; j < k; j++) wi -= cf[j] * Y[(size_t)j * n + i];
+      w[i] = wi;
+    }
+    if (do_dots)
+      for (int j = 0; j < k; j++) acc[j] += wi * Y[(size_t)j * n + i];
+    acc[32] += wi * wi;
+  }
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+  int nslots = do_dots ? k : 0;
+  for (int j = 0; j <= nslots; j++)
+  {
+    int slot = j < nslots ? j : 32;
+    double v = group_sum<32>(acc[slot]);
+    if (lane == 0) red[warp][j] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x <= nslots)
+  {
+    double t = 0;
+    for (int g = 0; g < kBlock / 32; g++) t += red[g][threadIdx.x];
+    partial[(size_t)blockIdx.x * 33 + threadIdx.x] = t;
+  }
+}
+
+// sum per-block partials in block order: out[j] = sum_b partial[b][j], j <= nslots
+__global__ void reduce_partials_kernel(int nblocks, int nslots, const double *__restrict__ partial,
+                                       double *__restrict__ out)
+{
+  int j = threadIdx.x;
+  if (j > nslots) return;
+  double t = 0;
+  for (int b = 0; b < nblocks; b++) t += partial[(size_t)b * 33 + j];
+  out[j] = t;
+}
+
+__global__ void sum_blocks_kernel(int nblocks, const double *__restrict__ partial, double *out)
+{
+  __shared__ double red[32];
+  double t = 0;
+  // fixed per-thread order, then fixed tree
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) t += partial[b];
+  t = group_sum<32>(t);
+  if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = t;
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
+    double s = 0;
+    for (int w = 0; w < (int)blockDim.x / 32; w++) s += red[w];
+    out[0] = s;
+  }
+}
+
+__global__ void scale_kernel(int n, double alpha, const double *__restrict__ x, double *__restrict__ y)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = alpha * x[i];
+}
+
+// x += sum_j c[j] Z[j]
+__global__ void update_kernel(int n, int k, const double *__restrict__ c, const double *__restrict__ Z,
+                              double *__restrict__ x)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0;
+  for (int j = 0; j < k; j++) s += c[j] * Z[(size_t)j * n + i];
+  x[i] += s;
+}
+
+__global__ void axpy_kernel(int n, double alpha, const double *__restrict__ x, double *__restrict__ y)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] += alpha * x[i];
+}
+
+template <typename A, typename B> __global__ void convert_kernel(int n, const A *__restrict__ x, B *__restrict__ y)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = (B)x[i];
+}
+
+// zero a vector and copy the Dirichlet part of rhs into it (MultiGridScaIte.C:79-85:
+// zero start + SetDirichletNodes, MultiGrid3D.C:671)
+template <typename T, typename S>
+__global__ void mg_start_kernel(int n, int n_active, const S *__restrict__ rhs_in, T *__restrict__ rhs,
+                                T *__restrict__ sol)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  T v = (T)rhs_in[i];
+  rhs[i] = v;
+  sol[i] = i < n_active ? T(0) : v;
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+static int grid_for(cdgpu_ctx *ctx, long rows, int gs)
+{
+  long groups_per_block = kBlock / gs;
+  long need = (rows + groups_per_block - 1) / groups_per_block;
+  long cap = (long)ctx->sm_count * (2048 / kBlock);
+  return (int)std::max<long>(1, std::min(need, cap));
+}
+
+static int group_size(const Space &s)
+{
+  if (s.dim == 3 && s.order == 2) return 32;
+  if (s.dim == 3 || s.order == 2) return 16;
+  return 8;
+}
+
+#define GS_DISPATCH(gs, KERNEL, ...)                 \
+  do {                                               \
+    switch (gs)                                      \
+    {                                                \
+      case 32: KERNEL<32> __VA_ARGS__; break;        \
+      case 16: KERNEL<16> __VA_ARGS__; break;        \
+      case 8: KERNEL<8> __VA_ARGS__; break;          \
+      default: KERNEL<4> __VA_ARGS__; break;         \
+    }                                                \
+  } while (0)
+
+template <typename T> static const T *mat(const Space &s);
+template <> const double *mat<double>(const Space &s) { return s.d_a; }
+template <> const float *mat<float>(const Space &s) { return s.d_a32; }
+template <typename T> static const T *dg(const Space &s);
+template <> const double *dg<double>(const Space &s) { return s.d_diag; }
+template <> const float *dg<float>(const Space &s) { return s.d_diag32; }
+template <typename T> static const T *pval(const Level &l);
+template <> const double *pval<double>(const Level &l) { return l.d_p_val; }
+template <> const float *pval<float>(const Level &l) { return l.d_p_val32; }
+template <typename T> static const T *rval(const Level &l);
+template <> const double *rval<double>(const Level &l) { return l.d_r_val; }
+template <> const float *rval<float>(const Level &l) { return l.d_r_val32; }
+template <typename T> static LevelVec<T> &vecs(Level &l);
+template <> LevelVec<double> &vecs<double>(Level &l) { return l.v64; }
+template <> LevelVec<float> &vecs<float>(Level &l) { return l.v32; }
+
+template <typename T, int GS>
+static void launch_jacobi(cdgpu_ctx *ctx, const Space &s, const T *x, const T *f, T *xo, T omega)
+{
+  jacobi_kernel<T, GS><<<grid_for(ctx, s.n_dof, GS), kBlock, 0, ctx->stream>>>(
+      s.n_dof, s.n_active, s.d_row_ptr, s.d_kcol, mat<T>(s), dg<T>(s), x, f, xo, omega);
+}
+template <typename T, int GS>
+static void launch_defect(cdgpu_ctx *ctx, const Space &s, const T *x, const T *f, T *d, double *partial,
+                          int grid)
+{
+  defect_kernel<T, GS><<<grid, kBlock, 0, ctx->stream>>>(s.n_dof, s.d_row_ptr, s.d_kcol, mat<T>(s), x,
+                                                         f, d, partial);
+}
+template <typename T, int GS>
+static void launch_spmv(cdgpu_ctx *ctx, const Space &s, const T *x, T *y)
+{
+  spmv_kernel<T, GS><<<grid_for(ctx, s.n_dof, GS), kBlock, 0, ctx->stream>>>(
+      s.n_dof, s.d_row_ptr, s.d_kcol, mat<T>(s), x, y);
+}
+
+template <typename T> static int jacobi_sweep(cdgpu_ctx *ctx, Level &L, T omega)
+{
+  LevelVec<T> &v = vecs<T>(L);
+  const Space &s = *L.sp;
+  int gs = group_size(s);
+  switch (gs)
+  {
+    case 32: launch_jacobi<T, 32>(ctx, s, v.sol, v.rhs, v.alt, omega); break;
+    case 16: launch_jacobi<T, 16>(ctx, s, v.sol, v.rhs, v.alt, omega); break;
+    default: launch_jacobi<T, 8>(ctx, s, v.sol, v.rhs, v.alt, omega); break;
+  }
+  CD_LAUNCHED(ctx);
+  std::swap(v.sol, v.alt);
+  return CDGPU_OK;
+}
+
+template <typename T> static int jacobi_first(cdgpu_ctx *ctx, Level &L, T omega, int all_zero)
+{
+  LevelVec<T> &v = vecs<T>(L);
+  const Space &s = *L.sp;
+  jacobi_first_kernel<T><<<(s.n_dof + 255) / 256, 256, 0, ctx->stream>>>(
+      s.n_dof, s.n_active, s.d_row_ptr, s.d_kcol, s.d_dir_start, mat<T>(s), dg<T>(s), v.sol, v.rhs,
+      v.alt, omega, all_zero);
+  CD_LAUNCHED(ctx);
+  std::swap(v.sol, v.alt);
+  return CDGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// V/W/F cycle
+// ---------------------------------------------------------------------------
+struct CycleState
+{
+  const cdgpu_solver_params *p;
+  int rec[64];
+  bool sol_zero[64];   // active part and Dirichlet part zero
+  bool active_zero[64];
+};
+
+template <typename T> static int smooth(cdgpu_ctx *ctx, Hierarchy &h, CycleState &cs, int i, int count)
+{
+  Level &L = h.lev[i];
+  T omega = (T)cs.p->omega;
+  int rc;
+  for (int k = 0; k < count; k++)
+  {
+    if (cs.active_zero[i])
+      rc = jacobi_first<T>(ctx, L, omega, cs.sol_zero[i] ? 1 : 0);
+    else
+      rc = jacobi_sweep<T>(ctx, L, omega);
+    if (rc) return rc;
+    cs.active_zero[i] = cs.sol_zero[i] = false;
+  }
+  return CDGPU_OK;
+}
+
+template <typename T> static int coarse_solve(cdgpu_ctx *ctx, Hierarchy &h, CycleState &cs)
+{
+  Level &L = h.lev[0];
+  const Space &s = *L.sp;
+  LevelVec<T> &v = vecs<T>(L);
+  if (cs.p->coarse_smoother == 17)
+  {
+    size_t sm = sizeof(double) * s.n_dof;
+    coarse_exact_kernel<T><<<1, 1024, sm, ctx->stream>>>(s.n_dof, h.d_cinv, v.rhs, v.sol);
+    CD_LAUNCHED(ctx);
+  }
+  else
+  {
+    size_t sm = sizeof(double) * 2 * s.n_dof;
+    coarse_smooth_kernel<T><<<1, 256, sm, ctx->stream>>>(s.n_dof, s.n_active, s.d_row_ptr, s.d_kcol,
+                                                         mat<T>(s), v.rhs, v.sol, cs.p->omega,
+                                                         cs.p->coarse_smoother, cs.p->coarse_maxit,
+                                                         cs.p->coarse_red);
+    CD_LAUNCHED(ctx);
+  }
+  cs.sol_zero[0] = cs.active_zero[0] = false;
+  return CDGPU_OK;
+}
+
+template <typename T> static int cycle(cdgpu_ctx *ctx, Hierarchy &h, CycleState &cs, int i)
+{
+  if (i == 0) return coarse_solve<T>(ctx, h, cs);
+  Level &L = h.lev[i], &C = h.lev[i - 1];
+  const Space &s = *L.sp, &sc = *C.sp;
+  LevelVec<T> &v = vecs<T>(L), &vc = vecs<T>(C);
+  int rc;
+  if ((rc = smooth<T>(ctx, h, cs, i, cs.p->pre))) return rc;
+  int gs = group_size(s);
+  switch (gs)
+  {
+    case 32: launch_defect<T, 32>(ctx, s, v.sol, v.rhs, v.def, nullptr, grid_for(ctx, s.n_dof, 32)); break;
+    case 16: launch_defect<T, 16>(ctx, s, v.sol, v.rhs, v.def, nullptr, grid_for(ctx, s.n_dof, 16)); break;
+    default: launch_defect<T, 8>(ctx, s, v.sol, v.rhs, v.def, nullptr, grid_for(ctx, s.n_dof, 8)); break;
+  }
+  CD_LAUNCHED(ctx);
+  restrict_kernel<T, 16><<<grid_for(ctx, sc.n_dof, 16), kBlock, 0, ctx->stream>>>(
+      sc.n_dof, sc.n_active, L.d_r_row, L.d_r_col, rval<T>(L), v.def, vc.rhs, vc.sol);
+  CD_LAUNCHED(ctx);
+  cs.sol_zero[i - 1] = cs.active_zero[i - 1] = true;
+  for (int j = 0; j < cs.rec[i]; j++)
+    if ((rc = cycle<T>(ctx, h, cs, i - 1))) return rc;
+  if (cs.p->cycle < 1) cs.rec[i] = 1;
+  prolong_kernel<T, 8><<<grid_for(ctx, s.n_active, 8), kBlock, 0, ctx->stream>>>(
+      s.n_dof, s.n_active, L.d_p_row, L.d_p_col, pval<T>(L), vc.sol, v.sol, (T)cs.p->gmg_damp);
+  CD_LAUNCHED(ctx);
+  return smooth<T>(ctx, h, cs, i, cs.p->post);
+}
+
+// one preconditioner application z = M^{-1} r (TMultiGridScaIte::Iterate with zero start)
+template <typename T>
+static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *r, double *z)
+{
+  int L = (int)h.lev.size();
+  Level &F = h.lev[L - 1];
+  LevelVec<T> &v = vecs<T>(F);
+  int n = F.sp->n_dof;
+  mg_start_kernel<T, double><<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, F.sp->n_active, r, v.rhs, v.sol);
+  CD_LAUNCHED(ctx);
+  CycleState cs;
+  cs.p = &p;
+  // SetRecursion(levels = L-1), MultiGrid3D.C:691-703
+  cs.rec[1] = 1;
+  for (int k = 2; k <= L - 1; k++) cs.rec[k] = p.cycle > 0 ? p.cycle : 2;
+  for (int k = 0; k < L; k++) cs.sol_zero[k] = cs.active_zero[k] = false;
+  cs.active_zero[L - 1] = true;
+  int rc = cycle<T>(ctx, h, cs, L - 1);
+  if (rc) return rc;
+  convert_kernel<T, double><<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, v.sol, z);
+  CD_LAUNCHED(ctx);
+  return CDGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// hierarchy buffers and the exact coarse inverse
+// ---------------------------------------------------------------------------
+template <typename T> static int alloc_vecs(cdgpu_ctx *ctx, LevelVec<T> &v, int n)
+{
+  int rc;
+  if ((rc = dev_alloc(ctx, &v.sol, n)) || (rc = dev_alloc(ctx, &v.alt, n)) ||
+      (rc = dev_alloc(ctx, &v.rhs, n)) || (rc = dev_alloc(ctx, &v.def, n)))
+    return rc;
+  CD_CUDA(ctx, cudaMemset(v.sol, 0, sizeof(T) * n));
+  CD_CUDA(ctx, cudaMemset(v.alt, 0, sizeof(T) * n));
+  return CDGPU_OK;
+}
+
+int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m)
+{
+  int rc;
+  for (auto &L : h.lev)
+  {
+    if (!L.v64.sol && (rc = alloc_vecs(ctx, L.v64, L.sp->n_dof))) return rc;
+    if (!L.v32.sol && (rc = alloc_vecs(ctx, L.v32, L.sp->n_dof))) return rc;
+  }
+  int n = h.lev.back().sp->n_dof;
+  if (h.m != m)
+  {
+    if ((rc = dev_alloc(ctx, &h.d_V, (size_t)(m + 1) * n)) || (rc = dev_alloc(ctx, &h.d_Z, (size_t)(m + 1) * n)))
+      return rc;
+    h.m = m;
+  }
+  if (!h.d_w)
+  {
+    h.partial_blocks = std::min(ctx->sm_count * 4, (n + kBlock - 1) / kBlock);
+    if (h.partial_blocks < 1) h.partial_blocks = 1;
+    if ((rc = dev_alloc(ctx, &h.d_w, n)) || (rc = dev_alloc(ctx, &h.d_ctl, 256)) ||
+        (rc = dev_alloc(ctx, &h.d_partial, (size_t)std::max(h.partial_blocks, ctx->sm_count * 8) * 33)) ||
+        (rc = dev_alloc(ctx, &h.d_x, n)) || (rc = dev_alloc(ctx, &h.d_b, n)))
+      return rc;
+    CD_CUDA(ctx, cudaMallocHost((void **)&h.h_ctl, 256 * sizeof(double)));
+  }
+  return CDGPU_OK;
+}
+
+static int refresh_coarse_inverse(cdgpu_ctx *ctx, Hierarchy &h)
+{
+  Space &s = *h.lev[0].sp;
+  if (h.d_cinv && h.cinv_version == s.assembly_version) return CDGPU_OK;
+  int n = s.n_dof;
+  if (n > 4096) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "exact coarse solve: coarsest level larger than 4096 DOFs");
+  std::vector<double> a((size_t)s.nnz), dense((size_t)n * n, 0.0);
+  CD_CUDA(ctx, cudaMemcpyAsync(a.data(), s.d_a, sizeof(double) * s.nnz, cudaMemcpyDeviceToHost, ctx->stream));
+  CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int r = 0; r < n; r++)
+    for (int j = s.h_row_ptr[r]; j < s.h_row_ptr[r + 1]; j++) dense[(size_t)r * n + s.h_kcol[j]] = a[j];
+  if (!dense_inverse(n, dense)) return fail(ctx, CDGPU_ERR_INVALID, "exact coarse solve: singular coarse matrix");
+  int rc;
+  if ((rc = dev_alloc(ctx, &h.d_cinv, dense.size()))) return rc;
+  CD_CUDA(ctx, cudaMemcpy(h.d_cinv, dense.data(), dense.size() * sizeof(double), cudaMemcpyHostToDevice));
+  h.cinv_version = s.assembly_version;
+  return CDGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 building blocks on the finest level
+// ---------------------------------------------------------------------------
+static int finest_defect_norm(cdgpu_ctx *ctx, Hierarchy &h, const double *x, const double *f, double *d,
+                              double *norm_out_dev)
+{
+  const Space &s = *h.lev.back().sp;
+  int gs = group_size(s);
+  int grid = std::min(grid_for(ctx, s.n_dof, gs), ctx->sm_count * 8);
+  switch (gs)
+  {
+    case 32: launch_defect<double, 32>(ctx, s, x, f, d, h.d_partial, grid); break;
+    case 16: launch_defect<double, 16>(ctx, s, x, f, d, h.d_partial, grid); break;
+    default: launch_defect<double, 8>(ctx, s, x, f, d, h.d_partial, grid); break;
+  }
+  CD_LAUNCHED(ctx);
+  sum_blocks_kernel<<<1, 256, 0, ctx->stream>>>(grid, h.d_partial, norm_out_dev);
+  CD_LAUNCHED(ctx);
+  return CDGPU_OK;
+}
+
+int spmv64(cdgpu_ctx *ctx, const Space &s, const double *x, double *y)
+{
+  int gs = group_size(s);
+  switch (gs)
+  {
+    case 32: launch_spmv<double, 32>(ctx, s, x, y); break;
+    case 16: launch_spmv<double, 16>(ctx, s, x, y); break;
+    default: launch_spmv<double, 8>(ctx, s, x, y); break;
+  }
+  CD_LAUNCHED(ctx);
+  return CDGPU_OK;
+}
+
+int defect64(cdgpu_ctx *ctx, const Space &s, const double *x, const double *f, double *d, double *res)
+{
+  int gs = group_size(s), rc;
+  int grid = std::min(grid_for(ctx, s.n_dof, gs), ctx->sm_count * 8);
+  double *partial = nullptr, *out = nullptr;
+  if ((rc = dev_alloc(ctx, &partial, grid)) || (rc = dev_alloc(ctx, &out, 1))) return rc;
+  switch (gs)
+  {
+    case 32: launch_defect<double, 32>(ctx, s, x, f, d, partial, grid); break;
+    case 16: launch_defect<double, 16>(ctx, s, x, f, d, partial, grid); break;
+    default: launch_defect<double, 8>(ctx, s, x, f, d, partial, grid); break;
+  }
+  CD_LAUNCHED(ctx);
+  sum_blocks_kernel<<<1, 256, 0, ctx->stream>>>(grid, partial, out);
+  CD_LAUNCHED(ctx);
+  double r2 = 0;
+  CD_CUDA(ctx, cudaMemcpyAsync(&r2, out, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  cudaFree(partial);
+  cudaFree(out);
+  if (res) *res = std::sqrt(r2);
+  return CDGPU_OK;
+}
+
+static int precondition(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *r, double *z)
+{
+  return p.precision == 1 ? mg_apply<float>(ctx, h, p, r, z) : mg_apply<double>(ctx, h, p, r, z);
+}
+
+// the host copy of the FGMRES control block: [0..k) h1, [33..33+k) h2, [66] ||w||^2
+static int read_ctl(cdgpu_ctx *ctx, Hierarchy &h, int count)
+{
+  CD_CUDA(ctx, cudaMemcpyAsync(h.h_ctl, h.d_ctl, sizeof(double) * count, cudaMemcpyDeviceToHost, ctx->stream));
+  CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CDGPU_OK;
+}
+
+// Givens helpers exactly as FgmresIte.C:149-181
+static void gen_rot(double dx, double dy, double &cs, double &sn)
+{
+  if (dy == 0.0) { cs = 1.0; sn = 0.0; }
+  else if (std::fabs(dy) > std::fabs(dx))
+  {
+    double t = dx / dy;
+    sn = 1.0 / std::sqrt(1.0 + t * t);
+    cs = t * sn;
+  }
+  else
+  {
+    double t = dy / dx;
+    cs = 1.0 / std::sqrt(1.0 + t * t);
+    sn = t * cs;
+  }
+}
+static void app_rot(double &dx, double &dy, double cs, double sn)
+{
+  double t = cs * dx + sn * dy;
+  dy = -sn * dx + cs * dy;
+  dx = t;
+}
+
+static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *f, double *x,
+                  cdgpu_solve_info *info)
+{
+  const Space &s = *h.lev.back().sp;
+  const int n = s.n_dof;
+  int m = std::min(p.restart, p.maxit);
+  if (m <= 0) m = 10;
+  if (m > 32) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "FGMRES: restart above 32 is not supported");
+  int rc;
+  if ((rc = setup_hierarchy_buffers(ctx, h, m))) return rc;
+  std::vector<double> H((size_t)(m + 1) * m, 0.0), sv(m + 1), cs(m + 1), sn(m + 1), y(m + 1);
+  const int blocks = (n + 255) / 256;
+  auto V = [&](int k) { return h.d_V + (size_t)k * n; };
+  auto Z = [&](int k) { return h.d_Z + (size_t)k * n; };
+  // r0 = f - A x, beta = ||r0|| (FgmresIte.C:275-284)
+  if ((rc = finest_defect_norm(ctx, h, x, f, V(0), h.d_ctl))) return rc;
+  if ((rc = read_ctl(ctx, h, 1))) return rc;
+  double res = std::sqrt(h.h_ctl[0]), res0 = res, beta = res;
+  info->initial_residual = res;
+  int maxite = p.maxit, ret = 0, status = CDGPU_OK;
+  if (beta <= p.res_norm_min)
+  {
+    if (p.minit == 0 || beta < 1e-20)
+    {
+      info->iterations = 0;
+      info->final_residual = res;
+      info->status = CDGPU_OK;
+      return CDGPU_OK;
+    }
+    maxite = p.minit;
+  }
+  int j = 1;
+  bool done = false;
+  while (j <= maxite && !done)
+  {
+    scale_kernel<<<blocks, 256, 0, ctx->stream>>>(n, 1.0 / beta, V(0), V(0));
+    CD_LAUNCHED(ctx);
+    std::fill(sv.begin(), sv.end(), 0.0);
+    sv[0] = beta;
+    int i;
+    for (i = 0; i < m && j <= maxite; i++, j++)
+    {
+      if ((rc = precondition(ctx, h, p, V(i), Z(i)))) return rc;
+      if ((rc = spmv64(ctx, s, Z(i), h.d_w))) return rc;
+      int k = i + 1, pb = h.partial_blocks;
+      // pass 1: h1 = V^T w
+      gs_pass_kernel<<<pb, kBlock, 0, ctx->stream>>>(n, k, h.d_V, h.d_w, nullptr, 1, h.d_partial);
+      CD_LAUNCHED(ctx);
+      reduce_partials_kernel<<<1, 64, 0, ctx->stream>>>(pb, k - 1, h.d_partial, h.d_ctl);
+      CD_LAUNCHED(ctx);
+      // pass 2: w -= V h1, h2 = V^T w
+      gs_pass_kernel<<<pb, kBlock, 0, ctx->stream>>>(n, k, h.d_V, h.d_w, h.d_ctl, 1, h.d_partial);
+      CD_LAUNCHED(ctx);
+      reduce_partials_kernel<<<1, 64, 0, ctx->stream>>>(pb, k - 1, h.d_partial, h.d_ctl + 33);
+      CD_LAUNCHED(ctx);
+      // w -= V h2, ||w||^2
+      gs_pass_kernel<<<pb, kBlock, 0, ctx->stream>>>(n, k, h.d_V, h.d_w, h.d_ctl + 33, 0, h.d_partial);
+      CD_LAUNCHED(ctx);
+      reduce_partials_kernel<<<1, 64, 0, ctx->stream>>>(pb, 0, h.d_partial, h.d_ctl + 66);
+      CD_LAUNCHED(ctx);
+      if ((rc = read_ctl(ctx, h, 67))) return rc;
+      // the slot-0 reduction of the last pass holds ||w||^2 (slot 32 of the partials)
+      for (int t = 0; t < k; t++) H[(size_t)t * m + i] = h.h_ctl[t] + h.h_ctl[33 + t];
+      double hn = std::sqrt(h.h_ctl[66]);
+      H[(size_t)(i + 1) * m + i] = hn;
+      if (hn != 0)
+      {
+        scale_kernel<<<blocks, 256, 0, ctx->stream>>>(n, 1.0 / hn, h.d_w, V(i + 1));
+        CD_LAUNCHED(ctx);
+      }
+      for (int t = 0; t < i; t++) app_rot(H[(size_t)t * m + i], H[(size_t)(t + 1) * m + i], cs[t], sn[t]);
+      gen_rot(H[(size_t)i * m + i], H[(size_t)(i + 1) * m + i], cs[i], sn[i]);
+      app_rot(H[(size_t)i * m + i], H[(size_t)(i + 1) * m + i], cs[i], sn[i]);
+      app_rot(sv[i], sv[i + 1], cs[i], sn[i]);
+      res = std::fabs(sv[i + 1]);
+      if (j >= p.minit && (res < p.res_norm_min || res < p.red_factor * res0))
+      {
+        // back substitution and x += Z y (UpdateGmresIterate, FgmresIte.C:198-216)
+        for (int a = 0; a <= i; a++) y[a] = sv[a];
+        for (int a = i; a >= 0; a--)
+        {
+          y[a] /= H[(size_t)a * m + a];
+          for (int b = a - 1; b >= 0; b--) y[b] -= H[(size_t)b * m + a] * y[a];
+        }
+        CD_CUDA(ctx, cudaMemcpyAsync(h.d_ctl + 100, y.data(), sizeof(double) * (i + 1), cudaMemcpyHostToDevice,
+                                     ctx->stream));
+        update_kernel<<<blocks, 256, 0, ctx->stream>>>(n, i + 1, h.d_ctl + 100, h.d_Z, x);
+        CD_LAUNCHED(ctx);
+        ret = j;
+        done = true;
+        break;
+      }
+      if (res > p.div_factor * res0)
+      {
+        ret = j;
+        status = CDGPU_ERR_DIVERGED;
+        done = true;
+        break;
+      }
+    }
+    if (done) break;
+    // restart: x += Z y over the full basis, new residual (FgmresIte.C:536-560)
+    for (int a = 0; a < m; a++) y[a] = sv[a];
+    for (int a = m - 1; a >= 0; a--)
+    {
+      y[a] /= H[(size_t)a * m + a];
+      for (int b = a - 1; b >= 0; b--) y[b] -= H[(size_t)b * m + a] * y[a];
+    }
+    CD_CUDA(ctx, cudaMemcpyAsync(h.d_ctl + 100, y.data(), sizeof(double) * m, cudaMemcpyHostToDevice, ctx->stream));
+    update_kernel<<<blocks, 256, 0, ctx->stream>>>(n, m, h.d_ctl + 100, h.d_Z, x);
+    CD_LAUNCHED(ctx);
+    if ((rc = finest_defect_norm(ctx, h, x, f, V(0), h.d_ctl))) return rc;
+    if ((rc = read_ctl(ctx, h, 1))) return rc;
+    res = res0 = beta = std::sqrt(h.h_ctl[0]);
+  }
+  if (!done)
+  {
+    ret = j > maxite ? maxite : j;
+    if (res > p.res_norm_min && res > res0 * p.red_factor) status = CDGPU_ERR_NOT_CONVERGED;
+  }
+  CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  info->iterations = ret;
+  info->final_residual = res;
+  info->status = status;
+  return CDGPU_OK;
+}
+
+static int fixed_point(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *f,
+                       double *x, cdgpu_solve_info *info)
+{
+  const Space &s = *h.lev.back().sp;
+  const int n = s.n_dof;
+  int rc;
+  if ((rc = setup_hierarchy_buffers(ctx, h, std::max(h.m, 1)))) return rc;
+  double *d = h.d_w, *z = h.d_V;
+  if ((rc = finest_defect_norm(ctx, h, x, f, d, h.d_ctl))) return rc;
+  if ((rc = read_ctl(ctx, h, 1))) return rc;
+  double res = std::sqrt(h.h_ctl[0]), res0 = res;
+  info->initial_residual = res;
+  int maxite = p.maxit, i, status = CDGPU_OK;
+  if (res <= p.res_norm_min) maxite = p.minit;
+  for (i = 1; i <= maxite; i++)
+  {
+    if ((rc = precondition(ctx, h, p, d, z))) return rc;
+    axpy_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, 1.0, z, x);
+    CD_LAUNCHED(ctx);
+    if ((rc = finest_defect_norm(ctx, h, x, f, d, h.d_ctl))) return rc;
+    if ((rc = read_ctl(ctx, h, 1))) return rc;
+    res = std::sqrt(h.h_ctl[0]);
+    if (i < p.minit) continue;
+    if (res <= res0 * p.red_factor) break;
+    if (res <= p.res_norm_min) break;
+    if (res > p.div_factor * res0) { status = CDGPU_ERR_DIVERGED; break; }
+  }
+  if (i > maxite && res > p.res_norm_min && res > res0 * p.red_factor) status = CDGPU_ERR_NOT_CONVERGED;
+  info->iterations = i;
+  info->final_residual = res;
+  info->status = status;
+  return CDGPU_OK;
+}
+
+int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *d_rhs, double *d_sol,
+              cdgpu_solve_info *info)
+{
+  for (auto &L : h.lev)
+    if (!L.sp->assembled) return fail(ctx, CDGPU_ERR_INVALID, "solve: every level must be assembled");
+  if (p.smoother != 1) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "solve: only the damped Jacobi smoother (1) runs on the GPU");
+  if (p.slc) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "solve: step-length control is not supported on the GPU");
+  if (p.coarse_smoother != 1 && p.coarse_smoother != 2 && p.coarse_smoother != 3 && p.coarse_smoother != 17)
+    return fail(ctx, CDGPU_ERR_UNSUPPORTED, "solve: coarse smoother must be 1, 2, 3 or 17");
+  if (p.precision != 0 && p.precision != 1) return fail(ctx, CDGPU_ERR_INVALID, "solve: precision must be 0 or 1");
+  if (p.coarse_smoother != 17 && h.lev[0].sp->n_dof > 6000)
+    return fail(ctx, CDGPU_ERR_UNSUPPORTED, "solve: coarse smoother loop needs a coarsest level below 6000 DOFs");
+  int rc;
+  if (p.coarse_smoother == 17 && (rc = refresh_coarse_inverse(ctx, h))) return rc;
+  cdgpu_solve_info local{};
+  if (!info) info = &local;
+  if (p.solver == 11) rc = fixed_point(ctx, h, p, d_rhs, d_sol, info);
+  else if (p.solver == 16) rc = fgmres(ctx, h, p, d_rhs, d_sol, info);
+  else return fail(ctx, CDGPU_ERR_UNSUPPORTED, "solve: SC_SOLVER_SCALAR must be 16 (FGMRES) or 11 (fixed point)");
+  return rc;
+}

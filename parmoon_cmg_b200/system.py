@@ -1,0 +1,247 @@
+"""Host-side mirror of ParMooN's convection-diffusion facade over libcdgpu.
+
+``TSystemCD3D`` and ``TSystemCD2D`` keep the reference's call surface
+(src/System/SystemCD3D.C:36-396, src/System/SystemCD2D.C:39-205):
+construct with the FE spaces of all multigrid levels, ``Init`` with the
+coefficients and boundary data, ``Assemble``, ``Solve(sol, rhs)``.  All work
+runs in libcdgpu through its C ABI; this module only marshals numpy arrays.
+Errors raise :class:`CdgpuError` where the reference prints a message and
+calls ``exit(4711)``.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import CdgpuError, Coeffs, SolveInfo, SolverParams
+
+GALERKIN, SUPG = _lib.GALERKIN, _lib.SUPG
+GMG = 1  # SOLVER_TYPE, 3DPrograms/CD3D_ParMooN.C:33
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Context:
+    """One libcdgpu context (device + CUDA stream)."""
+
+    def __init__(self, device=0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        st = self.lib.cdgpu_create(C.byref(h), device)
+        if st != 0:
+            raise CdgpuError(st, self.lib.cdgpu_status_string(st).decode())
+        self.h = h
+
+    def check(self, st):
+        if st != 0:
+            msg = self.lib.cdgpu_last_error(self.h).decode()
+            raise CdgpuError(st, f"{self.lib.cdgpu_status_string(st).decode()}: {msg}")
+
+    @property
+    def stream(self):
+        return int(self.lib.cdgpu_stream(self.h))
+
+    @property
+    def kernel_launches(self):
+        return int(self.lib.cdgpu_kernel_launches(self.h))
+
+    def close(self):
+        if self.h:
+            self.lib.cdgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- thin wrappers of the C ABI -------------------------------------
+    def upload_space(self, sp):
+        sid = C.c_int()
+        coords, gn, bi = _f64(sp["coords"]), _i32(sp["global_numbers"]), _i32(sp["begin_index"])
+        self.check(self.lib.cdgpu_upload_space(
+            self.h, sp["dim"], sp["order"], len(bi) - 1, _p(coords), _p(gn), _p(bi),
+            int(sp["n_dof"]), int(sp["n_active"]), int(sp.get("hanging_bound", sp["n_active"])),
+            C.byref(sid)))
+        return sid.value
+
+    def build_pattern(self, sid):
+        nnz = C.c_int()
+        self.check(self.lib.cdgpu_build_pattern(self.h, sid, C.byref(nnz)))
+        return nnz.value
+
+    def upload_pattern(self, sid, row_ptr, kcol):
+        row_ptr, kcol = _i32(row_ptr), _i32(kcol)
+        self.check(self.lib.cdgpu_upload_pattern(self.h, sid, _p(row_ptr), _p(kcol), len(kcol)))
+
+    def get_pattern(self, sid, n_dof, nnz):
+        rp = np.zeros(n_dof + 1, np.int32)
+        kc = np.zeros(nnz, np.int32)
+        self.check(self.lib.cdgpu_get_pattern(self.h, sid, _p(rp), _p(kc)))
+        return rp, kc
+
+    def set_coeffs(self, sid, coeffs, table=None):
+        tab = _f64(table) if table is not None else None
+        self.check(self.lib.cdgpu_set_coeffs(self.h, sid, C.byref(coeffs), _p(tab)))
+
+    def quadrature_points(self, sid, n_cells, dim):
+        nq = C.c_int()
+        self.check(self.lib.cdgpu_quadrature_points(self.h, sid, None, C.byref(nq)))
+        out = np.zeros((n_cells, nq.value, dim))
+        self.check(self.lib.cdgpu_quadrature_points(self.h, sid, _p(out), C.byref(nq)))
+        return out
+
+    def assemble(self, sid, disctype, n_dof, nnz, dirichlet=None, want_entries=True, want_rhs=True):
+        ent = np.zeros(nnz) if want_entries else None
+        rhs = np.zeros(n_dof) if want_rhs else None
+        d = _f64(dirichlet) if dirichlet is not None else None
+        self.check(self.lib.cdgpu_assemble(self.h, sid, disctype, _p(d), _p(ent), _p(rhs)))
+        return ent, rhs
+
+    def add_neumann(self, sid, cells, edges, g, n_dof=None):
+        """Add Neumann data; returns the updated right-hand side when n_dof is given."""
+        cells, edges, g = _i32(cells), _i32(edges), _f64(g)
+        rhs = np.zeros(n_dof) if n_dof is not None else None
+        self.check(self.lib.cdgpu_add_neumann(self.h, sid, len(cells), _p(cells), _p(edges), _p(g),
+                                              _p(rhs)))
+        return rhs
+
+    def spmv(self, sid, x):
+        x = _f64(x)
+        y = np.zeros_like(x)
+        self.check(self.lib.cdgpu_spmv(self.h, sid, _p(x), _p(y)))
+        return y
+
+    def defect(self, sid, x, f):
+        x, f = _f64(x), _f64(f)
+        d = np.zeros_like(x)
+        res = C.c_double()
+        self.check(self.lib.cdgpu_defect(self.h, sid, _p(x), _p(f), _p(d), C.byref(res)))
+        return d, res.value
+
+    def hierarchy(self, sids, parents):
+        L = len(sids)
+        ids = (C.c_int * L)(*sids)
+        keep = [_i32(p) if p is not None else None for p in parents]
+        ptrs = (C.c_void_p * L)(*[(a.ctypes.data if a is not None else None) for a in keep])
+        mg = C.c_int()
+        self.check(self.lib.cdgpu_hierarchy(self.h, L, C.cast(ids, C.c_void_p),
+                                            C.cast(ptrs, C.c_void_p), C.byref(mg)))
+        return mg.value
+
+    def assemble_hierarchy(self, mg, disctype):
+        self.check(self.lib.cdgpu_assemble_hierarchy(self.h, mg, disctype))
+
+    def solve(self, mg, params, rhs, sol):
+        rhs = _f64(rhs)
+        sol = _f64(sol).copy()
+        info = SolveInfo()
+        self.check(self.lib.cdgpu_solve(self.h, mg, C.byref(params), _p(rhs), _p(sol), C.byref(info)))
+        return sol, info
+
+    def solve_device(self, mg, params, d_rhs, d_sol):
+        info = SolveInfo()
+        self.check(self.lib.cdgpu_solve_device(self.h, mg, C.byref(params), C.c_void_p(d_rhs),
+                                               C.c_void_p(d_sol), C.byref(info)))
+        return info
+
+    def rhs_device(self, sid):
+        p = C.c_void_p()
+        self.check(self.lib.cdgpu_rhs_device(self.h, sid, C.byref(p)))
+        return p.value
+
+
+def coeffs(kind=_lib.COEFF_CONSTANT, eps=1.0, b=(0.0, 0.0, 0.0), c=0.0, f=1.0, delta0=1.0,
+           poly_degree=1):
+    b = tuple(b) + (0.0,) * (3 - len(b))
+    return Coeffs(kind=kind, poly_degree=poly_degree, eps=eps, b1=b[0], b2=b[1], b3=b[2], c=c,
+                  f=f, delta0=delta0)
+
+
+def solver_params(**kw):
+    """ParamDB-style solver settings; defaults are the multigrid configs' (FGMRES(30),
+    V(2,2) damped Jacobi with omega 0.8, relative residual 1e-10, FP64 everywhere) with the
+    exact FP64 coarse solve."""
+    d = dict(solver=16, restart=30, maxit=1000, minit=0, smoother=1, coarse_smoother=17, pre=2,
+             post=2, coarse_maxit=10, cycle=1, slc=0, precision=0, red_factor=1e-10,
+             res_norm_min=0.0, div_factor=1e10, omega=0.8, coarse_red=0.1, gmg_damp=1.0)
+    d.update(kw)
+    return SolverParams(**d)
+
+
+class TSystemCD3D:
+    """Mirror of TSystemCD3D (include/System/SystemCD3D.h:97-110) on the GPU.
+
+    fespaces: spaces of all multigrid levels, coarsest first (dicts as produced by
+    :func:`parmoon_cmg_b200.mesh.structured_space` or by the reference's TFESpace3D);
+    parents[l]: parent cell map of level l (index 0 unused)."""
+
+    dim = 3
+
+    def __init__(self, fespaces, parents, disctype=GALERKIN, solver=GMG, ctx=None, pattern=None):
+        if solver != GMG:
+            raise CdgpuError(_lib.ERR_UNSUPPORTED, "only the GMG solver type runs on the GPU")
+        self.ctx = ctx or Context()
+        self.spaces = fespaces
+        self.disctype = disctype
+        self.sids = [self.ctx.upload_space(s) for s in fespaces]
+        self.nnz = []
+        for i, sid in enumerate(self.sids):
+            if pattern is not None and pattern[i] is not None:
+                self.ctx.upload_pattern(sid, *pattern[i])
+                self.nnz.append(len(pattern[i][1]))
+            else:
+                self.nnz.append(self.ctx.build_pattern(sid))
+        self.mg = self.ctx.hierarchy(self.sids, parents)
+        self.N_DOF = int(fespaces[-1]["n_dof"])
+        self.N_Active = int(fespaces[-1]["n_active"])
+
+    def Init(self, coeff, table=None):
+        for i, sid in enumerate(self.sids):
+            self.ctx.set_coeffs(sid, coeff, table[i] if table is not None else None)
+
+    def Assemble(self, sol=None, rhs=None, dirichlet=None, entries=False):
+        """Assemble all levels (SystemCD3D.C:314-339); returns the finest (entries, rhs) and
+        copies the Dirichlet part of rhs into sol like SystemCD3D.C:330."""
+        out = None
+        for i, sid in enumerate(self.sids):
+            sp = self.spaces[i]
+            last = i == len(self.sids) - 1
+            d = dirichlet if last else None
+            ent, r = self.ctx.assemble(sid, self.disctype, int(sp["n_dof"]), self.nnz[i], d,
+                                       want_entries=entries and last, want_rhs=last)
+            if last:
+                out = (ent, r)
+        if rhs is not None:
+            rhs[:] = out[1]
+        if sol is not None:
+            sol[self.N_Active:] = out[1][self.N_Active:]
+        return out
+
+    def Solve(self, sol, rhs, params=None):
+        """FGMRES / fixed point with one multigrid cycle as preconditioner (SystemCD3D.C:342-368)."""
+        params = params or solver_params()
+        x, info = self.ctx.solve(self.mg, params, rhs, sol)
+        sol[:] = x
+        if info.status == _lib.ERR_DIVERGED:
+            raise CdgpuError(info.status, "fgmres iteration diverges")
+        return info
+
+
+class TSystemCD2D(TSystemCD3D):
+    """2D counterpart.  The reference's TSystemCD2D takes one space and has no multigrid
+    branch (src/System/SystemCD2D.C:191-193); here it takes every level's space and
+    solves with the same multigrid-preconditioned FGMRES as the 3D system."""
+
+    dim = 2
