@@ -70,6 +70,10 @@ typedef struct cdgpu_solver_params
   int cycle;           /* SC_MG_CYCLE_SCALAR: 1 V, 2 W, 0 F */
   int slc;             /* SC_STEP_LENGTH_CONTROL_ALL_SCALAR (must be 0 on the GPU) */
   int precision;       /* 0: FP64 multigrid (drop-in); 1: FP32 multigrid inside FP64 FGMRES */
+  int stop_rule;       /* 0: the reference's rule, red_factor relative to the residual at the last
+                          restart (FgmresIte.C:430-431, 557); 1: red_factor relative to the initial
+                          residual of the solve (no counterpart in the reference) */
+  int pad_;
   double red_factor;   /* SC_LIN_RED_FACTOR_SCALAR */
   double res_norm_min; /* SC_LIN_RES_NORM_MIN_SCALAR */
   double div_factor;   /* SC_DIV_FACTOR */
@@ -181,9 +185,11 @@ int cdgpu_solve(cdgpu_ctx *ctx, int mg_id, const cdgpu_solver_params *params, co
 /* same with device vectors (length n_dof of the finest level) */
 int cdgpu_solve_device(cdgpu_ctx *ctx, int mg_id, const cdgpu_solver_params *params,
                        const double *d_rhs, double *d_sol, cdgpu_solve_info *info);
-/* assemble every level of a hierarchy (TSystemCD3D::Assemble loops over all levels) and
- * copy the finest right-hand side's Dirichlet part into d_sol like SystemCD3D.C:330 */
-int cdgpu_assemble_hierarchy(cdgpu_ctx *ctx, int mg_id, int disctype);
+/* assemble every level of a hierarchy, as TSystemCD3D::Assemble loops over all levels
+ * (src/System/SystemCD3D.C:314-339).  disctype is used on the finest level,
+ * coarse_disctype on the others (the reference uses one DISCTYPE for all levels; a SUPG
+ * coarse-grid operator under a Galerkin fine level only changes the preconditioner). */
+int cdgpu_assemble_hierarchy(cdgpu_ctx *ctx, int mg_id, int disctype, int coarse_disctype);
 /* device pointer of the assembled right-hand side of a space */
 int cdgpu_rhs_device(cdgpu_ctx *ctx, int space_id, double **d_rhs);
 

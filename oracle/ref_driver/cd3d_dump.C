@@ -22,6 +22,8 @@
 #include <MainUtilities.h>
 #include <LinAlg.h>
 #include <ItMethod.h>
+#include <FgmresIte.h>
+#include <FixedPointIte.h>
 
 #include <string.h>
 #include <math.h>
@@ -82,13 +84,24 @@ class DumpSystemCD3D : public TSystemCD3D
   }
   // one application of the multigrid preconditioner (TMultiGridScaIte::Iterate)
   void ApplyPrec(double *z, double *r) { prec->Iterate(sqmatrices, NULL, z, r); }
+  // re-create the Krylov method after ParamDB changes, with the constructor calls of
+  // src/System/SystemCD3D.C:180-199 (the method reads its tolerances when constructed)
+  void RebuildKrylov()
+  {
+    delete Itmethod;
+    if (TDatabase::ParamDB->SC_SOLVER_SCALAR == 11)
+      Itmethod = new TFixedPointIte(MatVect_Scalar, Defect_Scalar, prec, 0, N_DOF, 1);
+    else
+      Itmethod = new TFgmresIte(MatVect_Scalar, Defect_Scalar, prec, 0, N_DOF, 1);
+  }
 };
 
 int main(int argc, char *argv[])
 {
   if (argc < 9)
   {
-    fprintf(stderr, "usage: %s file.dat outdir|- eps b1 b2 b3 c f [prolong_max_ndof]\n", argv[0]);
+    fprintf(stderr, "usage: %s file.dat outdir|- eps b1 b2 b3 c f [prolong_max_ndof [rtol_initial]]\n",
+            argv[0]);
     return 2;
   }
   TDatabase *Database = new TDatabase();
@@ -98,6 +111,7 @@ int main(int argc, char *argv[])
   C_eps = atof(argv[3]); C_b1 = atof(argv[4]); C_b2 = atof(argv[5]); C_b3 = atof(argv[6]);
   C_c = atof(argv[7]); C_f = atof(argv[8]);
   long prolong_max = argc > 9 ? atol(argv[9]) : 0;
+  double rtol_initial = argc > 10 ? atof(argv[10]) : 0.0; // > 0: stop relative to the initial residual
   dump_open(outdir);
 
   if (TDatabase::ParamDB->PROBLEM_TYPE == 0) TDatabase::ParamDB->PROBLEM_TYPE = 1;
@@ -226,6 +240,18 @@ int main(int argc, char *argv[])
   if (TDatabase::ParamDB->SOLVER_TYPE == 1)
   {
     t0 = wall_now();
+    if (rtol_initial > 0)
+    {
+      // stop at ||r|| <= rtol * ||r0||: the absolute SC_LIN_RES_NORM_MIN_SCALAR set from the
+      // initial residual (ScalarDefect, src/FE/Blas2.C:11), relative test switched off
+      std::vector<double> d(nf);
+      double r0 = 0;
+      ScalarDefect(S->A(LEVELS - 1), Sol[LEVELS - 1], Rhs[LEVELS - 1], d.data(), r0);
+      TDatabase::ParamDB->SC_LIN_RES_NORM_MIN_SCALAR = rtol_initial * r0;
+      TDatabase::ParamDB->SC_LIN_RED_FACTOR_SCALAR = 0.0;
+      S->RebuildKrylov();
+      meta_d("initial_residual", r0);
+    }
     its = S->SolveCount(Sol[LEVELS - 1], Rhs[LEVELS - 1]);
     t_solve = wall_now() - t0;
     dump_f64("solution", Sol[LEVELS - 1], nf);

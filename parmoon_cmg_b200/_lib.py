@@ -34,7 +34,7 @@ class SolverParams(C.Structure):
                 ("minit", C.c_int), ("smoother", C.c_int), ("coarse_smoother", C.c_int),
                 ("pre", C.c_int), ("post", C.c_int), ("coarse_maxit", C.c_int),
                 ("cycle", C.c_int), ("slc", C.c_int), ("precision", C.c_int),
-                ("red_factor", C.c_double), ("res_norm_min", C.c_double),
+                ("stop_rule", C.c_int), ("pad_", C.c_int), ("red_factor", C.c_double), ("res_norm_min", C.c_double),
                 ("div_factor", C.c_double), ("omega", C.c_double), ("coarse_red", C.c_double),
                 ("gmg_damp", C.c_double)]
 
@@ -68,7 +68,7 @@ SIGNATURES = {
     "cdgpu_hierarchy": (_I, [_P, _I, _P, _P, C.POINTER(_I)]),
     "cdgpu_solve": (_I, [_P, _I, C.POINTER(SolverParams), _P, _P, C.POINTER(SolveInfo)]),
     "cdgpu_solve_device": (_I, [_P, _I, C.POINTER(SolverParams), _P, _P, C.POINTER(SolveInfo)]),
-    "cdgpu_assemble_hierarchy": (_I, [_P, _I, _I]),
+    "cdgpu_assemble_hierarchy": (_I, [_P, _I, _I, _I]),
     "cdgpu_rhs_device": (_I, [_P, _I, C.POINTER(C.c_void_p)]),
 }
 

@@ -51,7 +51,7 @@ static void free_mg(Hierarchy *h)
     for (void *p : ptrs)
       if (p) cudaFree(p);
   }
-  void *ptrs[] = {h->d_cinv, h->d_V, h->d_Z, h->d_w, h->d_ctl, h->d_partial, h->d_x, h->d_b};
+  void *ptrs[] = {h->d_cinv, h->d_cpiv, h->d_V, h->d_Z, h->d_w, h->d_ctl, h->d_partial, h->d_x, h->d_b};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -461,14 +461,15 @@ int cdgpu_hierarchy(cdgpu_ctx *ctx, int n_levels, const int *space_ids, const in
   return CDGPU_OK;
 }
 
-int cdgpu_assemble_hierarchy(cdgpu_ctx *ctx, int mg_id, int disctype)
+int cdgpu_assemble_hierarchy(cdgpu_ctx *ctx, int mg_id, int disctype, int coarse_disctype)
 {
   Hierarchy *h = get_mg(ctx, mg_id);
   if (!h) return fail(ctx, CDGPU_ERR_INVALID, "assemble_hierarchy: bad id");
   cudaSetDevice(ctx->device);
-  for (auto &L : h->lev)
+  for (size_t l = 0; l < h->lev.size(); l++)
   {
-    int rc = assemble_space(ctx, *L.sp, disctype, nullptr);
+    int d = l + 1 == h->lev.size() ? disctype : coarse_disctype;
+    int rc = assemble_space(ctx, *h->lev[l].sp, d, nullptr);
     if (rc) return rc;
   }
   return CDGPU_OK;

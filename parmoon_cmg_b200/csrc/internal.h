@@ -91,6 +91,7 @@ struct Hierarchy
 {
   std::vector<Level> lev;
   double *d_cinv = nullptr; // explicit inverse of the coarsest matrix (exact coarse solve)
+  int *d_cpiv = nullptr;    // pivots of its Gauss-Jordan inversion + error flag
   long cinv_version = -1;
   // FGMRES workspace
   int m = 0;

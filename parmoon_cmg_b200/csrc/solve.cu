@@ -662,21 +662,129 @@ int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m)
   return CDGPU_OK;
 }
 
+__global__ void csr_to_dense_kernel(int n, const int *__restrict__ rp, const int *__restrict__ kc,
+                                    const double *__restrict__ a, double *__restrict__ dense)
+{
+  int r = blockIdx.x;
+  for (int c = threadIdx.x; c < n; c += blockDim.x) dense[(size_t)r * n + c] = 0.0;
+  __syncthreads();
+  for (int j = rp[r] + threadIdx.x; j < rp[r + 1]; j += blockDim.x) dense[(size_t)r * n + kc[j]] = a[j];
+}
+
+// In-place Gauss-Jordan inversion with partial (row) pivoting, one CTA; the matrix lives in
+// shared memory when it fits, otherwise in the global buffer itself.  flag[0] = 1 when a
+// zero pivot is met.
+__global__ void __launch_bounds__(1024) gj_invert_kernel(int n, double *__restrict__ g, int use_smem,
+                                                         int *__restrict__ piv, int *__restrict__ flag)
+{
+  extern __shared__ double sm[];
+  double *A = use_smem ? sm : g;
+  __shared__ double red_v[32];
+  __shared__ int red_i[32];
+  __shared__ int p_s;
+  const int nt = blockDim.x, t = threadIdx.x, lane = t % 32, warp = t / 32;
+  if (use_smem)
+    for (int i = t; i < n * n; i += nt) A[i] = g[i];
+  __syncthreads();
+  for (int k = 0; k < n; k++)
+  {
+    // pivot search in column k, rows k..n-1 (largest magnitude, lowest row on ties)
+    double bv = -1.0;
+    int bi = n;
+    for (int i = k + t; i < n; i += nt)
+    {
+      double v = fabs(A[(size_t)i * n + k]);
+      if (v > bv || (v == bv && i < bi)) { bv = v; bi = i; }
+    }
+    for (int o = 16; o > 0; o >>= 1)
+    {
+      double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
+    __syncthreads();
+    if (t == 0)
+    {
+      double v = -1.0;
+      int p = n;
+      for (int w = 0; w < nt / 32; w++)
+        if (red_v[w] > v || (red_v[w] == v && red_i[w] < p)) { v = red_v[w]; p = red_i[w]; }
+      p_s = p;
+      piv[k] = p;
+      if (!(v > 0.0)) flag[0] = 1;
+    }
+    __syncthreads();
+    const int p = p_s;
+    if (p != k)
+      for (int j = t; j < n; j += nt)
+      {
+        double tmp = A[(size_t)k * n + j];
+        A[(size_t)k * n + j] = A[(size_t)p * n + j];
+        A[(size_t)p * n + j] = tmp;
+      }
+    __syncthreads();
+    const double pivot = A[(size_t)k * n + k];
+    __syncthreads();
+    for (int j = t; j < n; j += nt)
+      A[(size_t)k * n + j] = (j == k ? 1.0 : A[(size_t)k * n + j]) / pivot;
+    __syncthreads();
+    // eliminate column k from the other rows: first every column but k (which holds the
+    // multipliers), then column k itself
+    for (int e = t; e < n * n; e += nt)
+    {
+      int i = e / n, j = e % n;
+      if (i == k || j == k) continue;
+      double f = A[(size_t)i * n + k];
+      if (f != 0.0) A[(size_t)i * n + j] -= f * A[(size_t)k * n + j];
+    }
+    __syncthreads();
+    for (int i = t; i < n; i += nt)
+      if (i != k) A[(size_t)i * n + k] = -A[(size_t)i * n + k] * A[(size_t)k * n + k];
+    __syncthreads();
+  }
+  // undo the row interchanges as column interchanges, last first
+  for (int k = n - 1; k >= 0; k--)
+  {
+    int p = piv[k];
+    if (p != k)
+      for (int i = t; i < n; i += nt)
+      {
+        double tmp = A[(size_t)i * n + k];
+        A[(size_t)i * n + k] = A[(size_t)i * n + p];
+        A[(size_t)i * n + p] = tmp;
+      }
+    __syncthreads();
+  }
+  if (use_smem)
+    for (int i = t; i < n * n; i += nt) g[i] = A[i];
+}
+
 static int refresh_coarse_inverse(cdgpu_ctx *ctx, Hierarchy &h)
 {
   Space &s = *h.lev[0].sp;
   if (h.d_cinv && h.cinv_version == s.assembly_version) return CDGPU_OK;
   int n = s.n_dof;
   if (n > 4096) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "exact coarse solve: coarsest level larger than 4096 DOFs");
-  std::vector<double> a((size_t)s.nnz), dense((size_t)n * n, 0.0);
-  CD_CUDA(ctx, cudaMemcpyAsync(a.data(), s.d_a, sizeof(double) * s.nnz, cudaMemcpyDeviceToHost, ctx->stream));
-  CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  for (int r = 0; r < n; r++)
-    for (int j = s.h_row_ptr[r]; j < s.h_row_ptr[r + 1]; j++) dense[(size_t)r * n + s.h_kcol[j]] = a[j];
-  if (!dense_inverse(n, dense)) return fail(ctx, CDGPU_ERR_INVALID, "exact coarse solve: singular coarse matrix");
   int rc;
-  if ((rc = dev_alloc(ctx, &h.d_cinv, dense.size()))) return rc;
-  CD_CUDA(ctx, cudaMemcpy(h.d_cinv, dense.data(), dense.size() * sizeof(double), cudaMemcpyHostToDevice));
+  if (h.cinv_version < 0 || !h.d_cinv)
+  {
+    if ((rc = dev_alloc(ctx, &h.d_cinv, (size_t)n * n)) || (rc = dev_alloc(ctx, &h.d_cpiv, n + 1)))
+      return rc;
+  }
+  csr_to_dense_kernel<<<n, 128, 0, ctx->stream>>>(n, s.d_row_ptr, s.d_kcol, s.d_a, h.d_cinv);
+  CD_LAUNCHED(ctx);
+  size_t sm = sizeof(double) * (size_t)n * n;
+  int use_smem = sm <= 200 * 1024;
+  if (use_smem)
+    CD_CUDA(ctx, cudaFuncSetAttribute(gj_invert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  CD_CUDA(ctx, cudaMemsetAsync(h.d_cpiv + n, 0, sizeof(int), ctx->stream));
+  gj_invert_kernel<<<1, 1024, use_smem ? sm : 0, ctx->stream>>>(n, h.d_cinv, use_smem, h.d_cpiv, h.d_cpiv + n);
+  CD_LAUNCHED(ctx);
+  int flag = 0;
+  CD_CUDA(ctx, cudaMemcpyAsync(&flag, h.d_cpiv + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (flag) return fail(ctx, CDGPU_ERR_INVALID, "exact coarse solve: singular coarse matrix");
   h.cinv_version = s.assembly_version;
   return CDGPU_OK;
 }
@@ -889,7 +997,8 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
     CD_LAUNCHED(ctx);
     if ((rc = finest_defect_norm(ctx, h, x, f, V(0), h.d_ctl))) return rc;
     if ((rc = read_ctl(ctx, h, 1))) return rc;
-    res = res0 = beta = std::sqrt(h.h_ctl[0]);
+    res = beta = std::sqrt(h.h_ctl[0]);
+    if (p.stop_rule == 0) res0 = res; // the reference measures the next cycle against this residual
   }
   if (!done)
   {

@@ -140,8 +140,9 @@ class Context:
                                             C.cast(ptrs, C.c_void_p), C.byref(mg)))
         return mg.value
 
-    def assemble_hierarchy(self, mg, disctype):
-        self.check(self.lib.cdgpu_assemble_hierarchy(self.h, mg, disctype))
+    def assemble_hierarchy(self, mg, disctype, coarse_disctype=None):
+        cd = disctype if coarse_disctype is None else coarse_disctype
+        self.check(self.lib.cdgpu_assemble_hierarchy(self.h, mg, disctype, cd))
 
     def solve(self, mg, params, rhs, sol):
         rhs = _f64(rhs)
@@ -174,7 +175,7 @@ def solver_params(**kw):
     V(2,2) damped Jacobi with omega 0.8, relative residual 1e-10, FP64 everywhere) with the
     exact FP64 coarse solve."""
     d = dict(solver=16, restart=30, maxit=1000, minit=0, smoother=1, coarse_smoother=17, pre=2,
-             post=2, coarse_maxit=10, cycle=1, slc=0, precision=0, red_factor=1e-10,
+             post=2, coarse_maxit=10, cycle=1, slc=0, precision=0, stop_rule=0, red_factor=1e-10,
              res_norm_min=0.0, div_factor=1e10, omega=0.8, coarse_red=0.1, gmg_damp=1.0)
     d.update(kw)
     return SolverParams(**d)
@@ -189,12 +190,15 @@ class TSystemCD3D:
 
     dim = 3
 
-    def __init__(self, fespaces, parents, disctype=GALERKIN, solver=GMG, ctx=None, pattern=None):
+    def __init__(self, fespaces, parents, disctype=GALERKIN, solver=GMG, ctx=None, pattern=None,
+                 coarse_disctype=None):
         if solver != GMG:
             raise CdgpuError(_lib.ERR_UNSUPPORTED, "only the GMG solver type runs on the GPU")
         self.ctx = ctx or Context()
         self.spaces = fespaces
         self.disctype = disctype
+        # discretisation of the coarse multigrid levels (the reference uses disctype everywhere)
+        self.coarse_disctype = disctype if coarse_disctype is None else coarse_disctype
         self.sids = [self.ctx.upload_space(s) for s in fespaces]
         self.nnz = []
         for i, sid in enumerate(self.sids):
@@ -219,7 +223,8 @@ class TSystemCD3D:
             sp = self.spaces[i]
             last = i == len(self.sids) - 1
             d = dirichlet if last else None
-            ent, r = self.ctx.assemble(sid, self.disctype, int(sp["n_dof"]), self.nnz[i], d,
+            disc = self.disctype if last else self.coarse_disctype
+            ent, r = self.ctx.assemble(sid, disc, int(sp["n_dof"]), self.nnz[i], d,
                                        want_entries=entries and last, want_rhs=last)
             if last:
                 out = (ent, r)
