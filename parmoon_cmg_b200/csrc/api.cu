@@ -46,15 +46,19 @@ static void free_mg(Hierarchy *h)
   for (auto &L : h->lev)
   {
     void *ptrs[] = {L.d_p_row, L.d_p_col, L.d_r_row, L.d_r_col, L.d_p_val, L.d_r_val, L.d_p_val32,
-                    L.d_r_val32, L.v64.sol, L.v64.alt, L.v64.rhs, L.v64.def, L.v32.sol, L.v32.alt,
-                    L.v32.rhs, L.v32.def};
+                    L.d_r_val32, L.c64.sol, L.c64.alt, L.c64.rhs, L.c64.def, L.c32.sol, L.c32.alt,
+                    L.c32.rhs, L.c32.def};
     for (void *p : ptrs)
       if (p) cudaFree(p);
   }
-  void *ptrs[] = {h->d_cinv, h->d_cpiv, h->d_V, h->d_Z, h->d_w, h->d_ctl, h->d_partial, h->d_x, h->d_b};
+  for (auto &g : h->gexec)
+    if (g) cudaGraphExecDestroy(g);
+  void *ptrs[] = {h->d_cinv, h->d_cpiv, h->d_V, h->d_Z, h->d_w, h->d_ctl, h->d_partial, h->d_x, h->d_b,
+                  h->d_io};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
+  if (h->h_io) cudaFreeHost(h->h_io);
   delete h;
 }
 

@@ -83,8 +83,8 @@ struct Level
   double *d_p_val = nullptr, *d_r_val = nullptr;
   float *d_p_val32 = nullptr, *d_r_val32 = nullptr;
   long p_nnz = 0;
-  LevelVec<double> v64;
-  LevelVec<float> v32;
+  LevelVec<double> v64, c64; // working pointers (ping-pong swapped) and their initial assignment
+  LevelVec<float> v32, c32;
 };
 
 struct Hierarchy
@@ -99,6 +99,13 @@ struct Hierarchy
   double *h_ctl = nullptr; // pinned mirror of the control block
   int partial_blocks = 0;
   double *d_x = nullptr, *d_b = nullptr; // host-API staging vectors
+  // captured multigrid cycle per precision (0 FP64, 1 FP32) and its in/out pointer slot
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  cdgpu_solver_params gparams[2] = {};
+  long long graph_nodes[2] = {0, 0};
+  double **d_io = nullptr;
+  double **h_io = nullptr; // pinned ring of 64 (in, out) pairs
+  unsigned io_slot = 0;
 };
 
 // ---------------------------------------------------------------------------

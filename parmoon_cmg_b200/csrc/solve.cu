@@ -31,7 +31,10 @@ namespace cg = cooperative_groups;
 static const int kBlock = 256;
 
 // ---------------------------------------------------------------------------
-// CSR kernels: one group of GS threads per row, grid-stride over rows
+// CSR kernels: one group of GS threads per row.  Rows are visited warp by warp: every
+// lane of a warp runs the same number of loop trips and reaches every shuffle, so the
+// full-warp shuffles of group_sum always see all 32 lanes (a group whose row is out of
+// range or needs no reduction contributes zeros).
 // ---------------------------------------------------------------------------
 template <int GS, typename T> __device__ __forceinline__ T group_sum(T v)
 {
@@ -40,21 +43,26 @@ template <int GS, typename T> __device__ __forceinline__ T group_sum(T v)
   return v;
 }
 
+#define CD_WARP_ROWS(n)                                                                      \
+  const int lane = threadIdx.x % GS, sub = (threadIdx.x % 32) / GS;                          \
+  const long nwarp = (long)gridDim.x * blockDim.x / 32;                                      \
+  for (long base = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32 * (32 / GS); base < (n); \
+       base += nwarp * (32 / GS))
+
 template <typename T, int GS>
 __global__ void __launch_bounds__(kBlock) spmv_kernel(int n, const int *__restrict__ rp,
                                                       const int *__restrict__ kc,
                                                       const T *__restrict__ a,
                                                       const T *__restrict__ x, T *__restrict__ y)
 {
-  const int lane = threadIdx.x % GS;
-  const int ng = gridDim.x * (blockDim.x / GS);
-  for (int r = blockIdx.x * (blockDim.x / GS) + threadIdx.x / GS; r < n; r += ng)
+  CD_WARP_ROWS(n)
   {
-    const int b = rp[r], e = rp[r + 1];
+    const int r = (int)base + sub;
     T s = 0;
-    for (int j = b + lane; j < e; j += GS) s += a[j] * __ldg(x + kc[j]);
+    if (r < n)
+      for (int j = rp[r] + lane; j < rp[r + 1]; j += GS) s += a[j] * __ldg(x + kc[j]);
     s = group_sum<GS>(s);
-    if (lane == 0) y[r] = s;
+    if (r < n && lane == 0) y[r] = s;
   }
 }
 
@@ -68,16 +76,15 @@ __global__ void __launch_bounds__(kBlock) defect_kernel(int n, const int *__rest
                                                         double *__restrict__ partial)
 {
   __shared__ double red[kBlock / GS];
-  const int lane = threadIdx.x % GS, grp = threadIdx.x / GS;
-  const int ng = gridDim.x * (blockDim.x / GS);
   double acc = 0;
-  for (int r = blockIdx.x * (blockDim.x / GS) + grp; r < n; r += ng)
+  CD_WARP_ROWS(n)
   {
-    const int b = rp[r], e = rp[r + 1];
+    const int r = (int)base + sub;
     T s = 0;
-    for (int j = b + lane; j < e; j += GS) s += a[j] * __ldg(x + kc[j]);
+    if (r < n)
+      for (int j = rp[r] + lane; j < rp[r + 1]; j += GS) s += a[j] * __ldg(x + kc[j]);
     s = group_sum<GS>(s);
-    if (lane == 0)
+    if (r < n && lane == 0)
     {
       T v = f[r] - s;
       d[r] = v;
@@ -86,7 +93,7 @@ __global__ void __launch_bounds__(kBlock) defect_kernel(int n, const int *__rest
   }
   if (partial)
   {
-    if (lane == 0) red[grp] = acc;
+    if (lane == 0) red[threadIdx.x / GS] = acc;
     __syncthreads();
     if (threadIdx.x == 0)
     {
@@ -108,27 +115,23 @@ __global__ void __launch_bounds__(kBlock) jacobi_kernel(int n, int n_active,
                                                         const T *__restrict__ f,
                                                         T *__restrict__ xo, T omega)
 {
-  const int lane = threadIdx.x % GS;
-  const int ng = gridDim.x * (blockDim.x / GS);
-  for (int r = blockIdx.x * (blockDim.x / GS) + threadIdx.x / GS; r < n; r += ng)
+  CD_WARP_ROWS(n)
   {
-    if (r >= n_active)
-    {
-      if (lane == 0) xo[r] = f[r];
-      continue;
-    }
-    const int b = rp[r], e = rp[r + 1];
+    const int r = (int)base + sub;
     T s = 0;
-    for (int j = b + lane; j < e; j += GS)
-    {
-      int c = kc[j];
-      if (c != r) s += a[j] * __ldg(x + c);
-    }
+    if (r < n_active)
+      for (int j = rp[r] + lane; j < rp[r + 1]; j += GS)
+      {
+        int c = kc[j];
+        if (c != r) s += a[j] * __ldg(x + c);
+      }
     s = group_sum<GS>(s);
-    if (lane == 0)
+    if (r < n && lane == 0)
     {
-      T t = x[r];
-      xo[r] = (T(1) - omega) * t + omega * (f[r] - s) / diag[r];
+      if (r >= n_active)
+        xo[r] = f[r]; // Dirichlet rows take the right-hand side
+      else
+        xo[r] = (T(1) - omega) * x[r] + omega * (f[r] - s) / diag[r];
     }
   }
 }
@@ -161,15 +164,14 @@ __global__ void __launch_bounds__(kBlock) restrict_kernel(int nc, int nc_active,
                                                           const T *__restrict__ d,
                                                           T *__restrict__ crhs, T *__restrict__ csol)
 {
-  const int lane = threadIdx.x % GS;
-  const int ng = gridDim.x * (blockDim.x / GS);
-  for (int r = blockIdx.x * (blockDim.x / GS) + threadIdx.x / GS; r < nc; r += ng)
+  CD_WARP_ROWS(nc)
   {
+    const int r = (int)base + sub;
     T s = 0;
     if (r < nc_active)
       for (int j = rr[r] + lane; j < rr[r + 1]; j += GS) s += rv[j] * __ldg(d + rc[j]);
     s = group_sum<GS>(s);
-    if (lane == 0) { crhs[r] = s; csol[r] = 0; }
+    if (r < nc && lane == 0) { crhs[r] = s; csol[r] = 0; }
   }
 }
 
@@ -183,14 +185,14 @@ __global__ void __launch_bounds__(kBlock) prolong_kernel(int nf, int nf_active,
                                                          const T *__restrict__ xc,
                                                          T *__restrict__ sol, T damp)
 {
-  const int lane = threadIdx.x % GS;
-  const int ng = gridDim.x * (blockDim.x / GS);
-  for (int r = blockIdx.x * (blockDim.x / GS) + threadIdx.x / GS; r < nf_active; r += ng)
+  CD_WARP_ROWS(nf_active)
   {
+    const int r = (int)base + sub;
     T s = 0;
-    for (int j = pr[r] + lane; j < pr[r + 1]; j += GS) s += pv[j] * __ldg(xc + pc[j]);
+    if (r < nf_active)
+      for (int j = pr[r] + lane; j < pr[r + 1]; j += GS) s += pv[j] * __ldg(xc + pc[j]);
     s = group_sum<GS>(s);
-    if (lane == 0) sol[r] += damp * s;
+    if (r < nf_active && lane == 0) sol[r] += damp * s;
   }
 }
 
@@ -411,15 +413,26 @@ template <typename A, typename B> __global__ void convert_kernel(int n, const A 
 
 // zero a vector and copy the Dirichlet part of rhs into it (MultiGridScaIte.C:79-85:
 // zero start + SetDirichletNodes, MultiGrid3D.C:671)
-template <typename T, typename S>
-__global__ void mg_start_kernel(int n, int n_active, const S *__restrict__ rhs_in, T *__restrict__ rhs,
+// The input vector is read through a device-side pointer slot so that one captured
+// CUDA graph serves every FGMRES basis vector.
+template <typename T>
+__global__ void mg_start_kernel(int n, int n_active, double *const *__restrict__ io, T *__restrict__ rhs,
                                 T *__restrict__ sol)
 {
+  const double *rhs_in = io[0];
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   T v = (T)rhs_in[i];
   rhs[i] = v;
   sol[i] = i < n_active ? T(0) : v;
+}
+
+template <typename T>
+__global__ void mg_finish_kernel(int n, const T *__restrict__ sol, double *const *__restrict__ io)
+{
+  double *out = io[1];
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (double)sol[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -466,6 +479,9 @@ template <> const float *rval<float>(const Level &l) { return l.d_r_val32; }
 template <typename T> static LevelVec<T> &vecs(Level &l);
 template <> LevelVec<double> &vecs<double>(Level &l) { return l.v64; }
 template <> LevelVec<float> &vecs<float>(Level &l) { return l.v32; }
+template <typename T> static LevelVec<T> &canon(Level &l);
+template <> LevelVec<double> &canon<double>(Level &l) { return l.c64; }
+template <> LevelVec<float> &canon<float>(Level &l) { return l.c32; }
 
 template <typename T, int GS>
 static void launch_jacobi(cdgpu_ctx *ctx, const Space &s, const T *x, const T *f, T *xo, T omega)
@@ -596,15 +612,18 @@ template <typename T> static int cycle(cdgpu_ctx *ctx, Hierarchy &h, CycleState 
   return smooth<T>(ctx, h, cs, i, cs.p->post);
 }
 
-// one preconditioner application z = M^{-1} r (TMultiGridScaIte::Iterate with zero start)
-template <typename T>
-static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *r, double *z)
+// enqueue one preconditioner application z = M^{-1} r (TMultiGridScaIte::Iterate with zero
+// start); r and z are read from the device pointer slot h.d_io
+template <typename T> static int mg_record(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p)
 {
   int L = (int)h.lev.size();
+  // every level starts from its own first buffer, so the recorded pointers are the same on
+  // every application
+  for (auto &lv : h.lev) vecs<T>(lv) = canon<T>(lv);
   Level &F = h.lev[L - 1];
   LevelVec<T> &v = vecs<T>(F);
   int n = F.sp->n_dof;
-  mg_start_kernel<T, double><<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, F.sp->n_active, r, v.rhs, v.sol);
+  mg_start_kernel<T><<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, F.sp->n_active, h.d_io, v.rhs, v.sol);
   CD_LAUNCHED(ctx);
   CycleState cs;
   cs.p = &p;
@@ -615,8 +634,55 @@ static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, 
   cs.active_zero[L - 1] = true;
   int rc = cycle<T>(ctx, h, cs, L - 1);
   if (rc) return rc;
-  convert_kernel<T, double><<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, v.sol, z);
+  mg_finish_kernel<T><<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, v.sol, h.d_io);
   CD_LAUNCHED(ctx);
+  return CDGPU_OK;
+}
+
+static bool same_cycle_params(const cdgpu_solver_params &a, const cdgpu_solver_params &b)
+{
+  return a.precision == b.precision && a.pre == b.pre && a.post == b.post && a.cycle == b.cycle &&
+         a.coarse_smoother == b.coarse_smoother && a.coarse_maxit == b.coarse_maxit &&
+         a.coarse_red == b.coarse_red && a.omega == b.omega && a.gmg_damp == b.gmg_damp;
+}
+
+// The whole V/W/F cycle (about 7 kernels per level) is captured once into a CUDA graph
+// and replayed for every basis vector; only the two pointers in h.d_io change.
+static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *r, double *z)
+{
+  const int k = p.precision == 1 ? 1 : 0;
+  int rc;
+  if (!h.gexec[k] || !same_cycle_params(h.gparams[k], p))
+  {
+    if (h.gexec[k]) { cudaGraphExecDestroy(h.gexec[k]); h.gexec[k] = nullptr; }
+    // dynamic shared memory of the coarse kernels is set outside the capture
+    const int nc = h.lev[0].sp->n_dof;
+    const int sm1 = (int)(sizeof(double) * nc), sm2 = 2 * sm1;
+    CD_CUDA(ctx, cudaFuncSetAttribute(coarse_exact_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm1));
+    CD_CUDA(ctx, cudaFuncSetAttribute(coarse_exact_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm1));
+    CD_CUDA(ctx, cudaFuncSetAttribute(coarse_smooth_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm2));
+    CD_CUDA(ctx, cudaFuncSetAttribute(coarse_smooth_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm2));
+    cudaGraph_t g = nullptr;
+    const long long before = ctx->launches;
+    CD_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    rc = k == 1 ? mg_record<float>(ctx, h, p) : mg_record<double>(ctx, h, p);
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    h.graph_nodes[k] = ctx->launches - before; // kernels per replay; capturing runs none
+    ctx->launches = before;
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture of the multigrid cycle");
+    e = cudaGraphInstantiate(&h.gexec[k], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { h.gexec[k] = nullptr; return cuda_fail(ctx, e, "graph instantiate"); }
+    h.gparams[k] = p;
+  }
+  int slot = (h.io_slot++) & 63;
+  h.h_io[2 * slot] = const_cast<double *>(r);
+  h.h_io[2 * slot + 1] = z;
+  CD_CUDA(ctx, cudaMemcpyAsync(h.d_io, h.h_io + 2 * slot, 2 * sizeof(double *), cudaMemcpyHostToDevice,
+                               ctx->stream));
+  CD_CUDA(ctx, cudaGraphLaunch(h.gexec[k], ctx->stream));
+  ctx->launches += h.graph_nodes[k];
   return CDGPU_OK;
 }
 
@@ -639,8 +705,10 @@ int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m)
   int rc;
   for (auto &L : h.lev)
   {
-    if (!L.v64.sol && (rc = alloc_vecs(ctx, L.v64, L.sp->n_dof))) return rc;
-    if (!L.v32.sol && (rc = alloc_vecs(ctx, L.v32, L.sp->n_dof))) return rc;
+    if (!L.c64.sol && (rc = alloc_vecs(ctx, L.c64, L.sp->n_dof))) return rc;
+    if (!L.c32.sol && (rc = alloc_vecs(ctx, L.c32, L.sp->n_dof))) return rc;
+    L.v64 = L.c64;
+    L.v32 = L.c32;
   }
   int n = h.lev.back().sp->n_dof;
   if (h.m != m)
@@ -658,6 +726,8 @@ int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m)
         (rc = dev_alloc(ctx, &h.d_x, n)) || (rc = dev_alloc(ctx, &h.d_b, n)))
       return rc;
     CD_CUDA(ctx, cudaMallocHost((void **)&h.h_ctl, 256 * sizeof(double)));
+    CD_CUDA(ctx, cudaMallocHost((void **)&h.h_io, 128 * sizeof(double *)));
+    if ((rc = dev_alloc(ctx, &h.d_io, 2))) return rc;
   }
   return CDGPU_OK;
 }
@@ -849,7 +919,7 @@ int defect64(cdgpu_ctx *ctx, const Space &s, const double *x, const double *f, d
 
 static int precondition(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *r, double *z)
 {
-  return p.precision == 1 ? mg_apply<float>(ctx, h, p, r, z) : mg_apply<double>(ctx, h, p, r, z);
+  return mg_apply(ctx, h, p, r, z);
 }
 
 // the host copy of the FGMRES control block: [0..k) h1, [33..33+k) h2, [66] ||w||^2
