@@ -34,7 +34,7 @@ static void free_space(Space *s)
   if (!s) return;
   void *ptrs[] = {s->d_coords, s->d_gn,  s->d_row_ptr, s->d_kcol,     s->d_dir_start, s->d_inc_ptr,
                   s->d_inc,    s->d_a,   s->d_rhs,     s->d_diag,     s->d_a32,       s->d_diag32,
-                  s->d_tab,    s->d_cellcoef, s->d_local, s->d_dir, s->d_ref};
+                  s->d_tab,    s->d_cellcoef, s->d_local, s->d_dir, s->d_ref, s->d_quadtab};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete s;
@@ -95,6 +95,8 @@ void cdgpu_destroy(cdgpu_ctx *ctx)
   cudaStreamSynchronize(ctx->stream);
   for (auto *h : ctx->mgs) free_mg(h);
   for (auto *s : ctx->spaces) free_space(s);
+  if (ctx->d_err) cudaFree(ctx->d_err);
+  if (ctx->h_err) cudaFreeHost(ctx->h_err);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -473,10 +475,10 @@ int cdgpu_assemble_hierarchy(cdgpu_ctx *ctx, int mg_id, int disctype, int coarse
   for (size_t l = 0; l < h->lev.size(); l++)
   {
     int d = l + 1 == h->lev.size() ? disctype : coarse_disctype;
-    int rc = assemble_space(ctx, *h->lev[l].sp, d, nullptr);
+    int rc = assemble_space(ctx, *h->lev[l].sp, d, nullptr, false);
     if (rc) return rc;
   }
-  return CDGPU_OK;
+  return assemble_check(ctx);
 }
 
 int cdgpu_solve_device(cdgpu_ctx *ctx, int mg_id, const cdgpu_solver_params *p, const double *d_rhs, double *d_sol,

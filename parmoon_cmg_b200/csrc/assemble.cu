@@ -488,13 +488,33 @@ static int launch_gather(cdgpu_ctx *ctx, const GatherArgs &g, int n_dof)
 // ---------------------------------------------------------------------------
 // driver
 // ---------------------------------------------------------------------------
-int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir)
+int assemble_check(cdgpu_ctx *ctx)
+{
+  CD_CUDA(ctx, cudaMemcpyAsync(ctx->h_err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  int e = *ctx->h_err;
+  if (e)
+  {
+    CD_CUDA(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    if (e == 1) return fail(ctx, CDGPU_ERR_PATTERN, "assemble: a cell coupling is missing from the CSR pattern");
+    return fail(ctx, CDGPU_ERR_UNSUPPORTED, "assemble: CSR row longer than the kernel's row buffer");
+  }
+  return CDGPU_OK;
+}
+
+int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, bool check)
 {
   if (s.nnz < 0) return fail(ctx, CDGPU_ERR_INVALID, "assemble: no pattern (call cdgpu_build_pattern)");
   if (!s.co_set) return fail(ctx, CDGPU_ERR_INVALID, "assemble: coefficients not set");
   if (disctype != CDGPU_GALERKIN && disctype != CDGPU_SUPG)
     return fail(ctx, CDGPU_ERR_UNSUPPORTED, "assemble: DISCTYPE must be GALERKIN (1) or SUPG (2)");
   int rc;
+  if (!ctx->d_err)
+  {
+    if ((rc = dev_alloc(ctx, &ctx->d_err, 1))) return rc;
+    CD_CUDA(ctx, cudaMallocHost((void **)&ctx->h_err, sizeof(int)));
+    CD_CUDA(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+  }
   if (!s.d_a)
   {
     if ((rc = dev_alloc(ctx, &s.d_a, s.nnz)) || (rc = dev_alloc(ctx, &s.d_a32, s.nnz)) ||
@@ -506,13 +526,17 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir)
   const double *d_dir = nullptr;
   if (h_dir && n_dir > 0)
   {
-    if ((rc = dev_alloc(ctx, &s.d_dir, n_dir))) return rc;
+    if (!s.d_dir && (rc = dev_alloc(ctx, &s.d_dir, n_dir))) return rc;
     CD_CUDA(ctx, cudaMemcpyAsync(s.d_dir, h_dir, sizeof(double) * n_dir, cudaMemcpyHostToDevice,
                                  ctx->stream));
     d_dir = s.d_dir;
   }
-  RefElement re;
-  make_ref_element(s.dim, s.order, re);
+  if (!s.re_ready)
+  {
+    make_ref_element(s.dim, s.order, s.re);
+    s.re_ready = true;
+  }
+  const RefElement &re = s.re;
   bool fast = s.all_affine && s.co.kind == CDGPU_COEFF_CONSTANT;
   int T = n_tensors(s.dim, disctype), Tr = n_rhs_tensors(s.dim, disctype);
   Coef co = to_coef(s.co);
@@ -536,20 +560,18 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir)
   }
   else
   {
-    static thread_local std::vector<double> dummy;
-    double *d_tab = nullptr;
-    std::vector<double> packed;
-    // reference tables for the quadrature path
-    packed.insert(packed.end(), re.qx.begin(), re.qx.end());
-    packed.insert(packed.end(), re.qw.begin(), re.qw.end());
-    packed.insert(packed.end(), re.phi.begin(), re.phi.end());
-    packed.insert(packed.end(), re.dphi.begin(), re.dphi.end());
-    packed.insert(packed.end(), re.hphi.begin(), re.hphi.end());
-    if ((rc = dev_alloc(ctx, &s.d_ref, packed.size()))) return rc;
-    s.ref_disctype = -1;
-    CD_CUDA(ctx, cudaMemcpyAsync(s.d_ref, packed.data(), packed.size() * sizeof(double),
-                                 cudaMemcpyHostToDevice, ctx->stream));
-    CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (!s.d_quadtab)
+    {
+      std::vector<double> packed;
+      packed.insert(packed.end(), re.qx.begin(), re.qx.end());
+      packed.insert(packed.end(), re.qw.begin(), re.qw.end());
+      packed.insert(packed.end(), re.phi.begin(), re.phi.end());
+      packed.insert(packed.end(), re.dphi.begin(), re.dphi.end());
+      packed.insert(packed.end(), re.hphi.begin(), re.hphi.end());
+      if ((rc = dev_alloc(ctx, &s.d_quadtab, packed.size()))) return rc;
+      CD_CUDA(ctx, cudaMemcpy(s.d_quadtab, packed.data(), packed.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    const double *d_tab = nullptr;
     if (s.co.kind == CDGPU_COEFF_TABLE)
     {
       if (!s.d_tab) return fail(ctx, CDGPU_ERR_INVALID, "assemble: coefficient table missing");
@@ -557,43 +579,31 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir)
     }
     if (!s.d_local && (rc = dev_alloc(ctx, &s.d_local, (size_t)s.n_cells * (s.nbf * s.nbf + s.nbf))))
       return rc;
-    const double *base = s.d_ref;
     LocalArgs a;
     a.dim = s.dim; a.nv = s.nv; a.nbf = s.nbf; a.nq = re.nq; a.n_cells = s.n_cells;
     a.disctype = disctype; a.affine_all = s.all_affine; a.co = co; a.coords = s.d_coords; a.tab = d_tab;
-    a.qx = base; a.qw = a.qx + re.qx.size(); a.phi = a.qw + re.qw.size();
+    a.qx = s.d_quadtab; a.qw = a.qx + re.qx.size(); a.phi = a.qw + re.qw.size();
     a.dphi = a.phi + re.phi.size(); a.hphi = a.dphi + re.dphi.size(); a.out = s.d_local;
     size_t sm = sizeof(double) * ((size_t)re.nq * s.nbf * s.dim + (size_t)re.nq * s.nbf + re.nq * 8 +
                                   (size_t)re.nq * s.dim * s.dim);
     CD_CUDA(ctx, cudaFuncSetAttribute(local_quad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     local_quad_kernel<<<s.n_cells, 256, sm, ctx->stream>>>(a);
     CD_LAUNCHED(ctx);
-    (void)dummy;
   }
-  int *d_err = nullptr;
-  if ((rc = dev_alloc(ctx, &d_err, 1))) return rc;
-  CD_CUDA(ctx, cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
   GatherArgs g;
   g.n_dof = s.n_dof; g.n_active = s.n_active; g.nbf = s.nbf; g.T = T; g.Tr = Tr; g.mode = fast ? 0 : 1;
   g.row_ptr = s.d_row_ptr; g.kcol = s.d_kcol; g.inc_ptr = s.d_inc_ptr; g.inc = s.d_inc; g.gn = s.d_gn;
   g.cellcoef = s.d_cellcoef; g.local = s.d_local; g.R = s.d_ref;
-  g.r = s.d_ref + (size_t)s.nbf * s.nbf * T; g.dir = d_dir;
-  g.a = s.d_a; g.rhs = s.d_rhs; g.diag = s.d_diag; g.a32 = s.d_a32; g.diag32 = s.d_diag32; g.err = d_err;
+  g.r = s.d_ref ? s.d_ref + (size_t)s.nbf * s.nbf * T : nullptr; g.dir = d_dir;
+  g.a = s.d_a; g.rhs = s.d_rhs; g.diag = s.d_diag; g.a32 = s.d_a32; g.diag32 = s.d_diag32; g.err = ctx->d_err;
   if (s.dim == 2 && s.order == 1) rc = launch_gather<4, 16>(ctx, g, s.n_dof);
   else if (s.dim == 2) rc = launch_gather<16, 32>(ctx, g, s.n_dof);
   else if (s.order == 1) rc = launch_gather<8, 32>(ctx, g, s.n_dof);
   else rc = launch_gather<32, CD_MAXROW>(ctx, g, s.n_dof);
-  if (rc) { cudaFree(d_err); return rc; }
-  int h_err = 0;
-  cudaError_t e = cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  cudaFree(d_err);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "assemble");
-  if (h_err == 1) return fail(ctx, CDGPU_ERR_PATTERN, "assemble: a cell coupling is missing from the CSR pattern");
-  if (h_err == 2) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "assemble: CSR row longer than the kernel's row buffer");
+  if (rc) return rc;
   s.assembled = true;
   s.assembly_version++;
-  return CDGPU_OK;
+  return check ? assemble_check(ctx) : CDGPU_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -63,8 +63,11 @@ struct Space
   double *d_local = nullptr;    // quadrature path: n_cells x (nbf*nbf + nbf)
   double *d_dir = nullptr;      // Dirichlet values
   double *d_ref = nullptr;      // reference tensors (affine path)
+  double *d_quadtab = nullptr;  // reference-element tables (quadrature path)
   int ref_disctype = -1;
   int n_tab = 0;
+  RefElement re;                // reference element of (dim, order), built on first use
+  bool re_ready = false;
 };
 
 // ---------------------------------------------------------------------------
@@ -120,6 +123,8 @@ struct cdgpu_ctx
   long long launches = 0;
   std::vector<Space *> spaces;
   std::vector<Hierarchy *> mgs;
+  int *d_err = nullptr; // assembly error flag (device) and its pinned host mirror
+  int *h_err = nullptr;
 };
 
 // error helpers: set ctx->err and return a status
@@ -158,7 +163,9 @@ void build_prolongation(const Space &coarse, const Space &fine, const int *paren
 bool dense_inverse(int n, std::vector<double> &a); // in place, row-major; false if singular
 
 // device entry points (assemble.cu / solve.cu)
-int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir);
+// assemble one space; with check = false the error flag is left for assemble_check
+int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, bool check = true);
+int assemble_check(cdgpu_ctx *ctx);
 int add_neumann(cdgpu_ctx *ctx, Space &s, int n_edges, const int *cell, const int *edge,
                 const double *g);
 int spmv64(cdgpu_ctx *ctx, const Space &s, const double *x, double *y);

@@ -43,6 +43,41 @@ template <int GS, typename T> __device__ __forceinline__ T group_sum(T v)
   return v;
 }
 
+// partial dot of CSR row [b, e) with x for one lane of a GS-thread group; four entries per
+// lane are loaded before they are used so that more loads are in flight
+template <typename T, int GS, bool SKIP_DIAG>
+__device__ __forceinline__ T row_dot(int b, int e, int lane, int row, const int *__restrict__ kc,
+                                     const T *__restrict__ a, const T *__restrict__ x)
+{
+  T s = 0;
+  int j = b + lane;
+  for (; j + 3 * GS < e; j += 4 * GS)
+  {
+    int c0 = kc[j], c1 = kc[j + GS], c2 = kc[j + 2 * GS], c3 = kc[j + 3 * GS];
+    T a0 = a[j], a1 = a[j + GS], a2 = a[j + 2 * GS], a3 = a[j + 3 * GS];
+    T x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
+    if (SKIP_DIAG)
+    {
+      if (c0 == row) a0 = 0;
+      if (c1 == row) a1 = 0;
+      if (c2 == row) a2 = 0;
+      if (c3 == row) a3 = 0;
+    }
+    s += a0 * x0;
+    s += a1 * x1;
+    s += a2 * x2;
+    s += a3 * x3;
+  }
+  for (; j < e; j += GS)
+  {
+    int c = kc[j];
+    T v = a[j];
+    if (SKIP_DIAG && c == row) v = 0;
+    s += v * __ldg(x + c);
+  }
+  return s;
+}
+
 #define CD_WARP_ROWS(n)                                                                      \
   const int lane = threadIdx.x % GS, sub = (threadIdx.x % 32) / GS;                          \
   const long nwarp = (long)gridDim.x * blockDim.x / 32;                                      \
@@ -59,8 +94,7 @@ __global__ void __launch_bounds__(kBlock) spmv_kernel(int n, const int *__restri
   {
     const int r = (int)base + sub;
     T s = 0;
-    if (r < n)
-      for (int j = rp[r] + lane; j < rp[r + 1]; j += GS) s += a[j] * __ldg(x + kc[j]);
+    if (r < n) s = row_dot<T, GS, false>(rp[r], rp[r + 1], lane, r, kc, a, x);
     s = group_sum<GS>(s);
     if (r < n && lane == 0) y[r] = s;
   }
@@ -81,8 +115,7 @@ __global__ void __launch_bounds__(kBlock) defect_kernel(int n, const int *__rest
   {
     const int r = (int)base + sub;
     T s = 0;
-    if (r < n)
-      for (int j = rp[r] + lane; j < rp[r + 1]; j += GS) s += a[j] * __ldg(x + kc[j]);
+    if (r < n) s = row_dot<T, GS, false>(rp[r], rp[r + 1], lane, r, kc, a, x);
     s = group_sum<GS>(s);
     if (r < n && lane == 0)
     {
@@ -119,12 +152,7 @@ __global__ void __launch_bounds__(kBlock) jacobi_kernel(int n, int n_active,
   {
     const int r = (int)base + sub;
     T s = 0;
-    if (r < n_active)
-      for (int j = rp[r] + lane; j < rp[r + 1]; j += GS)
-      {
-        int c = kc[j];
-        if (c != r) s += a[j] * __ldg(x + c);
-      }
+    if (r < n_active) s = row_dot<T, GS, true>(rp[r], rp[r + 1], lane, r, kc, a, x);
     s = group_sum<GS>(s);
     if (r < n && lane == 0)
     {
@@ -310,43 +338,58 @@ __global__ void coarse_smooth_kernel(int n, int n_active, const int *__restrict_
 // ---------------------------------------------------------------------------
 // dense vector kernels for FGMRES (FP64)
 // ---------------------------------------------------------------------------
-// per-block partial dot products of w with k basis vectors Y[0..k) (row stride n)
-// optionally after w -= Y coef (fused), and/or partial ||w||^2 (slot k)
-__global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, int k, const double *__restrict__ Y,
+// One fused pass of classical Gram-Schmidt over K basis vectors Y[0..K) (row stride n):
+//   GS_DOTS       partial dots  w . Y_j
+//   GS_AXPY_DOTS  w -= sum_j coef_j Y_j, then partial dots of the new w with every Y_j
+//   GS_AXPY_NORM  w -= sum_j coef_j Y_j, then partial ||w||^2
+// Every thread keeps the K basis values of its row in registers; per-block partials go to
+// partial[block * 33 + slot] and are summed in block order by reduce_partials_kernel.
+enum { GS_DOTS = 0, GS_AXPY_DOTS = 1, GS_AXPY_NORM = 2 };
+
+template <int K, int MODE>
+__global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, const double *__restrict__ Y,
                                                          double *__restrict__ w,
                                                          const double *__restrict__ coef,
-                                                         int do_dots, double *__restrict__ partial)
+                                                         double *__restrict__ partial)
 {
-  __shared__ double red[kBlock / 32][33];
-  double acc[33];
+  constexpr int NS = MODE == GS_AXPY_NORM ? 1 : K;
+  __shared__ double red[kBlock / 32][NS];
+  double acc[NS];
 #pragma unroll
-  for (int j = 0; j < 33; j++) acc[j] = 0;
-  double cf[32];
-  if (coef)
-    for (int j = 0; j < k; j++) cf[j] = coef[j];
+  for (int j = 0; j < NS; j++) acc[j] = 0;
+  double cf[K];
+#pragma unroll
+  for (int j = 0; j < K; j++) cf[j] = MODE == GS_DOTS ? 0.0 : coef[j];
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
   {
+    double y[K];
+#pragma unroll
+    for (int j = 0; j < K; j++) y[j] = __ldg(Y + (size_t)j * n + i);
     double wi = w[i];
-    if (coef)
+    if (MODE != GS_DOTS)
     {
-      for (int j = 0; j < k; j++) wi -= cf[j] * Y[(size_t)j * n + i];
+#pragma unroll
+      for (int j = 0; j < K; j++) wi -= cf[j] * y[j];
       w[i] = wi;
     }
-    if (do_dots)
-      for (int j = 0; j < k; j++) acc[j] += wi * Y[(size_t)j * n + i];
-    acc[32] += wi * wi;
+    if (MODE == GS_AXPY_NORM)
+      acc[0] += wi * wi;
+    else
+    {
+#pragma unroll
+      for (int j = 0; j < K; j++) acc[j] += wi * y[j];
+    }
   }
   const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
-  int nslots = do_dots ? k : 0;
-  for (int j = 0; j <= nslots; j++)
+#pragma unroll
+  for (int j = 0; j < NS; j++)
   {
-    int slot = j < nslots ? j : 32;
-    double v = group_sum<32>(acc[slot]);
+    double v = group_sum<32>(acc[j]);
     if (lane == 0) red[warp][j] = v;
   }
   __syncthreads();
-  if (threadIdx.x <= nslots)
+  if (threadIdx.x < NS)
   {
     double t = 0;
     for (int g = 0; g < kBlock / 32; g++) t += red[g][threadIdx.x];
@@ -354,15 +397,40 @@ __global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, int k, const dou
   }
 }
 
-// sum per-block partials in block order: out[j] = sum_b partial[b][j], j <= nslots
+template <int MODE>
+static void launch_gs(int k, int grid, cudaStream_t st, int n, const double *Y, double *w, const double *coef,
+                      double *partial)
+{
+  switch (k)
+  {
+#define CD_GS_CASE(K) case K: gs_pass_kernel<K, MODE><<<grid, kBlock, 0, st>>>(n, Y, w, coef, partial); break;
+    CD_GS_CASE(1) CD_GS_CASE(2) CD_GS_CASE(3) CD_GS_CASE(4) CD_GS_CASE(5) CD_GS_CASE(6) CD_GS_CASE(7)
+    CD_GS_CASE(8) CD_GS_CASE(9) CD_GS_CASE(10) CD_GS_CASE(11) CD_GS_CASE(12) CD_GS_CASE(13) CD_GS_CASE(14)
+    CD_GS_CASE(15) CD_GS_CASE(16) CD_GS_CASE(17) CD_GS_CASE(18) CD_GS_CASE(19) CD_GS_CASE(20) CD_GS_CASE(21)
+    CD_GS_CASE(22) CD_GS_CASE(23) CD_GS_CASE(24) CD_GS_CASE(25) CD_GS_CASE(26) CD_GS_CASE(27) CD_GS_CASE(28)
+    CD_GS_CASE(29) CD_GS_CASE(30) CD_GS_CASE(31) CD_GS_CASE(32)
+#undef CD_GS_CASE
+    default: break;
+  }
+}
+
+// out[j] = sum_b partial[b][j] for j < nslots, one block per slot, fixed summation order
 __global__ void reduce_partials_kernel(int nblocks, int nslots, const double *__restrict__ partial,
                                        double *__restrict__ out)
 {
-  int j = threadIdx.x;
-  if (j > nslots) return;
+  __shared__ double red[32];
+  const int j = blockIdx.x;
   double t = 0;
-  for (int b = 0; b < nblocks; b++) t += partial[(size_t)b * 33 + j];
-  out[j] = t;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) t += partial[(size_t)b * 33 + j];
+  t = group_sum<32>(t);
+  if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = t;
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
+    double s = 0;
+    for (int w = 0; w < (int)blockDim.x / 32; w++) s += red[w];
+    out[j] = s;
+  }
 }
 
 __global__ void sum_blocks_kernel(int nblocks, const double *__restrict__ partial, double *out)
@@ -1000,19 +1068,19 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
       if ((rc = spmv64(ctx, s, Z(i), h.d_w))) return rc;
       int k = i + 1, pb = h.partial_blocks;
       // pass 1: h1 = V^T w
-      gs_pass_kernel<<<pb, kBlock, 0, ctx->stream>>>(n, k, h.d_V, h.d_w, nullptr, 1, h.d_partial);
+      launch_gs<GS_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, nullptr, h.d_partial);
       CD_LAUNCHED(ctx);
-      reduce_partials_kernel<<<1, 64, 0, ctx->stream>>>(pb, k - 1, h.d_partial, h.d_ctl);
+      reduce_partials_kernel<<<k, 256, 0, ctx->stream>>>(pb, k, h.d_partial, h.d_ctl);
       CD_LAUNCHED(ctx);
       // pass 2: w -= V h1, h2 = V^T w
-      gs_pass_kernel<<<pb, kBlock, 0, ctx->stream>>>(n, k, h.d_V, h.d_w, h.d_ctl, 1, h.d_partial);
+      launch_gs<GS_AXPY_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, h.d_ctl, h.d_partial);
       CD_LAUNCHED(ctx);
-      reduce_partials_kernel<<<1, 64, 0, ctx->stream>>>(pb, k - 1, h.d_partial, h.d_ctl + 33);
+      reduce_partials_kernel<<<k, 256, 0, ctx->stream>>>(pb, k, h.d_partial, h.d_ctl + 33);
       CD_LAUNCHED(ctx);
       // w -= V h2, ||w||^2
-      gs_pass_kernel<<<pb, kBlock, 0, ctx->stream>>>(n, k, h.d_V, h.d_w, h.d_ctl + 33, 0, h.d_partial);
+      launch_gs<GS_AXPY_NORM>(k, pb, ctx->stream, n, h.d_V, h.d_w, h.d_ctl + 33, h.d_partial);
       CD_LAUNCHED(ctx);
-      reduce_partials_kernel<<<1, 64, 0, ctx->stream>>>(pb, 0, h.d_partial, h.d_ctl + 66);
+      reduce_partials_kernel<<<1, 256, 0, ctx->stream>>>(pb, 1, h.d_partial, h.d_ctl + 66);
       CD_LAUNCHED(ctx);
       if ((rc = read_ctl(ctx, h, 67))) return rc;
       // the slot-0 reduction of the last pass holds ||w||^2 (slot 32 of the partials)
