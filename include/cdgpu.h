@@ -163,6 +163,16 @@ int cdgpu_spmv(cdgpu_ctx *ctx, int space_id, const double *h_x, double *h_y);
 int cdgpu_defect(cdgpu_ctx *ctx, int space_id, const double *h_x, const double *h_f, double *h_d,
                  double *res);
 int cdgpu_spmv_device(cdgpu_ctx *ctx, int space_id, const double *d_x, double *d_y);
+/* The defect d = f - A x and *h_res = ||d||, like cdgpu_defect, for callers that cannot
+ * allocate device memory (for example while another allocator holds the whole device, or
+ * where the device synchronisation of cudaFree is not acceptable).  No counterpart in the
+ * reference.  d_x, d_f, d_d: device vectors of the space's length; h_res: host (nullable).
+ * Allocates nothing: the partial sums live in a fixed 32 KB array of the library, so at most
+ * 8,388,608 rows (CDGPU_ERR_UNSUPPORTED beyond).  The first call on a device looks up that
+ * array's address and should come before any stream capture; calls that overlap on the GPU
+ * share the array and race. */
+int cdgpu_defect_noalloc(cdgpu_ctx *ctx, int space_id, const double *d_x, const double *d_f,
+                         double *d_d, double *h_res);
 
 /* --- multigrid hierarchy ------------------------------------------------------
  * Replaces TMultiGrid3D/TMultiGrid2D + AddLevel(TMGLevel) (src/System/SystemCD3D.C:

@@ -65,6 +65,7 @@ SIGNATURES = {
     "cdgpu_spmv": (_I, [_P, _I, _P, _P]),
     "cdgpu_defect": (_I, [_P, _I, _P, _P, _P, C.POINTER(C.c_double)]),
     "cdgpu_spmv_device": (_I, [_P, _I, _P, _P]),
+    "cdgpu_defect_noalloc": (_I, [_P, _I, _P, _P, _P, C.POINTER(C.c_double)]),
     "cdgpu_hierarchy": (_I, [_P, _I, _P, _P, C.POINTER(_I)]),
     "cdgpu_solve": (_I, [_P, _I, C.POINTER(SolverParams), _P, _P, C.POINTER(SolveInfo)]),
     "cdgpu_solve_device": (_I, [_P, _I, C.POINTER(SolverParams), _P, _P, C.POINTER(SolveInfo)]),
