@@ -37,6 +37,9 @@ enum cdgpu_status
 /* discretisation types, include/General/Constants.h:188-190 */
 #define CDGPU_GALERKIN 1
 #define CDGPU_SUPG 2
+/* the mass-matrix form of the time-dependent system (MatrixMRhsAssemble,
+ * src/FE/ConvDiff2D.C:411, src/FE/TCD3D.C:11): M_ij = (phi_j, phi_i), rhs_i = (f, phi_i) */
+#define CDGPU_MASS 10
 
 /* coefficient kinds: how BilinearCoeffs (Examples/CD_2D, CD_3D) is evaluated */
 #define CDGPU_COEFF_CONSTANT 0 /* eps, b, c, f constant in space */
@@ -202,6 +205,26 @@ int cdgpu_solve_device(cdgpu_ctx *ctx, int mg_id, const cdgpu_solver_params *par
 int cdgpu_assemble_hierarchy(cdgpu_ctx *ctx, int mg_id, int disctype, int coarse_disctype);
 /* device pointer of the assembled right-hand side of a space */
 int cdgpu_rhs_device(cdgpu_ctx *ctx, int space_id, double **d_rhs);
+
+/* --- time-dependent problems (theta schemes) --------------------------------
+ * Replace TSystemTCD2D (src/System/SystemTCD2D.C): the constructor (mass and stiffness
+ * matrices on the hierarchy's levels), AssembleMRhs (94-123), AssembleARhs (124-153) and
+ * one step of AssembleSystMat + Solve + RestoreMassMat (154-235) as called by the time
+ * loop of 2DPrograms/TCD2D_ParMooN.C:241-290.  The mass matrix is updated in place like
+ * the reference's, so every step rounds like the reference.  The solve is the multigrid
+ * FGMRES of cdgpu_solve on the system matrices M + tau*theta1*A of every level.
+ * cdgpu_tcd_assemble_stiffness first saves the current right-hand side as the old one
+ * (the time loop's memcpy(oldrhs, rhs)).  Galerkin forms only. */
+int cdgpu_tcd_create(cdgpu_ctx *ctx, int mg_id, int disctype, int *tcd_id);
+int cdgpu_tcd_assemble_mass(cdgpu_ctx *ctx, int tcd_id);
+int cdgpu_tcd_assemble_stiffness(cdgpu_ctx *ctx, int tcd_id);
+int cdgpu_tcd_step(cdgpu_ctx *ctx, int tcd_id, const cdgpu_solver_params *params, double tau,
+                   double theta1, double theta2, double theta3, double theta4, double *h_sol,
+                   cdgpu_solve_info *info);
+int cdgpu_tcd_step_device(cdgpu_ctx *ctx, int tcd_id, const cdgpu_solver_params *params, double tau,
+                          double theta1, double theta2, double theta3, double theta4, double *d_sol,
+                          cdgpu_solve_info *info);
+int cdgpu_tcd_rhs(cdgpu_ctx *ctx, int tcd_id, double *h_rhs);
 
 #ifdef __cplusplus
 }

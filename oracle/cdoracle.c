@@ -521,6 +521,15 @@ int cdo_assemble(int dim, int order, int disctype, int n_cells, const double *co
           }
         }
       }
+      else if (disctype == 10)
+      {
+        /* mass form, MatrixMRhsAssemble (src/FE/ConvDiff2D.C:411-445) */
+        for (int i = 0; i < nbf; i++)
+        {
+          F[i] += mult * phi[q][i] * f;
+          for (int j = 0; j < nbf; j++) A[i][j] += mult * phi[q][j] * phi[q][i];
+        }
+      }
       else
       {
         for (int i = 0; i < nbf; i++)

@@ -211,3 +211,41 @@ def solve(levels, prm, rhs, sol0):
                           ptrs["p_row"], ptrs["p_col"], ptrs["p_val"], C.byref(prm), _p(rhs),
                           _p(sol), _p(hist), C.byref(fres))
     return sol, its, hist[:max(its, 0) + 1], fres.value
+
+
+def tcd_step(levels, M, A, f_old, f, sol, tau, th1, th2, th3, th4, prm):
+    """One theta-scheme step of TSystemTCD2D on the oracle's CSR levels.
+
+    levels: as for :func:`solve` (their ``entries`` are replaced by the system matrices);
+    M, A: per-level mass and stiffness entries (M is updated in place like the
+    reference's sqmatrixM and restored at the end).  Follows
+    src/System/SystemTCD2D.C:231-277 (AssembleSystMat), 323-330 (Solve with GMG) and
+    279-305 (RestoreMassMat): MatAdd acts on the active rows only (Blas2.C MatAdd),
+    B = tau*th3*f_old + tau*th4*f + M_active u_old, Dirichlet entries of B and u from f.
+    Returns (new solution, iterations)."""
+    fine = levels[-1]
+    na = int(fine["n_active"])
+    for lv, m, a in zip(levels, M, A):
+        k = int(lv["row_ptr"][lv["n_active"]])
+        m[:k] += (-tau * th2) * a[:k]
+    B = np.zeros(len(f))
+    B[:na] += tau * th3 * f_old[:na]
+    B[:na] += tau * th4 * f[:na]
+    Mu = spmv(fine["row_ptr"], fine["kcol"], M[-1], sol)
+    B[:na] += Mu[:na]
+    B[na:] = f[na:]
+    u = _f64(sol).copy()
+    u[na:] = f[na:]
+    gamma = -tau * th2
+    sys_levels = []
+    for lv, m, a in zip(levels, M, A):
+        k = int(lv["row_ptr"][lv["n_active"]])
+        m[:k] += (-gamma + tau * th1) * a[:k]
+        d = dict(lv)
+        d["entries"] = m.copy()
+        sys_levels.append(d)
+    u, its, _, _ = solve(sys_levels, prm, B, u)
+    for lv, m, a in zip(levels, M, A):
+        k = int(lv["row_ptr"][lv["n_active"]])
+        m[:k] += (-tau * th1) * a[:k]
+    return u, its

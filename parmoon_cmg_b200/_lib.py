@@ -71,6 +71,14 @@ SIGNATURES = {
     "cdgpu_solve_device": (_I, [_P, _I, C.POINTER(SolverParams), _P, _P, C.POINTER(SolveInfo)]),
     "cdgpu_assemble_hierarchy": (_I, [_P, _I, _I, _I]),
     "cdgpu_rhs_device": (_I, [_P, _I, C.POINTER(C.c_void_p)]),
+    "cdgpu_tcd_create": (_I, [_P, _I, _I, C.POINTER(_I)]),
+    "cdgpu_tcd_assemble_mass": (_I, [_P, _I]),
+    "cdgpu_tcd_assemble_stiffness": (_I, [_P, _I]),
+    "cdgpu_tcd_step": (_I, [_P, _I, C.POINTER(SolverParams), C.c_double, C.c_double, C.c_double,
+                            C.c_double, C.c_double, _P, C.POINTER(SolveInfo)]),
+    "cdgpu_tcd_step_device": (_I, [_P, _I, C.POINTER(SolverParams), C.c_double, C.c_double,
+                                   C.c_double, C.c_double, C.c_double, _P, C.POINTER(SolveInfo)]),
+    "cdgpu_tcd_rhs": (_I, [_P, _I, _P]),
 }
 
 _lib = None

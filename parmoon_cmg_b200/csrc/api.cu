@@ -93,6 +93,7 @@ void cdgpu_destroy(cdgpu_ctx *ctx)
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  for (auto *t : ctx->tcds) free_tcd(t);
   for (auto *h : ctx->mgs) free_mg(h);
   for (auto *s : ctx->spaces) free_space(s);
   if (ctx->d_err) cudaFree(ctx->d_err);

@@ -167,6 +167,12 @@ __global__ void cell_coef_kernel(CellCoefArgs a)
     for (int p = 0; p < dim; p++)
       for (int r = 0; r < dim; r++) K[p * dim + r] += delta * beta[p] * beta[r];
   double *o = a.out + (size_t)c * (a.T + a.Tr);
+  if (a.disctype == CDGPU_MASS)
+  {
+    o[0] = w;
+    o[1] = w * f;
+    return;
+  }
   if (dim == 2)
   {
     o[0] = w * K[0]; o[1] = w * K[3]; o[2] = w * K[1];
@@ -322,6 +328,11 @@ __global__ void local_quad_kernel(LocalArgs a)
       }
       const double *gj = g + (q * nbf + j) * dim;
       double phi_j = a.phi[q * nbf + j];
+      if (a.disctype == CDGPU_MASS)
+      {
+        acc += mult[q] * phi_j * phi_i; // MatrixMRhsAssemble, ConvDiff2D.C:411
+        continue;
+      }
       double val = c0 * (gi[0] * gj[0] + gi[1] * gj[1] + (dim == 3 ? gi[2] * gj[2] : 0.0));
       double bg = c1 * gj[0] + c2 * gj[1] + (dim == 3 ? c3 * gj[2] : 0.0);
       val += bg * phi_i;
@@ -506,8 +517,8 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, 
 {
   if (s.nnz < 0) return fail(ctx, CDGPU_ERR_INVALID, "assemble: no pattern (call cdgpu_build_pattern)");
   if (!s.co_set) return fail(ctx, CDGPU_ERR_INVALID, "assemble: coefficients not set");
-  if (disctype != CDGPU_GALERKIN && disctype != CDGPU_SUPG)
-    return fail(ctx, CDGPU_ERR_UNSUPPORTED, "assemble: DISCTYPE must be GALERKIN (1) or SUPG (2)");
+  if (disctype != CDGPU_GALERKIN && disctype != CDGPU_SUPG && disctype != CDGPU_MASS)
+    return fail(ctx, CDGPU_ERR_UNSUPPORTED, "assemble: DISCTYPE must be GALERKIN (1), SUPG (2) or MASS (10)");
   int rc;
   if (!ctx->d_err)
   {

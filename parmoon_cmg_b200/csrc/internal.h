@@ -114,8 +114,12 @@ struct Hierarchy
 // ---------------------------------------------------------------------------
 // context
 // ---------------------------------------------------------------------------
+struct Tcd; // time-dependent system (tcd.cu)
+void free_tcd(Tcd *t);
+
 struct cdgpu_ctx
 {
+  std::vector<Tcd *> tcds;
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;

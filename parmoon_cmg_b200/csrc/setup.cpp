@@ -139,6 +139,7 @@ void make_ref_element(int dim, int order, RefElement &re)
 // ---------------------------------------------------------------------------
 int n_tensors(int dim, int disctype)
 {
+  if (disctype == CDGPU_MASS) return 1;
   if (dim == 2) return disctype == CDGPU_SUPG ? 14 : 6;
   return disctype == CDGPU_SUPG ? 13 : 10;
 }
@@ -169,7 +170,9 @@ void reference_tensors(const RefElement &re, int disctype, std::vector<double> &
         auto Cb = [&](int b) { return ph[i] * dp[j * dim + b]; };
         auto Da = [&](int a) { return dp[i * dim + a] * ph[j]; };
         auto E = [&](int c, int d, int e) { return hp[(j * dim + c) * dim + d] * dp[i * dim + e]; };
-        if (dim == 2)
+        if (disctype == CDGPU_MASS)
+          o[0] += w * ph[i] * ph[j];
+        else if (dim == 2)
         {
           o[0] += w * I(0, 0);
           o[1] += w * I(1, 1);

@@ -244,6 +244,57 @@ class TSystemCD3D:
         return info
 
 
+class TSystemTCD2D:
+    """Mirror of TSystemTCD2D (src/System/SystemTCD2D.C) for theta schemes on the GPU.
+
+    The time loop of 2DPrograms/TCD2D_ParMooN.C:241-290 becomes::
+
+        S = TSystemTCD2D(spaces, parents); S.Init(coeffs(...))
+        S.AssembleMRhs(sol)                   # mass matrices, initial rhs
+        for step: S.AssembleARhs()            # stiffness + rhs at the new time (saves the old rhs)
+                  S.Step(sol, tau, theta...)  # AssembleSystMat + Solve + RestoreMassMat
+    """
+
+    def __init__(self, fespaces, parents, disctype=GALERKIN, ctx=None):
+        self.ctx = ctx or Context()
+        self.spaces = fespaces
+        self.sids = [self.ctx.upload_space(s) for s in fespaces]
+        for sid in self.sids:
+            self.ctx.build_pattern(sid)
+        self.mg = self.ctx.hierarchy(self.sids, parents)
+        tid = C.c_int()
+        self.ctx.check(self.ctx.lib.cdgpu_tcd_create(self.ctx.h, self.mg, disctype, C.byref(tid)))
+        self.tcd = tid.value
+        self.N_DOF = int(fespaces[-1]["n_dof"])
+        self.N_Active = int(fespaces[-1]["n_active"])
+
+    def Init(self, coeff):
+        for sid in self.sids:
+            self.ctx.set_coeffs(sid, coeff)
+
+    def rhs(self):
+        r = np.zeros(self.N_DOF)
+        self.ctx.check(self.ctx.lib.cdgpu_tcd_rhs(self.ctx.h, self.tcd, _p(r)))
+        return r
+
+    def AssembleMRhs(self, sol=None):
+        self.ctx.check(self.ctx.lib.cdgpu_tcd_assemble_mass(self.ctx.h, self.tcd))
+        if sol is not None:
+            sol[self.N_Active:] = self.rhs()[self.N_Active:]
+
+    def AssembleARhs(self):
+        self.ctx.check(self.ctx.lib.cdgpu_tcd_assemble_stiffness(self.ctx.h, self.tcd))
+
+    def Step(self, sol, tau, theta1, theta2, theta3, theta4, params=None):
+        params = params or solver_params()
+        info = SolveInfo()
+        x = _f64(sol).copy()
+        self.ctx.check(self.ctx.lib.cdgpu_tcd_step(self.ctx.h, self.tcd, C.byref(params), tau, theta1,
+                                                   theta2, theta3, theta4, _p(x), C.byref(info)))
+        sol[:] = x
+        return info
+
+
 class TSystemCD2D(TSystemCD3D):
     """2D counterpart.  The reference's TSystemCD2D takes one space and has no multigrid
     branch (src/System/SystemCD2D.C:191-193); here it takes every level's space and

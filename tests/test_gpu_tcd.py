@@ -1,0 +1,119 @@
+"""Theta-scheme time stepping (TSystemTCD2D) on the GPU against the oracle.
+
+The time loop of 2DPrograms/TCD2D_ParMooN.C:241-290 -- save the old right-hand side,
+AssembleARhs, AssembleSystMat, Solve, RestoreMassMat -- runs through the C ABI and
+through the oracle's restatement (oracle.tcd_step) on the same hierarchy; every
+step's solution agrees within the FP64 solution bar.
+"""
+import numpy as np
+import pytest
+
+from parmoon_cmg_b200 import _lib, mesh
+from parmoon_cmg_b200.system import Context, TSystemTCD2D, coeffs, solver_params
+
+TOL_SOL = 1e-10
+MASS = 10
+
+
+def oracle_levels(oracle_lib, spaces, parents, dim, order):
+    levels = []
+    for l, sp in enumerate(spaces):
+        rp, kc = oracle_lib.pattern(sp["global_numbers"], sp["begin_index"], sp["n_dof"], sp["n_active"])
+        lv = dict(n_dof=sp["n_dof"], n_active=sp["n_active"], row_ptr=rp, kcol=kc)
+        if l > 0:
+            lv["p_row"], lv["p_col"], lv["p_val"] = oracle_lib.prolongation(
+                dim, order, spaces[l - 1], dict(sp), parents[l])
+        levels.append(lv)
+    return levels
+
+
+def oracle_forms(oracle_lib, spaces, levels, dim, order, disctype, co):
+    ent, rhs = [], None
+    for sp, lv in zip(spaces, levels):
+        e, rhs = oracle_lib.assemble(dim, order, disctype, sp["coords"], sp["global_numbers"],
+                                     sp["begin_index"], sp["n_dof"], sp["n_active"], lv["row_ptr"],
+                                     lv["kcol"], co)
+        ent.append(e)
+    return ent, rhs
+
+
+def test_oracle_backward_euler_reaches_steady_state(oracle_lib):
+    """Property of the oracle's restatement: implicit Euler with long steps converges to
+    the stationary solution A u = f of the same problem."""
+    spaces, parents = mesh.structured_hierarchy(2, 1, 4, 2)
+    levels = oracle_levels(oracle_lib, spaces, parents, 2, 1)
+    co = oracle_lib.coeffs(0, eps=0.1, b=(1.0, 0.5), f=1.0)
+    M, fm = oracle_forms(oracle_lib, spaces, levels, 2, 1, MASS, co)
+    A, f = oracle_forms(oracle_lib, spaces, levels, 2, 1, 1, co)
+    prm = oracle_lib.solver_params(red_factor=1e-13, restart=32, maxit=200)
+    M0 = [m.copy() for m in M]
+    u = np.zeros(spaces[-1]["n_dof"])
+    for _ in range(12):
+        u, its = oracle_lib.tcd_step(levels, M, A, f, f, u, 1e3, 1.0, 0.0, 0.0, 1.0, prm)
+        assert its >= 0
+    steady = [dict(lv, entries=a) for lv, a in zip(levels, A)]
+    us, _, _, _ = oracle_lib.solve(steady, prm, f, np.zeros_like(f))
+    assert np.abs(u - us).max() <= 1e-8 * np.abs(us).max()
+    # RestoreMassMat brings M back up to rounding
+    for m, m0 in zip(M, M0):
+        assert np.abs(m - m0).max() <= 1e-12 * np.abs(m0).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order,scheme", [(1, "crank_nicolson"), (2, "backward_euler")])
+def test_tcd_steps_vs_oracle(oracle_lib, order, scheme):
+    from parmoon_cmg_b200 import _build
+    _build.build()
+    th = dict(crank_nicolson=(0.5, 0.5, 0.5, 0.5), backward_euler=(1.0, 0.0, 0.0, 1.0))[scheme]
+    tau = 0.05
+    spaces, parents = mesh.structured_hierarchy(2, order, 4, 3)
+    ctx = Context(0)
+    try:
+        S = TSystemTCD2D(spaces, parents, ctx=ctx)
+        co_steps = [coeffs(0, eps=0.05, b=(1.0, 0.5), c=0.1, f=1.0 + 0.5 * k) for k in range(4)]
+        S.Init(co_steps[0])
+        n = spaces[-1]["n_dof"]
+        sol = np.zeros(n)
+        S.AssembleMRhs(sol)
+        levels = oracle_levels(oracle_lib, spaces, parents, 2, order)
+
+        def oco(c):
+            return oracle_lib.coeffs(0, eps=c.eps, b=(c.b1, c.b2), c=c.c, f=c.f)
+
+        M, f = oracle_forms(oracle_lib, spaces, levels, 2, order, MASS, oco(co_steps[0]))
+        assert np.abs(S.rhs() - f).max() <= 1e-12 * np.abs(f).max()
+        u = sol.copy()
+        prm_o = oracle_lib.solver_params(red_factor=1e-13, restart=32, maxit=200)
+        prm = solver_params(coarse_smoother=3, red_factor=1e-13, restart=32, maxit=200)
+        for k in range(1, 4):
+            # the right-hand side changes in time (UpdateRhs in the reference's loop)
+            for sid in S.sids:
+                ctx.set_coeffs(sid, co_steps[k])
+            f_old = f
+            S.AssembleARhs()
+            A, f = oracle_forms(oracle_lib, spaces, levels, 2, order, 1, oco(co_steps[k]))
+            info = S.Step(sol, tau, *th, params=prm)
+            assert info.status == 0
+            u, its = oracle_lib.tcd_step(levels, M, A, f_old, f, u, tau, *th, prm_o)
+            assert its >= 0
+            assert np.abs(sol - u).max() <= TOL_SOL * np.abs(u).max()
+    finally:
+        ctx.close()
+
+
+@pytest.mark.gpu
+def test_tcd_rejects_bad_use():
+    from parmoon_cmg_b200 import _build
+    _build.build()
+    spaces, parents = mesh.structured_hierarchy(2, 1, 4, 2)
+    ctx = Context(0)
+    try:
+        S = TSystemTCD2D(spaces, parents, ctx=ctx)
+        S.Init(coeffs(0, eps=1.0, f=1.0))
+        with pytest.raises(_lib.CdgpuError):
+            S.Step(np.zeros(spaces[-1]["n_dof"]), 0.1, 1.0, 0.0, 0.0, 1.0)
+        with pytest.raises(_lib.CdgpuError):
+            import ctypes as C
+            ctx.check(ctx.lib.cdgpu_tcd_create(ctx.h, S.mg, _lib.SUPG, C.byref(C.c_int())))
+    finally:
+        ctx.close()
