@@ -367,6 +367,14 @@ def run_ours(args, rank, world, local):
     else:
         hbm, peak_src = 6650.0, "fallback"
     achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
+    # DRAM bytes (read + write) of one launch of this kernel on this workload, from the ncu
+    # capture summarised in profiles/
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "csr_kernel_spmv_f64_cd3d_q2_32.md")
+    if args.n == 32 and os.path.exists(prof):
+        for line in open(prof):
+            if line.startswith("traffic_bytes_per_launch:"):
+                traffic = int(line.split(":")[1])
 
     # end to end through the public facade with host buffers: Assemble returns the
     # right-hand side to the host (drop-in behaviour), Solve copies rhs and initial guess in
@@ -412,8 +420,8 @@ def run_ours(args, rank, world, local):
         "mixed_over_fp64": value / fp64_value,
         "assembly": {"ms_all_levels": ms_asm, "mcells_per_s": n_cells_total / (ms_asm * 1e-3) / 1e6},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
-                     "kernel": "spmv_kernel<double,32> (finest level, the FGMRES matvec)",
+                     "frac": achieved / hbm, "traffic": traffic,
+                     "kernel": "csr_kernel<double,8,16,SPMV> (finest level, the FGMRES matvec)",
                      "peak_source": peak_src, "spmv_ms": spmv_ms, "algorithmic_bytes": spmv_bytes},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 16 * n,
                 "d2h_bytes_per_step": 16 * n},

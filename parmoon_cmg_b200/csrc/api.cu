@@ -205,6 +205,7 @@ static int install_pattern(cdgpu_ctx *ctx, Space &s)
   CD_CUDA(ctx, cudaMemcpy(s.d_row_ptr, s.h_row_ptr.data(), sizeof(int) * (s.n_dof + 1), cudaMemcpyHostToDevice));
   CD_CUDA(ctx, cudaMemcpy(s.d_kcol, s.h_kcol.data(), sizeof(int) * s.nnz, cudaMemcpyHostToDevice));
   CD_CUDA(ctx, cudaMemcpy(s.d_dir_start, dir_start.data(), sizeof(int) * s.n_dof, cudaMemcpyHostToDevice));
+  s.shape = csr_shape(s.h_row_ptr.data(), s.n_dof);
   // a new pattern invalidates values sized for the old one
   void **vals[] = {(void **)&s.d_a, (void **)&s.d_a32};
   for (void **p : vals)
@@ -460,6 +461,8 @@ int cdgpu_hierarchy(cdgpu_ctx *ctx, int n_levels, const int *space_ids, const in
     cudaMemcpy(L.d_r_val, rval.data(), rval.size() * sizeof(double), cudaMemcpyHostToDevice);
     cudaError_t e = cudaMemcpy(L.d_r_val32, rval32.data(), rval32.size() * sizeof(float), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) { free_mg(h); return cuda_fail(ctx, e, "hierarchy"); }
+    L.p_shape = csr_shape(row.data(), f.n_dof);
+    L.r_shape = csr_shape(rrow.data(), c.n_dof);
   }
   int rc = setup_hierarchy_buffers(ctx, *h, 30);
   if (rc) { free_mg(h); return rc; }

@@ -1,0 +1,137 @@
+// CSR kernels of the solver: matrix-vector product, defect, damped Jacobi sweep,
+// restriction and prolongation, one template with an epilogue per operation.
+//
+// A group of GS threads takes one row; each thread issues all of its U column and value
+// loads of the row (predicated on the row length) before the first x gather, so a warp
+// keeps 32*U independent loads of the matrix stream in flight regardless of where the row
+// starts.  GS follows the longest row of the matrix (csr_shape), U = 8 (16 with GS = 8); a
+// tail loop takes the entries beyond GS*U.  On the 32^3 Q2 hexahedral matrix (rows of
+// 27..125 entries) GS = 8, U = 16 gave the fastest multigrid step among warp-per-row,
+// row-tiled shared-memory and sliced-ELL forms (product alone: FP64 49 us, FP32 37 us).  Rows are visited warp by
+// warp, so every lane of a warp reaches every shuffle.  Sums are deterministic: fixed
+// order within a row, per-block partials of the defect norm in block order.
+#pragma once
+
+#include "internal.h"
+
+enum { CM_SPMV = 0, CM_DEFECT = 1, CM_JACOBI = 2, CM_RESTRICT = 3, CM_PROLONG = 4 };
+
+template <typename T> struct CsrArgs
+{
+  int n = 0, n_active = 0;
+  const int *rp = nullptr, *kc = nullptr;
+  const T *a = nullptr, *x = nullptr, *f = nullptr, *diag = nullptr;
+  T *y = nullptr, *y2 = nullptr;
+  T omega = 0;
+  double *partial = nullptr;
+};
+
+template <int G, typename T> __device__ __forceinline__ T csr_group_sum(T v)
+{
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, G);
+  return v;
+}
+
+// epilogue of row r with row sum s = (A x)_r (acc collects this thread's defect norm)
+template <typename T, int MODE>
+__device__ __forceinline__ void csr_epilogue(const CsrArgs<T> &p, int r, T s, double &acc)
+{
+  if (MODE == CM_SPMV)
+    p.y[r] = s;
+  else if (MODE == CM_DEFECT)
+  {
+    T v = p.f[r] - s;
+    p.y[r] = v;
+    acc += (double)v * (double)v;
+  }
+  else if (MODE == CM_JACOBI)
+  {
+    // x + omega D^{-1} (f - A x) = (1 - omega) x + omega (f - sum_{j != r} a_rj x_j) / a_rr
+    // (MGLevel3D.C:443-537, MGLevel2D.C:318-368); Dirichlet rows take the right-hand side
+    if (r < p.n_active)
+      p.y[r] = p.x[r] + p.omega * (p.f[r] - s) / p.diag[r];
+    else
+      p.y[r] = p.f[r];
+  }
+  else if (MODE == CM_RESTRICT)
+  {
+    // coarse rhs = R d on active rows, zero elsewhere (CorrectDefect, MGLevel3D.C:588);
+    // coarse solution reset (MGLevel3D.C:557)
+    p.y[r] = r < p.n_active ? s : T(0);
+    p.y2[r] = T(0);
+  }
+  else // CM_PROLONG: sol += damp * (P xc) on active fine rows (Update, MGLevel3D.C:539)
+  {
+    if (r < p.n_active) p.y[r] += p.omega * s;
+  }
+}
+
+template <typename T, int GS, int U, int MODE>
+__global__ void __launch_bounds__(256) csr_kernel(CsrArgs<T> p)
+{
+  constexpr int NT = 256;
+  __shared__ double red[NT / 32];
+  const int lane = threadIdx.x % GS, sub = (threadIdx.x % 32) / GS;
+  const long nwarp = (long)gridDim.x * NT / 32;
+  const int rows_end = MODE == CM_PROLONG ? p.n_active : p.n;
+  double acc = 0;
+  for (long base = ((long)blockIdx.x * NT + threadIdx.x) / 32 * (32 / GS); base < rows_end;
+       base += nwarp * (32 / GS))
+  {
+    const int r = (int)base + sub;
+    T s = 0;
+    if (r < rows_end)
+    {
+      const int b = p.rp[r], e = p.rp[r + 1];
+      int c[U];
+      T v[U];
+#pragma unroll
+      for (int i = 0; i < U; i++)
+      {
+        const int j = b + lane + i * GS;
+        c[i] = j < e ? __ldcs(p.kc + j) : -1;
+        v[i] = j < e ? __ldcs(p.a + j) : T(0);
+      }
+#pragma unroll
+      for (int i = 0; i < U; i++)
+        if (c[i] >= 0) s += v[i] * __ldg(p.x + c[i]);
+      for (int j = b + lane + U * GS; j < e; j += GS) s += p.a[j] * __ldg(p.x + p.kc[j]);
+    }
+    s = csr_group_sum<GS>(s);
+    if (r < rows_end && lane == 0) csr_epilogue<T, MODE>(p, r, s, acc);
+  }
+  if (MODE == CM_DEFECT && p.partial)
+  {
+    acc = csr_group_sum<32>(acc);
+    if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+      double tot = 0;
+      for (int w = 0; w < NT / 32; w++) tot += red[w];
+      p.partial[blockIdx.x] = tot;
+    }
+  }
+}
+
+// grid of a CSR launch: one pass over the rows, at most 8 blocks of 256 threads per SM
+inline int csr_grid(const cdgpu_ctx *ctx, const CsrShape &sh, int rows)
+{
+  const long per_block = 256 / sh.gs;
+  const long need = (rows + per_block - 1) / per_block;
+  return (int)std::max<long>(1, std::min<long>(need, (long)ctx->sm_count * 8));
+}
+
+template <typename T, int MODE>
+inline void launch_csr(cdgpu_ctx *ctx, const CsrShape &sh, const CsrArgs<T> &p, int grid)
+{
+  switch (sh.gs)
+  {
+    case 1: csr_kernel<T, 1, 8, MODE><<<grid, 256, 0, ctx->stream>>>(p); break;
+    case 2: csr_kernel<T, 2, 8, MODE><<<grid, 256, 0, ctx->stream>>>(p); break;
+    case 4: csr_kernel<T, 4, 8, MODE><<<grid, 256, 0, ctx->stream>>>(p); break;
+    case 8: csr_kernel<T, 8, 16, MODE><<<grid, 256, 0, ctx->stream>>>(p); break;
+    default: csr_kernel<T, 32, 8, MODE><<<grid, 256, 0, ctx->stream>>>(p); break;
+  }
+}

@@ -32,6 +32,16 @@ void reference_tensors(const RefElement &re, int disctype, std::vector<double> &
                        std::vector<double> &r);
 
 // ---------------------------------------------------------------------------
+// launch shape of the CSR kernels of a matrix (csr.cuh): gs threads per row, each issuing
+// up to 8 (16 when gs = 8) loads of the row at once; set from the longest row
+// ---------------------------------------------------------------------------
+struct CsrShape
+{
+  int gs = 8;
+};
+CsrShape csr_shape(const int *row_ptr, int n_rows);
+
+// ---------------------------------------------------------------------------
 // finite element space with its matrix
 // ---------------------------------------------------------------------------
 struct Space
@@ -47,6 +57,7 @@ struct Space
   std::vector<int> h_row_ptr, h_kcol;
   int *d_row_ptr = nullptr, *d_kcol = nullptr;
   int *d_dir_start = nullptr; // first slot of each row whose column is a Dirichlet DOF
+  CsrShape shape;
   // DOF -> (cell, local index) incidence, ascending cell per DOF
   int *d_inc_ptr = nullptr, *d_inc = nullptr;
   // values
@@ -86,6 +97,7 @@ struct Level
   double *d_p_val = nullptr, *d_r_val = nullptr;
   float *d_p_val32 = nullptr, *d_r_val32 = nullptr;
   long p_nnz = 0;
+  CsrShape p_shape, r_shape;
   LevelVec<double> v64, c64; // working pointers (ping-pong swapped) and their initial assignment
   LevelVec<float> v32, c32;
 };

@@ -508,3 +508,14 @@ bool dense_inverse(int n, std::vector<double> &a)
   a.swap(inv);
   return true;
 }
+
+// threads per row of the CSR kernels: 1, 2 or 4 threads (8 loads each in flight) when that
+// covers the longest row, 8 threads (16 loads each) up to 128 entries, else 32
+CsrShape csr_shape(const int *rp, int n)
+{
+  int longest = 0;
+  for (int r = 0; r < n; r++) longest = std::max(longest, rp[r + 1] - rp[r]);
+  CsrShape sh;
+  sh.gs = longest <= 8 ? 1 : longest <= 16 ? 2 : longest <= 32 ? 4 : longest <= 128 ? 8 : 32;
+  return sh;
+}

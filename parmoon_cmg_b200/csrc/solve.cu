@@ -25,143 +25,22 @@
 #include <cstring>
 
 #include "internal.h"
+#include "csr.cuh"
 
 namespace cg = cooperative_groups;
 
 static const int kBlock = 256;
 
 // ---------------------------------------------------------------------------
-// CSR kernels: one group of GS threads per row.  Rows are visited warp by warp: every
-// lane of a warp runs the same number of loop trips and reaches every shuffle, so the
-// full-warp shuffles of group_sum always see all 32 lanes (a group whose row is out of
-// range or needs no reduction contributes zeros).
+// The CSR operations (product, defect, Jacobi sweep, restriction, prolongation) are the
+// kernels of csr.cuh.  group_sum: sum over aligned groups of GS lanes; every
+// lane of the warp must call it.
 // ---------------------------------------------------------------------------
 template <int GS, typename T> __device__ __forceinline__ T group_sum(T v)
 {
 #pragma unroll
   for (int o = GS / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, GS);
   return v;
-}
-
-// partial dot of CSR row [b, e) with x for one lane of a GS-thread group; four entries per
-// lane are loaded before they are used so that more loads are in flight
-template <typename T, int GS, bool SKIP_DIAG>
-__device__ __forceinline__ T row_dot(int b, int e, int lane, int row, const int *__restrict__ kc,
-                                     const T *__restrict__ a, const T *__restrict__ x)
-{
-  T s = 0;
-  int j = b + lane;
-  for (; j + 3 * GS < e; j += 4 * GS)
-  {
-    int c0 = kc[j], c1 = kc[j + GS], c2 = kc[j + 2 * GS], c3 = kc[j + 3 * GS];
-    T a0 = a[j], a1 = a[j + GS], a2 = a[j + 2 * GS], a3 = a[j + 3 * GS];
-    T x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
-    if (SKIP_DIAG)
-    {
-      if (c0 == row) a0 = 0;
-      if (c1 == row) a1 = 0;
-      if (c2 == row) a2 = 0;
-      if (c3 == row) a3 = 0;
-    }
-    s += a0 * x0;
-    s += a1 * x1;
-    s += a2 * x2;
-    s += a3 * x3;
-  }
-  for (; j < e; j += GS)
-  {
-    int c = kc[j];
-    T v = a[j];
-    if (SKIP_DIAG && c == row) v = 0;
-    s += v * __ldg(x + c);
-  }
-  return s;
-}
-
-#define CD_WARP_ROWS(n)                                                                      \
-  const int lane = threadIdx.x % GS, sub = (threadIdx.x % 32) / GS;                          \
-  const long nwarp = (long)gridDim.x * blockDim.x / 32;                                      \
-  for (long base = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32 * (32 / GS); base < (n); \
-       base += nwarp * (32 / GS))
-
-template <typename T, int GS>
-__global__ void __launch_bounds__(kBlock) spmv_kernel(int n, const int *__restrict__ rp,
-                                                      const int *__restrict__ kc,
-                                                      const T *__restrict__ a,
-                                                      const T *__restrict__ x, T *__restrict__ y)
-{
-  CD_WARP_ROWS(n)
-  {
-    const int r = (int)base + sub;
-    T s = 0;
-    if (r < n) s = row_dot<T, GS, false>(rp[r], rp[r + 1], lane, r, kc, a, x);
-    s = group_sum<GS>(s);
-    if (r < n && lane == 0) y[r] = s;
-  }
-}
-
-// d = f - A x, and per-block partial sums of d^2 (fixed order -> deterministic)
-template <typename T, int GS>
-__global__ void __launch_bounds__(kBlock) defect_kernel(int n, const int *__restrict__ rp,
-                                                        const int *__restrict__ kc,
-                                                        const T *__restrict__ a,
-                                                        const T *__restrict__ x,
-                                                        const T *__restrict__ f, T *__restrict__ d,
-                                                        double *__restrict__ partial)
-{
-  __shared__ double red[kBlock / GS];
-  double acc = 0;
-  CD_WARP_ROWS(n)
-  {
-    const int r = (int)base + sub;
-    T s = 0;
-    if (r < n) s = row_dot<T, GS, false>(rp[r], rp[r + 1], lane, r, kc, a, x);
-    s = group_sum<GS>(s);
-    if (r < n && lane == 0)
-    {
-      T v = f[r] - s;
-      d[r] = v;
-      acc += (double)v * (double)v;
-    }
-  }
-  if (partial)
-  {
-    if (lane == 0) red[threadIdx.x / GS] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0)
-    {
-      double t = 0;
-      for (int g = 0; g < kBlock / GS; g++) t += red[g];
-      partial[blockIdx.x] = t;
-    }
-  }
-}
-
-// damped Jacobi sweep (MGLevel3D.C:443-537 / MGLevel2D.C:318-368) from x_in into x_out
-template <typename T, int GS>
-__global__ void __launch_bounds__(kBlock) jacobi_kernel(int n, int n_active,
-                                                        const int *__restrict__ rp,
-                                                        const int *__restrict__ kc,
-                                                        const T *__restrict__ a,
-                                                        const T *__restrict__ diag,
-                                                        const T *__restrict__ x,
-                                                        const T *__restrict__ f,
-                                                        T *__restrict__ xo, T omega)
-{
-  CD_WARP_ROWS(n)
-  {
-    const int r = (int)base + sub;
-    T s = 0;
-    if (r < n_active) s = row_dot<T, GS, true>(rp[r], rp[r + 1], lane, r, kc, a, x);
-    s = group_sum<GS>(s);
-    if (r < n && lane == 0)
-    {
-      if (r >= n_active)
-        xo[r] = f[r]; // Dirichlet rows take the right-hand side
-      else
-        xo[r] = (T(1) - omega) * x[r] + omega * (f[r] - s) / diag[r];
-    }
-  }
 }
 
 // first sweep when the active part of x is zero: only Dirichlet columns (numbered last,
@@ -182,62 +61,32 @@ __global__ void jacobi_first_kernel(int n, int n_active, const int *__restrict__
   xo[r] = omega * s / diag[r];
 }
 
-// coarse right-hand side = R d, zero on non-active rows (CorrectDefect, MGLevel3D.C:588),
-// coarse solution reset to zero (MGLevel3D.C:557)
-template <typename T, int GS>
-__global__ void __launch_bounds__(kBlock) restrict_kernel(int nc, int nc_active,
-                                                          const int *__restrict__ rr,
-                                                          const int *__restrict__ rc,
-                                                          const T *__restrict__ rv,
-                                                          const T *__restrict__ d,
-                                                          T *__restrict__ crhs, T *__restrict__ csol)
-{
-  CD_WARP_ROWS(nc)
-  {
-    const int r = (int)base + sub;
-    T s = 0;
-    if (r < nc_active)
-      for (int j = rr[r] + lane; j < rr[r + 1]; j += GS) s += rv[j] * __ldg(d + rc[j]);
-    s = group_sum<GS>(s);
-    if (r < nc && lane == 0) { crhs[r] = s; csol[r] = 0; }
-  }
-}
-
-// sol += damp * (P xc) on active rows; the correction of Dirichlet rows is zeroed
-// (CorrectNodes, MGLevel3D.C:562) so they are left unchanged (Update, MGLevel3D.C:539)
-template <typename T, int GS>
-__global__ void __launch_bounds__(kBlock) prolong_kernel(int nf, int nf_active,
-                                                         const int *__restrict__ pr,
-                                                         const int *__restrict__ pc,
-                                                         const T *__restrict__ pv,
-                                                         const T *__restrict__ xc,
-                                                         T *__restrict__ sol, T damp)
-{
-  CD_WARP_ROWS(nf_active)
-  {
-    const int r = (int)base + sub;
-    T s = 0;
-    if (r < nf_active)
-      for (int j = pr[r] + lane; j < pr[r + 1]; j += GS) s += pv[j] * __ldg(xc + pc[j]);
-    s = group_sum<GS>(s);
-    if (r < nf_active && lane == 0) sol[r] += damp * s;
-  }
-}
-
-// exact coarse solve with the explicit FP64 inverse of the whole coarse matrix
-// (Dirichlet identity rows included, like SolveExact, MGLevel3D.C:839)
+// exact coarse solve (SolveExact, MGLevel3D.C:839) with the explicit FP64 inverse of the
+// active block: Dirichlet rows are identity rows, so sol_D = rhs_D and
+// sol_A = inv(A_AA) (rhs_A - A_AD rhs_D); A_AD is read from the CSR values of each active
+// row from its first Dirichlet column (dir_start) on.
 template <typename T>
-__global__ void coarse_exact_kernel(int n, const double *__restrict__ cinv, const T *__restrict__ rhs,
+__global__ void coarse_exact_kernel(int n, int na, const int *__restrict__ rp, const int *__restrict__ kc,
+                                    const int *__restrict__ dir_start, const double *__restrict__ a,
+                                    const double *__restrict__ cinv, const T *__restrict__ rhs,
                                     T *__restrict__ sol)
 {
   extern __shared__ double b[];
   for (int i = threadIdx.x; i < n; i += blockDim.x) b[i] = (double)rhs[i];
   __syncthreads();
+  for (int i = threadIdx.x; i < na; i += blockDim.x)
+  {
+    double v = b[i];
+    for (int j = dir_start[i]; j < rp[i + 1]; j++) v -= a[j] * b[kc[j]];
+    b[n + i] = v;
+  }
+  for (int i = na + threadIdx.x; i < n; i += blockDim.x) sol[i] = (T)b[i];
+  __syncthreads();
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nw = blockDim.x / 32;
-  for (int r = warp; r < n; r += nw)
+  for (int r = warp; r < na; r += nw)
   {
     double s = 0;
-    for (int j = lane; j < n; j += 32) s += cinv[(size_t)r * n + j] * b[j];
+    for (int j = lane; j < na; j += 32) s += cinv[(size_t)r * na + j] * b[n + j];
     s = group_sum<32>(s);
     if (lane == 0) sol[r] = (T)s;
   }
@@ -506,32 +355,6 @@ __global__ void mg_finish_kernel(int n, const T *__restrict__ sol, double *const
 // ---------------------------------------------------------------------------
 // launch helpers
 // ---------------------------------------------------------------------------
-static int grid_for(cdgpu_ctx *ctx, long rows, int gs)
-{
-  long groups_per_block = kBlock / gs;
-  long need = (rows + groups_per_block - 1) / groups_per_block;
-  long cap = (long)ctx->sm_count * (2048 / kBlock);
-  return (int)std::max<long>(1, std::min(need, cap));
-}
-
-static int group_size(const Space &s)
-{
-  if (s.dim == 3 && s.order == 2) return 32;
-  if (s.dim == 3 || s.order == 2) return 16;
-  return 8;
-}
-
-#define GS_DISPATCH(gs, KERNEL, ...)                 \
-  do {                                               \
-    switch (gs)                                      \
-    {                                                \
-      case 32: KERNEL<32> __VA_ARGS__; break;        \
-      case 16: KERNEL<16> __VA_ARGS__; break;        \
-      case 8: KERNEL<8> __VA_ARGS__; break;          \
-      default: KERNEL<4> __VA_ARGS__; break;         \
-    }                                                \
-  } while (0)
-
 template <typename T> static const T *mat(const Space &s);
 template <> const double *mat<double>(const Space &s) { return s.d_a; }
 template <> const float *mat<float>(const Space &s) { return s.d_a32; }
@@ -551,37 +374,78 @@ template <typename T> static LevelVec<T> &canon(Level &l);
 template <> LevelVec<double> &canon<double>(Level &l) { return l.c64; }
 template <> LevelVec<float> &canon<float>(Level &l) { return l.c32; }
 
-template <typename T, int GS>
-static void launch_jacobi(cdgpu_ctx *ctx, const Space &s, const T *x, const T *f, T *xo, T omega)
+// the CSR operations of the solver (csr.cuh)
+template <typename T> static CsrArgs<T> csr_args(const Space &s, const T *x)
 {
-  jacobi_kernel<T, GS><<<grid_for(ctx, s.n_dof, GS), kBlock, 0, ctx->stream>>>(
-      s.n_dof, s.n_active, s.d_row_ptr, s.d_kcol, mat<T>(s), dg<T>(s), x, f, xo, omega);
+  CsrArgs<T> p;
+  p.n = s.n_dof;
+  p.n_active = s.n_active;
+  p.rp = s.d_row_ptr;
+  p.kc = s.d_kcol;
+  p.a = mat<T>(s);
+  p.x = x;
+  return p;
 }
-template <typename T, int GS>
-static void launch_defect(cdgpu_ctx *ctx, const Space &s, const T *x, const T *f, T *d, double *partial,
-                          int grid)
+template <typename T> static void csr_jacobi(cdgpu_ctx *ctx, const Space &s, const T *x, const T *f, T *xo, T omega)
 {
-  defect_kernel<T, GS><<<grid, kBlock, 0, ctx->stream>>>(s.n_dof, s.d_row_ptr, s.d_kcol, mat<T>(s), x,
-                                                         f, d, partial);
+  CsrArgs<T> p = csr_args<T>(s, x);
+  p.f = f;
+  p.diag = dg<T>(s);
+  p.y = xo;
+  p.omega = omega;
+  launch_csr<T, CM_JACOBI>(ctx, s.shape, p, csr_grid(ctx, s.shape, s.n_dof));
 }
-template <typename T, int GS>
-static void launch_spmv(cdgpu_ctx *ctx, const Space &s, const T *x, T *y)
+template <typename T>
+static void csr_defect(cdgpu_ctx *ctx, const Space &s, const T *x, const T *f, T *d, double *partial, int grid)
 {
-  spmv_kernel<T, GS><<<grid_for(ctx, s.n_dof, GS), kBlock, 0, ctx->stream>>>(
-      s.n_dof, s.d_row_ptr, s.d_kcol, mat<T>(s), x, y);
+  CsrArgs<T> p = csr_args<T>(s, x);
+  p.f = f;
+  p.y = d;
+  p.partial = partial;
+  launch_csr<T, CM_DEFECT>(ctx, s.shape, p, grid);
+}
+template <typename T> static void csr_spmv(cdgpu_ctx *ctx, const Space &s, const T *x, T *y)
+{
+  CsrArgs<T> p = csr_args<T>(s, x);
+  p.y = y;
+  launch_csr<T, CM_SPMV>(ctx, s.shape, p, csr_grid(ctx, s.shape, s.n_dof));
+}
+// coarse rhs = R d (zero on non-active coarse rows), coarse solution reset
+template <typename T>
+static void csr_restrict(cdgpu_ctx *ctx, const Level &L, const Space &sc, const T *d, T *crhs, T *csol)
+{
+  CsrArgs<T> p;
+  p.n = sc.n_dof;
+  p.n_active = sc.n_active;
+  p.rp = L.d_r_row;
+  p.kc = L.d_r_col;
+  p.a = rval<T>(L);
+  p.x = d;
+  p.y = crhs;
+  p.y2 = csol;
+  launch_csr<T, CM_RESTRICT>(ctx, L.r_shape, p, csr_grid(ctx, L.r_shape, p.n));
+}
+// sol += damp * P xc on active fine rows
+template <typename T>
+static void csr_prolong(cdgpu_ctx *ctx, const Level &L, const Space &s, const T *xc, T *sol, T damp)
+{
+  CsrArgs<T> p;
+  p.n = s.n_dof;
+  p.n_active = s.n_active;
+  p.rp = L.d_p_row;
+  p.kc = L.d_p_col;
+  p.a = pval<T>(L);
+  p.x = xc;
+  p.y = sol;
+  p.omega = damp;
+  launch_csr<T, CM_PROLONG>(ctx, L.p_shape, p, csr_grid(ctx, L.p_shape, p.n_active));
 }
 
 template <typename T> static int jacobi_sweep(cdgpu_ctx *ctx, Level &L, T omega)
 {
   LevelVec<T> &v = vecs<T>(L);
   const Space &s = *L.sp;
-  int gs = group_size(s);
-  switch (gs)
-  {
-    case 32: launch_jacobi<T, 32>(ctx, s, v.sol, v.rhs, v.alt, omega); break;
-    case 16: launch_jacobi<T, 16>(ctx, s, v.sol, v.rhs, v.alt, omega); break;
-    default: launch_jacobi<T, 8>(ctx, s, v.sol, v.rhs, v.alt, omega); break;
-  }
+  csr_jacobi<T>(ctx, s, v.sol, v.rhs, v.alt, omega);
   CD_LAUNCHED(ctx);
   std::swap(v.sol, v.alt);
   return CDGPU_OK;
@@ -634,8 +498,9 @@ template <typename T> static int coarse_solve(cdgpu_ctx *ctx, Hierarchy &h, Cycl
   LevelVec<T> &v = vecs<T>(L);
   if (cs.p->coarse_smoother == 17)
   {
-    size_t sm = sizeof(double) * s.n_dof;
-    coarse_exact_kernel<T><<<1, 1024, sm, ctx->stream>>>(s.n_dof, h.d_cinv, v.rhs, v.sol);
+    size_t sm = sizeof(double) * (s.n_dof + s.n_active);
+    coarse_exact_kernel<T><<<1, 1024, sm, ctx->stream>>>(s.n_dof, s.n_active, s.d_row_ptr, s.d_kcol,
+                                                         s.d_dir_start, s.d_a, h.d_cinv, v.rhs, v.sol);
     CD_LAUNCHED(ctx);
   }
   else
@@ -659,23 +524,15 @@ template <typename T> static int cycle(cdgpu_ctx *ctx, Hierarchy &h, CycleState 
   LevelVec<T> &v = vecs<T>(L), &vc = vecs<T>(C);
   int rc;
   if ((rc = smooth<T>(ctx, h, cs, i, cs.p->pre))) return rc;
-  int gs = group_size(s);
-  switch (gs)
-  {
-    case 32: launch_defect<T, 32>(ctx, s, v.sol, v.rhs, v.def, nullptr, grid_for(ctx, s.n_dof, 32)); break;
-    case 16: launch_defect<T, 16>(ctx, s, v.sol, v.rhs, v.def, nullptr, grid_for(ctx, s.n_dof, 16)); break;
-    default: launch_defect<T, 8>(ctx, s, v.sol, v.rhs, v.def, nullptr, grid_for(ctx, s.n_dof, 8)); break;
-  }
+  csr_defect<T>(ctx, s, v.sol, v.rhs, v.def, nullptr, csr_grid(ctx, s.shape, s.n_dof));
   CD_LAUNCHED(ctx);
-  restrict_kernel<T, 16><<<grid_for(ctx, sc.n_dof, 16), kBlock, 0, ctx->stream>>>(
-      sc.n_dof, sc.n_active, L.d_r_row, L.d_r_col, rval<T>(L), v.def, vc.rhs, vc.sol);
+  csr_restrict<T>(ctx, L, sc, v.def, vc.rhs, vc.sol);
   CD_LAUNCHED(ctx);
   cs.sol_zero[i - 1] = cs.active_zero[i - 1] = true;
   for (int j = 0; j < cs.rec[i]; j++)
     if ((rc = cycle<T>(ctx, h, cs, i - 1))) return rc;
   if (cs.p->cycle < 1) cs.rec[i] = 1;
-  prolong_kernel<T, 8><<<grid_for(ctx, s.n_active, 8), kBlock, 0, ctx->stream>>>(
-      s.n_dof, s.n_active, L.d_p_row, L.d_p_col, pval<T>(L), vc.sol, v.sol, (T)cs.p->gmg_damp);
+  csr_prolong<T>(ctx, L, s, vc.sol, v.sol, (T)cs.p->gmg_damp);
   CD_LAUNCHED(ctx);
   return smooth<T>(ctx, h, cs, i, cs.p->post);
 }
@@ -725,7 +582,7 @@ static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, 
     if (h.gexec[k]) { cudaGraphExecDestroy(h.gexec[k]); h.gexec[k] = nullptr; }
     // dynamic shared memory of the coarse kernels is set outside the capture
     const int nc = h.lev[0].sp->n_dof;
-    const int sm1 = (int)(sizeof(double) * nc), sm2 = 2 * sm1;
+    const int sm1 = (int)(sizeof(double) * (nc + h.lev[0].sp->n_active)), sm2 = (int)(2 * sizeof(double) * nc);
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_exact_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm1));
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_exact_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm1));
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_smooth_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm2));
@@ -800,13 +657,15 @@ int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m)
   return CDGPU_OK;
 }
 
-__global__ void csr_to_dense_kernel(int n, const int *__restrict__ rp, const int *__restrict__ kc,
+// dense copy of the active block A_AA (rows and columns below na) of a CSR matrix
+__global__ void csr_to_dense_kernel(int na, const int *__restrict__ rp, const int *__restrict__ kc,
                                     const double *__restrict__ a, double *__restrict__ dense)
 {
   int r = blockIdx.x;
-  for (int c = threadIdx.x; c < n; c += blockDim.x) dense[(size_t)r * n + c] = 0.0;
+  for (int c = threadIdx.x; c < na; c += blockDim.x) dense[(size_t)r * na + c] = 0.0;
   __syncthreads();
-  for (int j = rp[r] + threadIdx.x; j < rp[r + 1]; j += blockDim.x) dense[(size_t)r * n + kc[j]] = a[j];
+  for (int j = rp[r] + threadIdx.x; j < rp[r + 1]; j += blockDim.x)
+    if (kc[j] < na) dense[(size_t)r * na + kc[j]] = a[j];
 }
 
 // In-place Gauss-Jordan inversion with partial (row) pivoting, one CTA; the matrix lives in
@@ -869,12 +728,13 @@ __global__ void __launch_bounds__(1024) gj_invert_kernel(int n, double *__restri
     __syncthreads();
     // eliminate column k from the other rows: first every column but k (which holds the
     // multipliers), then column k itself
-    for (int e = t; e < n * n; e += nt)
+    for (int i = warp; i < n; i += nt / 32)
     {
-      int i = e / n, j = e % n;
-      if (i == k || j == k) continue;
-      double f = A[(size_t)i * n + k];
-      if (f != 0.0) A[(size_t)i * n + j] -= f * A[(size_t)k * n + j];
+      if (i == k) continue;
+      const double f = A[(size_t)i * n + k];
+      if (f == 0.0) continue;
+      for (int j = lane; j < n; j += 32)
+        if (j != k) A[(size_t)i * n + j] -= f * A[(size_t)k * n + j];
     }
     __syncthreads();
     for (int i = t; i < n; i += nt)
@@ -902,25 +762,30 @@ static int refresh_coarse_inverse(cdgpu_ctx *ctx, Hierarchy &h)
 {
   Space &s = *h.lev[0].sp;
   if (h.d_cinv && h.cinv_version == s.assembly_version) return CDGPU_OK;
-  int n = s.n_dof;
-  if (n > 4096) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "exact coarse solve: coarsest level larger than 4096 DOFs");
+  const int na = s.n_active;
+  if (na > 4096)
+    return fail(ctx, CDGPU_ERR_UNSUPPORTED, "exact coarse solve: more than 4096 active DOFs on the coarsest level");
   int rc;
   if (h.cinv_version < 0 || !h.d_cinv)
   {
-    if ((rc = dev_alloc(ctx, &h.d_cinv, (size_t)n * n)) || (rc = dev_alloc(ctx, &h.d_cpiv, n + 1)))
+    if ((rc = dev_alloc(ctx, &h.d_cinv, (size_t)na * na)) || (rc = dev_alloc(ctx, &h.d_cpiv, na + 1)))
       return rc;
   }
-  csr_to_dense_kernel<<<n, 128, 0, ctx->stream>>>(n, s.d_row_ptr, s.d_kcol, s.d_a, h.d_cinv);
-  CD_LAUNCHED(ctx);
-  size_t sm = sizeof(double) * (size_t)n * n;
-  int use_smem = sm <= 200 * 1024;
-  if (use_smem)
-    CD_CUDA(ctx, cudaFuncSetAttribute(gj_invert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  CD_CUDA(ctx, cudaMemsetAsync(h.d_cpiv + n, 0, sizeof(int), ctx->stream));
-  gj_invert_kernel<<<1, 1024, use_smem ? sm : 0, ctx->stream>>>(n, h.d_cinv, use_smem, h.d_cpiv, h.d_cpiv + n);
-  CD_LAUNCHED(ctx);
+  CD_CUDA(ctx, cudaMemsetAsync(h.d_cpiv + na, 0, sizeof(int), ctx->stream));
+  if (na > 0)
+  {
+    csr_to_dense_kernel<<<na, 128, 0, ctx->stream>>>(na, s.d_row_ptr, s.d_kcol, s.d_a, h.d_cinv);
+    CD_LAUNCHED(ctx);
+    size_t sm = sizeof(double) * (size_t)na * na;
+    int use_smem = sm <= 200 * 1024;
+    if (use_smem)
+      CD_CUDA(ctx, cudaFuncSetAttribute(gj_invert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    gj_invert_kernel<<<1, 1024, use_smem ? sm : 0, ctx->stream>>>(na, h.d_cinv, use_smem, h.d_cpiv,
+                                                                  h.d_cpiv + na);
+    CD_LAUNCHED(ctx);
+  }
   int flag = 0;
-  CD_CUDA(ctx, cudaMemcpyAsync(&flag, h.d_cpiv + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CD_CUDA(ctx, cudaMemcpyAsync(&flag, h.d_cpiv + na, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (flag) return fail(ctx, CDGPU_ERR_INVALID, "exact coarse solve: singular coarse matrix");
   h.cinv_version = s.assembly_version;
@@ -934,14 +799,8 @@ static int finest_defect_norm(cdgpu_ctx *ctx, Hierarchy &h, const double *x, con
                               double *norm_out_dev)
 {
   const Space &s = *h.lev.back().sp;
-  int gs = group_size(s);
-  int grid = std::min(grid_for(ctx, s.n_dof, gs), ctx->sm_count * 8);
-  switch (gs)
-  {
-    case 32: launch_defect<double, 32>(ctx, s, x, f, d, h.d_partial, grid); break;
-    case 16: launch_defect<double, 16>(ctx, s, x, f, d, h.d_partial, grid); break;
-    default: launch_defect<double, 8>(ctx, s, x, f, d, h.d_partial, grid); break;
-  }
+  const int grid = csr_grid(ctx, s.shape, s.n_dof); // <= 8 blocks per SM, within d_partial
+  csr_defect<double>(ctx, s, x, f, d, h.d_partial, grid);
   CD_LAUNCHED(ctx);
   sum_blocks_kernel<<<1, 256, 0, ctx->stream>>>(grid, h.d_partial, norm_out_dev);
   CD_LAUNCHED(ctx);
@@ -950,29 +809,18 @@ static int finest_defect_norm(cdgpu_ctx *ctx, Hierarchy &h, const double *x, con
 
 int spmv64(cdgpu_ctx *ctx, const Space &s, const double *x, double *y)
 {
-  int gs = group_size(s);
-  switch (gs)
-  {
-    case 32: launch_spmv<double, 32>(ctx, s, x, y); break;
-    case 16: launch_spmv<double, 16>(ctx, s, x, y); break;
-    default: launch_spmv<double, 8>(ctx, s, x, y); break;
-  }
+  csr_spmv<double>(ctx, s, x, y);
   CD_LAUNCHED(ctx);
   return CDGPU_OK;
 }
 
 int defect64(cdgpu_ctx *ctx, const Space &s, const double *x, const double *f, double *d, double *res)
 {
-  int gs = group_size(s), rc;
-  int grid = std::min(grid_for(ctx, s.n_dof, gs), ctx->sm_count * 8);
+  int rc;
+  const int grid = csr_grid(ctx, s.shape, s.n_dof);
   double *partial = nullptr, *out = nullptr;
   if ((rc = dev_alloc(ctx, &partial, grid)) || (rc = dev_alloc(ctx, &out, 1))) return rc;
-  switch (gs)
-  {
-    case 32: launch_defect<double, 32>(ctx, s, x, f, d, partial, grid); break;
-    case 16: launch_defect<double, 16>(ctx, s, x, f, d, partial, grid); break;
-    default: launch_defect<double, 8>(ctx, s, x, f, d, partial, grid); break;
-  }
+  csr_defect<double>(ctx, s, x, f, d, partial, grid);
   CD_LAUNCHED(ctx);
   sum_blocks_kernel<<<1, 256, 0, ctx->stream>>>(grid, partial, out);
   CD_LAUNCHED(ctx);
