@@ -226,6 +226,47 @@ int cdgpu_tcd_step_device(cdgpu_ctx *ctx, int tcd_id, const cdgpu_solver_params 
                           cdgpu_solve_info *info);
 int cdgpu_tcd_rhs(cdgpu_ctx *ctx, int tcd_id, double *h_rhs);
 
+/* --- batched solves and serving ---------------------------------------------
+ * No single reference function: the reference solves one system per process
+ * (TSystemCD2D/3D::Solve).  A batch runs many independent solves of the GMG-FGMRES kind of
+ * cdgpu_solve at once: every kernel launch of an FGMRES iteration serves all running
+ * instances (grouped launches, one thread block range per instance), and the FGMRES
+ * control (Givens rotations, stopping tests, restarts) runs on the device per instance, so
+ * instances at different iterations, of different sizes, orders and dimensions share the
+ * launches.  Instances can be submitted while others run (they start at the next
+ * iteration) and released when done, which is how a request loop admits new solves as
+ * memory frees up.
+ *
+ * The mesh structure (pattern, transfer operators, colour classes) comes from a hierarchy
+ * built with cdgpu_hierarchy and is shared by every instance that names it; each instance
+ * owns its coefficients, matrices on every level (FP64 and FP32), multigrid vectors and
+ * Krylov workspace.  The multigrid cycle runs in FP32 inside FP64 FGMRES (the mixed form of
+ * cdgpu_solve) with the exact FP64 coarse solve.  params->smoother: 1 damped Jacobi
+ * (MGLevel3D.C:443), 2 multicolour SOR, 3 multicolour SSOR (the colouring is a greedy
+ * colouring of the matrix graph, so SOR/SSOR sweep the rows colour by colour rather than in
+ * the reference's lexicographic order).  params->coarse_smoother must be 17 (exact).
+ * stop_rule, red_factor, res_norm_min, maxit, restart (<= 32) as for cdgpu_solve. */
+int cdgpu_batch_create(cdgpu_ctx *ctx, const cdgpu_solver_params *params, int *batch_id);
+/* add one instance: coefficients co on every level of hierarchy mg_id, assembled with
+ * disctype on the finest level and coarse_disctype on the others (Dirichlet values 0),
+ * initial guess 0; the instance joins at the next cdgpu_batch_advance.  *slot identifies
+ * it until cdgpu_batch_release. */
+int cdgpu_batch_submit(cdgpu_ctx *ctx, int batch_id, int mg_id, const cdgpu_coeffs *co, int disctype,
+                       int coarse_disctype, int *slot);
+/* run up to `iterations` FGMRES iterations of every running instance; *running (nullable)
+ * = instances still running afterwards */
+int cdgpu_batch_advance(cdgpu_ctx *ctx, int batch_id, int iterations, int *running);
+/* slots that finished since the last poll (at most max_slots; *count = how many) */
+int cdgpu_batch_poll(cdgpu_ctx *ctx, int batch_id, int *slots, int max_slots, int *count);
+/* solution (finest level, n_dof values) and statistics of a finished instance */
+int cdgpu_batch_fetch(cdgpu_ctx *ctx, int batch_id, int slot, double *h_sol, cdgpu_solve_info *info);
+/* free an instance's device memory (finished or not); the slot number may be reused */
+int cdgpu_batch_release(cdgpu_ctx *ctx, int batch_id, int slot);
+/* device bytes held by the batch's instances (for admission under a memory budget) */
+int cdgpu_batch_memory(cdgpu_ctx *ctx, int batch_id, unsigned long long *bytes);
+/* device bytes one instance on hierarchy mg_id would take */
+int cdgpu_batch_instance_bytes(cdgpu_ctx *ctx, int batch_id, int mg_id, unsigned long long *bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -79,6 +79,14 @@ SIGNATURES = {
     "cdgpu_tcd_step_device": (_I, [_P, _I, C.POINTER(SolverParams), C.c_double, C.c_double,
                                    C.c_double, C.c_double, C.c_double, _P, C.POINTER(SolveInfo)]),
     "cdgpu_tcd_rhs": (_I, [_P, _I, _P]),
+    "cdgpu_batch_create": (_I, [_P, C.POINTER(SolverParams), C.POINTER(_I)]),
+    "cdgpu_batch_submit": (_I, [_P, _I, _I, C.POINTER(Coeffs), _I, _I, C.POINTER(_I)]),
+    "cdgpu_batch_advance": (_I, [_P, _I, _I, C.POINTER(_I)]),
+    "cdgpu_batch_poll": (_I, [_P, _I, _P, _I, C.POINTER(_I)]),
+    "cdgpu_batch_fetch": (_I, [_P, _I, _I, _P, C.POINTER(SolveInfo)]),
+    "cdgpu_batch_release": (_I, [_P, _I, _I]),
+    "cdgpu_batch_memory": (_I, [_P, _I, C.POINTER(C.c_ulonglong)]),
+    "cdgpu_batch_instance_bytes": (_I, [_P, _I, _I, C.POINTER(C.c_ulonglong)]),
 }
 
 _lib = None

@@ -46,7 +46,7 @@ static void free_mg(Hierarchy *h)
   for (auto &L : h->lev)
   {
     void *ptrs[] = {L.d_p_row, L.d_p_col, L.d_r_row, L.d_r_col, L.d_p_val, L.d_r_val, L.d_p_val32,
-                    L.d_r_val32, L.c64.sol, L.c64.alt, L.c64.rhs, L.c64.def, L.c32.sol, L.c32.alt,
+                    L.d_r_val32, L.d_color_rows, L.c64.sol, L.c64.alt, L.c64.rhs, L.c64.def, L.c32.sol, L.c32.alt,
                     L.c32.rhs, L.c32.def};
     for (void *p : ptrs)
       if (p) cudaFree(p);
@@ -94,6 +94,7 @@ void cdgpu_destroy(cdgpu_ctx *ctx)
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   for (auto *t : ctx->tcds) free_tcd(t);
+  for (auto *b : ctx->batches) free_batch(b);
   for (auto *h : ctx->mgs) free_mg(h);
   for (auto *s : ctx->spaces) free_space(s);
   if (ctx->d_err) cudaFree(ctx->d_err);

@@ -98,6 +98,12 @@ struct Level
   float *d_p_val32 = nullptr, *d_r_val32 = nullptr;
   long p_nnz = 0;
   CsrShape p_shape, r_shape;
+  // colour classes of the active rows (greedy distance-1 colouring of the matrix graph) for
+  // the multicolour SOR/SSOR smoothers of the batched solver: rows of colour c are
+  // d_color_rows[h_color_ptr[c] .. h_color_ptr[c+1])
+  int n_colors = -1;
+  std::vector<int> h_color_ptr;
+  int *d_color_rows = nullptr;
   LevelVec<double> v64, c64; // working pointers (ping-pong swapped) and their initial assignment
   LevelVec<float> v32, c32;
 };
@@ -128,10 +134,13 @@ struct Hierarchy
 // ---------------------------------------------------------------------------
 struct Tcd; // time-dependent system (tcd.cu)
 void free_tcd(Tcd *t);
+struct Batch; // batched solves (batch.cu)
+void free_batch(Batch *b);
 
 struct cdgpu_ctx
 {
   std::vector<Tcd *> tcds;
+  std::vector<Batch *> batches;
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;

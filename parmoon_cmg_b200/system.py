@@ -301,3 +301,80 @@ class TSystemCD2D(TSystemCD3D):
     solves with the same multigrid-preconditioned FGMRES as the 3D system."""
 
     dim = 2
+
+
+class Batch:
+    """Many independent GMG-FGMRES solves advanced together on one GPU (cdgpu_batch_*).
+
+    ``add_structure`` registers a mesh hierarchy once (pattern, transfers, colour classes);
+    ``submit`` adds an instance on a structure with its own coefficients (assembled on
+    submission); ``advance`` runs FGMRES iterations of every running instance in grouped
+    launches; ``poll`` returns the instances that finished; ``fetch`` reads a solution;
+    ``release`` frees an instance's device memory.  The multigrid cycle runs in FP32
+    inside FP64 FGMRES with the exact FP64 coarse solve."""
+
+    def __init__(self, params, ctx=None):
+        self.ctx = ctx or Context()
+        bid = C.c_int()
+        self.ctx.check(self.ctx.lib.cdgpu_batch_create(self.ctx.h, C.byref(params), C.byref(bid)))
+        self.id = bid.value
+        self.structures = []
+
+    def add_structure(self, spaces, parents):
+        """Upload a hierarchy (spaces coarsest first); returns its structure id."""
+        sids = [self.ctx.upload_space(s) for s in spaces]
+        for sid in sids:
+            self.ctx.build_pattern(sid)
+        mg = self.ctx.hierarchy(sids, parents)
+        self.structures.append(dict(mg=mg, n_dof=int(spaces[-1]["n_dof"]), sids=sids))
+        return len(self.structures) - 1
+
+    def instance_bytes(self, structure):
+        out = C.c_ulonglong()
+        self.ctx.check(self.ctx.lib.cdgpu_batch_instance_bytes(self.ctx.h, self.id,
+                                                               self.structures[structure]["mg"],
+                                                               C.byref(out)))
+        return out.value
+
+    def submit(self, structure, coeff, disctype=SUPG, coarse_disctype=None):
+        slot = C.c_int()
+        st = self.structures[structure]
+        cd = disctype if coarse_disctype is None else coarse_disctype
+        self.ctx.check(self.ctx.lib.cdgpu_batch_submit(self.ctx.h, self.id, st["mg"], C.byref(coeff),
+                                                       disctype, cd, C.byref(slot)))
+        return slot.value
+
+    def advance(self, iterations=1):
+        running = C.c_int()
+        self.ctx.check(self.ctx.lib.cdgpu_batch_advance(self.ctx.h, self.id, iterations, C.byref(running)))
+        return running.value
+
+    def poll(self, max_slots=65536):
+        buf = (C.c_int * max_slots)()
+        cnt = C.c_int()
+        self.ctx.check(self.ctx.lib.cdgpu_batch_poll(self.ctx.h, self.id, C.cast(buf, C.c_void_p), max_slots,
+                                                     C.byref(cnt)))
+        return list(buf[:cnt.value])
+
+    def fetch(self, slot, n_dof):
+        x = np.zeros(n_dof)
+        info = SolveInfo()
+        self.ctx.check(self.ctx.lib.cdgpu_batch_fetch(self.ctx.h, self.id, slot, _p(x), C.byref(info)))
+        return x, info
+
+    def release(self, slot):
+        self.ctx.check(self.ctx.lib.cdgpu_batch_release(self.ctx.h, self.id, slot))
+
+    def memory(self):
+        out = C.c_ulonglong()
+        self.ctx.check(self.ctx.lib.cdgpu_batch_memory(self.ctx.h, self.id, C.byref(out)))
+        return out.value
+
+    def run(self, iterations_per_poll=8):
+        """Advance until no instance is running; returns the finished slots in order."""
+        done = []
+        while True:
+            running = self.advance(iterations_per_poll)
+            done += self.poll()
+            if running == 0:
+                return done + self.poll()
