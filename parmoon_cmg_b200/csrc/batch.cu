@@ -99,7 +99,7 @@ struct Batch
   size_t partial_cap = 0;
   int *d_tab = nullptr;
   size_t tab_cap = 0;
-  bool dirty = true;
+  bool dirty = true, check_pending = false;
   std::vector<int> done_queue;
   size_t bytes = 0;
   // tables of the current running set
@@ -649,19 +649,14 @@ __global__ void b_begin_step(BTab t, BCtl *__restrict__ ctl)
   }
 }
 
-// batched Gauss-Jordan inverses of the active blocks of the coarsest levels, one block per
-// instance, in global memory (partial pivoting; flag on a zero pivot)
-__global__ void b_coarse_inverse(int K, double *const *__restrict__ mats, const int *__restrict__ sizes,
-                                 int *__restrict__ pivs, int *__restrict__ flag)
+// Gauss-Jordan inverse of the active block of an instance's coarsest level, one block, in
+// global memory (partial pivoting; flag on a zero pivot)
+__global__ void b_coarse_inverse(double *__restrict__ A, int n, int *__restrict__ piv, int *__restrict__ flag)
 {
   __shared__ double red_v[32];
   __shared__ int red_i[32];
   __shared__ int p_s;
-  for (int k = blockIdx.x; k < K; k += gridDim.x)
   {
-    double *A = mats[k];
-    const int n = sizes[k];
-    int *piv = pivs + (size_t)k * 4096;
     const int nt = blockDim.x, t = threadIdx.x, lane = t % 32, warp = t / 32;
     for (int col = 0; col < n; col++)
     {
@@ -1280,7 +1275,7 @@ int cdgpu_batch_submit(cdgpu_ctx *ctx, int batch_id, int mg_id, const cdgpu_coef
     double *cinv;
     int *piv, *flag;
     const int na = c.n_active;
-    if ((rc = balloc(ctx, in, &cinv, (size_t)na * na)) || (rc = balloc(ctx, in, &piv, 4096)) ||
+    if ((rc = balloc(ctx, in, &cinv, (size_t)na * na)) || (rc = balloc(ctx, in, &piv, std::max(na, 1))) ||
         (rc = balloc(ctx, in, &flag, 1)))
     {
       free_inst(ctx, in);
@@ -1290,21 +1285,17 @@ int cdgpu_batch_submit(cdgpu_ctx *ctx, int batch_id, int mg_id, const cdgpu_coef
     {
       b_dense_active<<<na, 128, 0, ctx->stream>>>(na, c.d_row_ptr, c.d_kcol, B.a64, cinv);
       CD_LAUNCHED(ctx);
-      double **d_mats;
-      int *d_sizes;
-      if ((rc = balloc(ctx, in, &d_mats, 1)) || (rc = balloc(ctx, in, &d_sizes, 1))) { free_inst(ctx, in); return rc; }
-      CD_CUDA(ctx, cudaMemcpyAsync(d_mats, &cinv, sizeof(double *), cudaMemcpyHostToDevice, ctx->stream));
-      CD_CUDA(ctx, cudaMemcpyAsync(d_sizes, &na, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
       CD_CUDA(ctx, cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream));
-      b_coarse_inverse<<<1, 512, 0, ctx->stream>>>(1, d_mats, d_sizes, piv, flag);
+      b_coarse_inverse<<<1, 512, 0, ctx->stream>>>(cinv, na, piv, flag);
       CD_LAUNCHED(ctx);
     }
     B.cinv = cinv;
   }
-  rc = assemble_check(ctx); // synchronises the stream (the host temporaries above are read)
-  if (rc) { free_inst(ctx, in); return rc; }
-  CD_CUDA(ctx, cudaMemcpy(b.d_lev + (size_t)sl * kMaxDepth, lv.data(), sizeof(BLevel) * kMaxDepth,
-                          cudaMemcpyHostToDevice));
+  // pageable host sources: the copy is staged before the call returns.  Assembly errors
+  // (a cell coupling missing from the pattern) are collected at the next advance.
+  CD_CUDA(ctx, cudaMemcpyAsync(b.d_lev + (size_t)sl * kMaxDepth, lv.data(), sizeof(BLevel) * kMaxDepth,
+                               cudaMemcpyHostToDevice, ctx->stream));
+  b.check_pending = true;
   in.state = ST_RUN;
   b.bytes += in.bytes;
   b.dirty = true;
@@ -1319,6 +1310,11 @@ int cdgpu_batch_advance(cdgpu_ctx *ctx, int batch_id, int iterations, int *runni
   Batch &b = *bp;
   cudaSetDevice(ctx->device);
   int rc;
+  if (b.check_pending)
+  {
+    if ((rc = assemble_check(ctx))) return rc;
+    b.check_pending = false;
+  }
   if (b.dirty && (rc = build_tables(ctx, b))) return rc;
   for (int it = 0; it < iterations && !b.run.empty(); it++)
     if ((rc = batch_iteration(ctx, b))) return rc;

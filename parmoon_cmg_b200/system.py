@@ -323,10 +323,9 @@ class Batch:
     def add_structure(self, spaces, parents):
         """Upload a hierarchy (spaces coarsest first); returns its structure id."""
         sids = [self.ctx.upload_space(s) for s in spaces]
-        for sid in sids:
-            self.ctx.build_pattern(sid)
+        nnz = [self.ctx.build_pattern(sid) for sid in sids]
         mg = self.ctx.hierarchy(sids, parents)
-        self.structures.append(dict(mg=mg, n_dof=int(spaces[-1]["n_dof"]), sids=sids))
+        self.structures.append(dict(mg=mg, n_dof=int(spaces[-1]["n_dof"]), sids=sids, nnz=nnz))
         return len(self.structures) - 1
 
     def instance_bytes(self, structure):
@@ -357,9 +356,11 @@ class Batch:
         return list(buf[:cnt.value])
 
     def fetch(self, slot, n_dof):
-        x = np.zeros(n_dof)
+        """(solution, SolveInfo) of a slot; n_dof = 0 reads the statistics only."""
+        x = np.zeros(n_dof) if n_dof else None
         info = SolveInfo()
-        self.ctx.check(self.ctx.lib.cdgpu_batch_fetch(self.ctx.h, self.id, slot, _p(x), C.byref(info)))
+        self.ctx.check(self.ctx.lib.cdgpu_batch_fetch(self.ctx.h, self.id, slot, _p(x) if x is not None else None,
+                                                      C.byref(info)))
         return x, info
 
     def release(self, slot):
