@@ -256,6 +256,24 @@ int cdgpu_batch_submit(cdgpu_ctx *ctx, int batch_id, int mg_id, const cdgpu_coef
 /* run up to `iterations` FGMRES iterations of every running instance; *running (nullable)
  * = instances still running afterwards */
 int cdgpu_batch_advance(cdgpu_ctx *ctx, int batch_id, int iterations, int *running);
+/* a time-dependent instance (theta scheme, as cdgpu_tcd_* per instance, SystemTCD2D.C:
+ * 154-235): mass matrix M and stiffness matrix A (disctype, every level) with coefficients
+ * co, system matrices M + tau*theta1*A on every level and K = M - tau*theta2*A on the finest,
+ * formed in the reference's order of in-place updates; h_u0 = initial solution (n_dof
+ * values; its Dirichlet entries are replaced by the boundary values).  The coefficients are
+ * constant in time, so f_old = f.  The instance idles until cdgpu_batch_tcd_step. */
+int cdgpu_batch_submit_tcd(cdgpu_ctx *ctx, int batch_id, int mg_id, const cdgpu_coeffs *co, int disctype,
+                           double tau, double theta1, double theta2, double theta3, double theta4,
+                           const double *h_u0, int *slot);
+/* one time step of every time-dependent instance of the batch: right-hand side
+ * tau*theta3*f_old + tau*theta4*f + K u_old, then FGMRES from u_old to the batch's stopping
+ * rule.  The right-hand sides and the first `iterations` FGMRES iterations are one CUDA graph
+ * (captured on the first step, replayed while the batch's instances are unchanged); solves
+ * that need more continue in rounds of `iterations`.  *max_iterations (nullable) = the
+ * iterations the slowest instance was given. */
+int cdgpu_batch_tcd_step(cdgpu_ctx *ctx, int batch_id, int iterations, int *max_iterations);
+/* current solution of a time-dependent instance (same as cdgpu_batch_fetch) */
+int cdgpu_batch_tcd_solution(cdgpu_ctx *ctx, int batch_id, int slot, double *h_sol, cdgpu_solve_info *info);
 /* slots that finished since the last poll (at most max_slots; *count = how many) */
 int cdgpu_batch_poll(cdgpu_ctx *ctx, int batch_id, int *slots, int max_slots, int *count);
 /* solution (finest level, n_dof values) and statistics of a finished instance */

@@ -82,6 +82,10 @@ SIGNATURES = {
     "cdgpu_batch_create": (_I, [_P, C.POINTER(SolverParams), C.POINTER(_I)]),
     "cdgpu_batch_submit": (_I, [_P, _I, _I, C.POINTER(Coeffs), _I, _I, C.POINTER(_I)]),
     "cdgpu_batch_advance": (_I, [_P, _I, _I, C.POINTER(_I)]),
+    "cdgpu_batch_submit_tcd": (_I, [_P, _I, _I, C.POINTER(Coeffs), _I, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.c_double, _P, C.POINTER(_I)]),
+    "cdgpu_batch_tcd_step": (_I, [_P, _I, _I, C.POINTER(_I)]),
+    "cdgpu_batch_tcd_solution": (_I, [_P, _I, _I, _P, C.POINTER(SolveInfo)]),
     "cdgpu_batch_poll": (_I, [_P, _I, _P, _I, C.POINTER(_I)]),
     "cdgpu_batch_fetch": (_I, [_P, _I, _I, _P, C.POINTER(SolveInfo)]),
     "cdgpu_batch_release": (_I, [_P, _I, _I]),

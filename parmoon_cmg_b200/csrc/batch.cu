@@ -68,6 +68,10 @@ struct BCtl
   const double *a64;
   double cs[kMaxM], sn[kMaxM], s[kMaxM + 1], y[kMaxM];
   double dots1[kSlots], dots2[kSlots], nrm2;
+  // time-dependent instances: K = M - tau theta2 A (finest), f = (f, phi), c3/c4 = tau theta3/4
+  int tcd, na;
+  double c3, c4;
+  const double *K, *f;
 };
 
 // a grouped launch: items (slots) and the prefix sums of their virtual blocks
@@ -81,7 +85,7 @@ struct BInst
 {
   bool used = false;
   int mg = -1, L = 0, state = ST_EMPTY;
-  bool reported = false;
+  bool reported = false, tcd = false;
   size_t bytes = 0;
   std::vector<void *> allocs;
 };
@@ -106,6 +110,9 @@ struct Batch
   std::vector<int> run;
   int depth = 0;
   BTab fine_vec, fine_csr, items;
+  BTab tcd_csr, tcd_items; // every time-dependent instance, running or idle
+  cudaGraphExec_t tcd_graph = nullptr;
+  int tcd_graph_k = 0;
   std::vector<BTab> smooth, restrict_, coarse;
   std::vector<std::vector<BTab>> color;
   std::vector<int> ncolor_max;
@@ -125,6 +132,7 @@ void free_batch(Batch *b)
   if (!b) return;
   for (auto &in : b->inst)
     for (void *p : in.allocs) cudaFree(p);
+  if (b->tcd_graph) cudaGraphExecDestroy(b->tcd_graph);
   void *ptrs[] = {b->d_ctl, b->d_lev, b->d_state, b->d_partial, b->d_tab};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -740,6 +748,74 @@ __global__ void b_dense_active(int na, const int *__restrict__ rp, const int *__
 
 __global__ void b_init_ctl(BCtl *__restrict__ ctl, int slot, BCtl init) { ctl[slot] = init; }
 
+// theta-scheme matrices of one level from the mass matrix M and the stiffness matrix A, in
+// the reference's order of in-place updates (SystemTCD2D.C:249-270, MatAdd on active rows):
+// K = M - tau theta2 A, S = K + (tau theta2 + tau theta1) A; Dirichlet rows keep M's
+// identity rows.  A is overwritten by S (FP64), S32 and the diagonals are filled; K is
+// written when non-null (finest level).
+__global__ void b_tcd_combine(int n, int na, const int *__restrict__ rp, const int *__restrict__ kc,
+                              const double *__restrict__ M, double *__restrict__ AS, float *__restrict__ S32,
+                              double *__restrict__ d64, float *__restrict__ d32, double mtt2, double tt12,
+                              double *__restrict__ K)
+{
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  for (int j = rp[r]; j < rp[r + 1]; j++)
+  {
+    const double m = M[j], a = AS[j];
+    double k = m, sv = m;
+    if (r < na)
+    {
+      k = m + mtt2 * a;
+      sv = k + tt12 * a;
+    }
+    if (K) K[j] = k;
+    AS[j] = sv;
+    S32[j] = (float)sv;
+    if (kc[j] == r) { d64[r] = sv; d32[r] = (float)sv; }
+  }
+}
+
+// right-hand side of a step (SystemTCD2D.C:237-262): b = tau theta3 f_old + tau theta4 f +
+// K u_old on active rows (f_old = f: coefficients constant in time), b = f on Dirichlet rows
+__global__ void b_tcd_rhs(BTab t, const BCtl *__restrict__ ctl)
+{
+  const int lane = threadIdx.x % 4;
+  for (int vb = blockIdx.x; vb < t.total; vb += gridDim.x)
+  {
+    const int k = find_item(t, vb), slot = t.item[k];
+    const BCtl &c = ctl[slot];
+    const int r = (vb - t.bstart[k]) * kCsrRows + threadIdx.x / 4;
+    const bool valid = r < c.n;
+    const double s = row4<double, double>(c.rp, c.kc, c.K, c.x, r, valid && r < c.na, lane);
+    if (valid && lane == 0)
+    {
+      if (r < c.na)
+      {
+        double v = 0.0;
+        v += c.c3 * c.f[r];
+        v += c.c4 * c.f[r];
+        c.b[r] = v + s;
+      }
+      else
+        c.b[r] = c.f[r];
+    }
+  }
+}
+
+__global__ void b_tcd_begin(BTab t, BCtl *__restrict__ ctl)
+{
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < t.K; k += gridDim.x * blockDim.x)
+  {
+    BCtl &c = ctl[t.item[k]];
+    if (c.state == ST_EMPTY) continue;
+    c.state = ST_RUN;
+    c.action = A_START;
+    c.its = 0;
+    c.status = CDGPU_OK;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -852,8 +928,11 @@ static int grow(cdgpu_ctx *ctx, Batch &b, int need)
 static int build_tables(cdgpu_ctx *ctx, Batch &b)
 {
   b.run.clear();
+  // time-dependent instances stay in the tables between steps (their kernels skip them
+  // while they are idle), so the tables and the captured step do not change per step
   for (int i = 0; i < (int)b.inst.size(); i++)
-    if (b.inst[i].used && b.inst[i].state == ST_RUN) b.run.push_back(i);
+    if (b.inst[i].used && (b.inst[i].state == ST_RUN || b.inst[i].tcd)) b.run.push_back(i);
+  if (b.tcd_graph) { cudaGraphExecDestroy(b.tcd_graph); b.tcd_graph = nullptr; }
   int D = 0;
   for (int i : b.run) D = std::max(D, b.inst[i].L);
   b.depth = D;
@@ -894,6 +973,12 @@ static int build_tables(cdgpu_ctx *ctx, Batch &b)
   v.clear();
   for (int i : b.run) v.push_back({i, 1});
   add(b.items, v);
+  fill(kCsrRows, nrows, [&](int i, int) { return b.inst[i].tcd; }, 0);
+  add(b.tcd_csr, v);
+  v.clear();
+  for (int i : b.run)
+    if (b.inst[i].tcd) v.push_back({i, 1});
+  add(b.tcd_items, v);
   b.smooth.assign(D, BTab());
   b.restrict_.assign(D, BTab());
   b.coarse.assign(D, BTab());
@@ -1108,6 +1193,50 @@ static int batch_iteration(cdgpu_ctx *ctx, Batch &b)
   return CDGPU_OK;
 }
 
+// assemble one form of a shared space into the given arrays (the space's own value arrays
+// and coefficients are restored afterwards)
+static int assemble_to(cdgpu_ctx *ctx, Space &s, int disctype, const cdgpu_coeffs &co, double *a64, float *a32,
+                       double *d64, float *d32, double *rhs64)
+{
+  int rc;
+  if (!s.d_a)
+  {
+    // the space's own arrays are only scratch for a first assembly
+    if ((rc = dev_alloc(ctx, &s.d_a, s.nnz)) || (rc = dev_alloc(ctx, &s.d_a32, s.nnz)) ||
+        (rc = dev_alloc(ctx, &s.d_rhs, s.n_dof)) || (rc = dev_alloc(ctx, &s.d_diag, s.n_dof)) ||
+        (rc = dev_alloc(ctx, &s.d_diag32, s.n_dof)))
+      return rc;
+  }
+  double *sa = s.d_a, *srhs = s.d_rhs, *sd = s.d_diag;
+  float *sa32 = s.d_a32, *sd32 = s.d_diag32;
+  cdgpu_coeffs sco = s.co;
+  bool sset = s.co_set, sasm = s.assembled;
+  s.d_a = a64; s.d_rhs = rhs64; s.d_diag = d64; s.d_a32 = a32; s.d_diag32 = d32;
+  s.co = co;
+  s.co_set = true;
+  rc = assemble_space(ctx, s, disctype, nullptr, false);
+  s.d_a = sa; s.d_rhs = srhs; s.d_diag = sd; s.d_a32 = sa32; s.d_diag32 = sd32;
+  s.co = sco; s.co_set = sset; s.assembled = sasm;
+  return rc;
+}
+
+static int running_count(const Batch &b)
+{
+  int r = 0;
+  for (auto &in : b.inst)
+    if (in.used && in.state == ST_RUN) r++;
+  return r;
+}
+
+// theta-scheme parameters of a time-dependent instance
+struct TcdSpec
+{
+  double tau, th1, th2, th3, th4;
+};
+
+static int submit_impl(cdgpu_ctx *ctx, Batch &b, int mg_id, const cdgpu_coeffs *co, int disctype,
+                       int coarse_disctype, const TcdSpec *tcd, const double *h_u0, int *slot);
+
 extern "C" {
 
 int cdgpu_batch_create(cdgpu_ctx *ctx, const cdgpu_solver_params *params, int *batch_id)
@@ -1153,154 +1282,18 @@ int cdgpu_batch_submit(cdgpu_ctx *ctx, int batch_id, int mg_id, const cdgpu_coef
   Batch *bp = get_batch(ctx, batch_id);
   if (!bp || mg_id < 0 || mg_id >= (int)ctx->mgs.size() || !co || !slot)
     return fail(ctx, CDGPU_ERR_INVALID, "batch_submit: bad argument");
-  if (co->kind == CDGPU_COEFF_TABLE)
-    return fail(ctx, CDGPU_ERR_UNSUPPORTED, "batch_submit: coefficient tables are not batched");
-  Batch &b = *bp;
-  Hierarchy &h = *ctx->mgs[mg_id];
-  const int L = (int)h.lev.size();
-  if (L > kMaxDepth) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "batch_submit: more than 12 levels");
-  const Space &cs = *h.lev[0].sp;
-  if (cs.n_active > 4096) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "batch_submit: coarsest level above 4096 active DOFs");
-  if ((size_t)(cs.n_dof + cs.n_active) * sizeof(double) > 200 * 1024)
-    return fail(ctx, CDGPU_ERR_UNSUPPORTED, "batch_submit: coarsest level too large for the exact solve");
-  cudaSetDevice(ctx->device);
-  int rc;
-  if (b.p.smoother != 1 && (rc = ensure_colors(ctx, h))) return rc;
-  // a free slot
-  int sl = -1;
-  for (int i = 0; i < (int)b.inst.size(); i++)
-    if (!b.inst[i].used) { sl = i; break; }
-  if (sl < 0) { sl = (int)b.inst.size(); b.inst.emplace_back(); }
-  if ((rc = grow(ctx, b, (int)b.inst.size()))) return rc;
-  BInst &in = b.inst[sl];
-  in = BInst();
-  in.used = true;
-  in.mg = mg_id;
-  in.L = L;
-  const int m = b.m;
-  std::vector<BLevel> lv(kMaxDepth);
-  // per level: values, vectors; assemble with this instance's coefficients
-  for (int l = 0; l < L; l++)
-  {
-    Level &Lv = h.lev[l];
-    Space &s = *Lv.sp;
-    if (s.nnz < 0) { free_inst(ctx, in); return fail(ctx, CDGPU_ERR_INVALID, "batch_submit: level without pattern"); }
-    const int d = L - 1 - l;
-    BLevel &B = lv[d];
-    double *a64, *d64, *rhs64;
-    float *a32, *d32;
-    if ((rc = balloc(ctx, in, &a64, s.nnz)) || (rc = balloc(ctx, in, &d64, s.n_dof)) ||
-        (rc = balloc(ctx, in, &rhs64, s.n_dof)) || (rc = balloc(ctx, in, &a32, s.nnz)) ||
-        (rc = balloc(ctx, in, &d32, s.n_dof)) || (rc = balloc(ctx, in, &B.v[0], s.n_dof)) ||
-        (rc = balloc(ctx, in, &B.v[1], s.n_dof)) || (rc = balloc(ctx, in, (float **)&B.rhs, s.n_dof)) ||
-        (rc = balloc(ctx, in, &B.def, s.n_dof)))
-    {
-      free_inst(ctx, in);
-      return rc;
-    }
-    // assemble into this instance's arrays through the shared space
-    double *sa = s.d_a, *srhs = s.d_rhs, *sd = s.d_diag;
-    float *sa32 = s.d_a32, *sd32 = s.d_diag32;
-    cdgpu_coeffs sco = s.co;
-    bool sset = s.co_set, sasm = s.assembled;
-    if (!s.d_a)
-    {
-      // the space's own arrays are only scratch for its first assembly
-      if ((rc = dev_alloc(ctx, &s.d_a, s.nnz)) || (rc = dev_alloc(ctx, &s.d_a32, s.nnz)) ||
-          (rc = dev_alloc(ctx, &s.d_rhs, s.n_dof)) || (rc = dev_alloc(ctx, &s.d_diag, s.n_dof)) ||
-          (rc = dev_alloc(ctx, &s.d_diag32, s.n_dof)))
-      {
-        free_inst(ctx, in);
-        return rc;
-      }
-      sa = s.d_a; srhs = s.d_rhs; sd = s.d_diag; sa32 = s.d_a32; sd32 = s.d_diag32;
-    }
-    s.d_a = a64; s.d_rhs = rhs64; s.d_diag = d64; s.d_a32 = a32; s.d_diag32 = d32;
-    s.co = *co;
-    s.co_set = true;
-    rc = assemble_space(ctx, s, l == L - 1 ? disctype : coarse_disctype, nullptr, false);
-    s.d_a = sa; s.d_rhs = srhs; s.d_diag = sd; s.d_a32 = sa32; s.d_diag32 = sd32;
-    s.co = sco; s.co_set = sset; s.assembled = sasm;
-    if (rc) { free_inst(ctx, in); return rc; }
-    B.n = s.n_dof;
-    B.na = s.n_active;
-    B.rp = s.d_row_ptr;
-    B.kc = s.d_kcol;
-    B.dirst = s.d_dir_start;
-    B.color_rows = Lv.d_color_rows;
-    B.a32 = a32;
-    B.d32 = d32;
-    B.a64 = a64;
-    if (l > 0)
-    {
-      // this level is the fine one of the transfer to level l-1
-      const Space &c = *h.lev[l - 1].sp;
-      B.nc = c.n_dof;
-      B.nca = c.n_active;
-      B.prp = Lv.d_p_row; B.pkc = Lv.d_p_col; B.pv = Lv.d_p_val32;
-      B.rrp = Lv.d_r_row; B.rkc = Lv.d_r_col; B.rv = Lv.d_r_val32;
-    }
-    if (l == L - 1)
-    {
-      // FGMRES workspace and the right-hand side
-      BCtl c{};
-      c.state = ST_RUN;
-      c.action = A_START;
-      c.n = s.n_dof;
-      c.m = m;
-      c.rp = s.d_row_ptr;
-      c.kc = s.d_kcol;
-      c.a64 = a64;
-      if ((rc = balloc(ctx, in, &c.V, (size_t)(m + 1) * s.n_dof)) || (rc = balloc(ctx, in, &c.Z, (size_t)(m + 1) * s.n_dof)) ||
-          (rc = balloc(ctx, in, &c.w, s.n_dof)) || (rc = balloc(ctx, in, &c.x, s.n_dof)) ||
-          (rc = balloc(ctx, in, &c.H, (size_t)(m + 1) * m)))
-      {
-        free_inst(ctx, in);
-        return rc;
-      }
-      c.b = rhs64;
-      // initial guess: 0 on active rows, the Dirichlet values on Dirichlet rows
-      CD_CUDA(ctx, cudaMemsetAsync(c.x, 0, sizeof(double) * s.n_dof, ctx->stream));
-      if (s.n_dof > s.n_active)
-        CD_CUDA(ctx, cudaMemcpyAsync(c.x + s.n_active, rhs64 + s.n_active, sizeof(double) * (s.n_dof - s.n_active),
-                                     cudaMemcpyDeviceToDevice, ctx->stream));
-      b_init_ctl<<<1, 1, 0, ctx->stream>>>(b.d_ctl, sl, c);
-      CD_LAUNCHED(ctx);
-    }
-  }
-  // exact coarse solve: inverse of the coarsest level's active block
-  {
-    const Space &c = *h.lev[0].sp;
-    BLevel &B = lv[L - 1];
-    double *cinv;
-    int *piv, *flag;
-    const int na = c.n_active;
-    if ((rc = balloc(ctx, in, &cinv, (size_t)na * na)) || (rc = balloc(ctx, in, &piv, std::max(na, 1))) ||
-        (rc = balloc(ctx, in, &flag, 1)))
-    {
-      free_inst(ctx, in);
-      return rc;
-    }
-    if (na > 0)
-    {
-      b_dense_active<<<na, 128, 0, ctx->stream>>>(na, c.d_row_ptr, c.d_kcol, B.a64, cinv);
-      CD_LAUNCHED(ctx);
-      CD_CUDA(ctx, cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream));
-      b_coarse_inverse<<<1, 512, 0, ctx->stream>>>(cinv, na, piv, flag);
-      CD_LAUNCHED(ctx);
-    }
-    B.cinv = cinv;
-  }
-  // pageable host sources: the copy is staged before the call returns.  Assembly errors
-  // (a cell coupling missing from the pattern) are collected at the next advance.
-  CD_CUDA(ctx, cudaMemcpyAsync(b.d_lev + (size_t)sl * kMaxDepth, lv.data(), sizeof(BLevel) * kMaxDepth,
-                               cudaMemcpyHostToDevice, ctx->stream));
-  b.check_pending = true;
-  in.state = ST_RUN;
-  b.bytes += in.bytes;
-  b.dirty = true;
-  *slot = sl;
-  return CDGPU_OK;
+  return submit_impl(ctx, *bp, mg_id, co, disctype, coarse_disctype, nullptr, nullptr, slot);
+}
+
+int cdgpu_batch_submit_tcd(cdgpu_ctx *ctx, int batch_id, int mg_id, const cdgpu_coeffs *co, int disctype,
+                           double tau, double theta1, double theta2, double theta3, double theta4,
+                           const double *h_u0, int *slot)
+{
+  Batch *bp = get_batch(ctx, batch_id);
+  if (!bp || mg_id < 0 || mg_id >= (int)ctx->mgs.size() || !co || !slot || !h_u0 || !(tau > 0))
+    return fail(ctx, CDGPU_ERR_INVALID, "batch_submit_tcd: bad argument");
+  TcdSpec t{tau, theta1, theta2, theta3, theta4};
+  return submit_impl(ctx, *bp, mg_id, co, disctype, disctype, &t, h_u0, slot);
 }
 
 int cdgpu_batch_advance(cdgpu_ctx *ctx, int batch_id, int iterations, int *running)
@@ -1316,7 +1309,7 @@ int cdgpu_batch_advance(cdgpu_ctx *ctx, int batch_id, int iterations, int *runni
     b.check_pending = false;
   }
   if (b.dirty && (rc = build_tables(ctx, b))) return rc;
-  for (int it = 0; it < iterations && !b.run.empty(); it++)
+  for (int it = 0; it < iterations && running_count(b) > 0; it++)
     if ((rc = batch_iteration(ctx, b))) return rc;
   // collect the states
   if (!b.run.empty())
@@ -1328,8 +1321,11 @@ int cdgpu_batch_advance(cdgpu_ctx *ctx, int batch_id, int iterations, int *runni
       if (b.h_state[i] == ST_DONE && b.inst[i].state == ST_RUN)
       {
         b.inst[i].state = ST_DONE;
-        b.done_queue.push_back(i);
-        changed = true;
+        if (!b.inst[i].tcd)
+        {
+          b.done_queue.push_back(i);
+          changed = true;
+        }
       }
     if (changed) b.dirty = true;
   }
@@ -1338,6 +1334,88 @@ int cdgpu_batch_advance(cdgpu_ctx *ctx, int batch_id, int iterations, int *runni
     if (in.used && in.state == ST_RUN) r++;
   if (running) *running = r;
   return CDGPU_OK;
+}
+
+int cdgpu_batch_tcd_step(cdgpu_ctx *ctx, int batch_id, int iterations, int *max_iterations)
+{
+  Batch *bp = get_batch(ctx, batch_id);
+  if (!bp || iterations < 1) return fail(ctx, CDGPU_ERR_INVALID, "batch_tcd_step: bad argument");
+  Batch &b = *bp;
+  cudaSetDevice(ctx->device);
+  int rc;
+  if (b.check_pending)
+  {
+    if ((rc = assemble_check(ctx))) return rc;
+    b.check_pending = false;
+  }
+  if (b.dirty && (rc = build_tables(ctx, b))) return rc;
+  if (b.tcd_items.K == 0) return fail(ctx, CDGPU_ERR_INVALID, "batch_tcd_step: no time-dependent instance");
+  for (auto &in : b.inst)
+    if (in.used && in.tcd) in.state = ST_RUN;
+  // the step -- right-hand sides, restart of every time-dependent solve from its previous
+  // solution, `iterations` FGMRES iterations of everything running -- is one CUDA graph,
+  // captured on first use and replayed for every step while the instance set is unchanged
+  if (!b.tcd_graph || b.tcd_graph_k != iterations)
+  {
+    if (b.tcd_graph) { cudaGraphExecDestroy(b.tcd_graph); b.tcd_graph = nullptr; }
+    // coarse-solve shared memory is configured outside the capture
+    size_t sm = 0;
+    for (int i : b.run)
+    {
+      const Space &c = *ctx->mgs[b.inst[i].mg]->lev[0].sp;
+      sm = std::max(sm, sizeof(double) * (c.n_dof + c.n_active));
+    }
+    if (sm > 48 * 1024)
+      CD_CUDA(ctx, cudaFuncSetAttribute(b_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const long long before = ctx->launches;
+    CD_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    b_tcd_rhs<<<std::max(1, std::min(b.tcd_csr.total, ctx->sm_count * 8)), kNT, 0, ctx->stream>>>(b.tcd_csr, b.d_ctl);
+    rc = cudaGetLastError() == cudaSuccess ? CDGPU_OK : CDGPU_ERR_CUDA;
+    if (!rc)
+    {
+      b_tcd_begin<<<1, 256, 0, ctx->stream>>>(b.tcd_items, b.d_ctl);
+      for (int it = 0; it < iterations && !rc; it++) rc = batch_iteration(ctx, b);
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    ctx->launches = before;
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture of the time step");
+    e = cudaGraphInstantiate(&b.tcd_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { b.tcd_graph = nullptr; return cuda_fail(ctx, e, "graph instantiate"); }
+    b.tcd_graph_k = iterations;
+  }
+  CD_CUDA(ctx, cudaGraphLaunch(b.tcd_graph, ctx->stream));
+  // solves that need more iterations continue outside the graph
+  int r = 1, rounds = 0;
+  while (true)
+  {
+    CD_CUDA(ctx, cudaMemcpyAsync(b.h_state, b.d_state, sizeof(int) * b.cap, cudaMemcpyDeviceToHost, ctx->stream));
+    CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    r = 0;
+    for (int i : b.run)
+    {
+      BInst &in = b.inst[i];
+      if (in.state == ST_RUN && b.h_state[i] == ST_DONE)
+      {
+        in.state = ST_DONE;
+        if (!in.tcd) { b.done_queue.push_back(i); b.dirty = true; }
+      }
+      if (in.tcd && in.state == ST_RUN) r++;
+    }
+    if (r == 0) break;
+    for (int it = 0; it < iterations; it++)
+      if ((rc = batch_iteration(ctx, b))) return rc;
+    rounds++;
+  }
+  if (max_iterations) *max_iterations = iterations * (rounds + 1);
+  return CDGPU_OK;
+}
+
+int cdgpu_batch_tcd_solution(cdgpu_ctx *ctx, int batch_id, int slot, double *h_sol, cdgpu_solve_info *info)
+{
+  return cdgpu_batch_fetch(ctx, batch_id, slot, h_sol, info);
 }
 
 int cdgpu_batch_poll(cdgpu_ctx *ctx, int batch_id, int *slots, int max_slots, int *count)
@@ -1405,3 +1483,180 @@ int cdgpu_batch_memory(cdgpu_ctx *ctx, int batch_id, unsigned long long *bytes)
 }
 
 } // extern "C"
+
+static int submit_impl(cdgpu_ctx *ctx, Batch &b, int mg_id, const cdgpu_coeffs *co, int disctype,
+                       int coarse_disctype, const TcdSpec *tcd, const double *h_u0, int *slot)
+{
+  if (co->kind == CDGPU_COEFF_TABLE)
+    return fail(ctx, CDGPU_ERR_UNSUPPORTED, "batch_submit: coefficient tables are not batched");
+  Hierarchy &h = *ctx->mgs[mg_id];
+  const int L = (int)h.lev.size();
+  if (L > kMaxDepth) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "batch_submit: more than 12 levels");
+  const Space &cs = *h.lev[0].sp;
+  if (cs.n_active > 4096) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "batch_submit: coarsest level above 4096 active DOFs");
+  if ((size_t)(cs.n_dof + cs.n_active) * sizeof(double) > 200 * 1024)
+    return fail(ctx, CDGPU_ERR_UNSUPPORTED, "batch_submit: coarsest level too large for the exact solve");
+  cudaSetDevice(ctx->device);
+  int rc;
+  if (b.p.smoother != 1 && (rc = ensure_colors(ctx, h))) return rc;
+  // a free slot
+  int sl = -1;
+  for (int i = 0; i < (int)b.inst.size(); i++)
+    if (!b.inst[i].used) { sl = i; break; }
+  if (sl < 0) { sl = (int)b.inst.size(); b.inst.emplace_back(); }
+  if ((rc = grow(ctx, b, (int)b.inst.size()))) return rc;
+  BInst &in = b.inst[sl];
+  in = BInst();
+  in.used = true;
+  in.mg = mg_id;
+  in.L = L;
+  const int m = b.m;
+  std::vector<BLevel> lv(kMaxDepth);
+  double *tcd_K = nullptr;
+  // per level: values, vectors; assemble with this instance's coefficients
+  for (int l = 0; l < L; l++)
+  {
+    Level &Lv = h.lev[l];
+    Space &s = *Lv.sp;
+    if (s.nnz < 0) { free_inst(ctx, in); return fail(ctx, CDGPU_ERR_INVALID, "batch_submit: level without pattern"); }
+    const int d = L - 1 - l;
+    BLevel &B = lv[d];
+    double *a64, *d64, *rhs64;
+    float *a32, *d32;
+    if ((rc = balloc(ctx, in, &a64, s.nnz)) || (rc = balloc(ctx, in, &d64, s.n_dof)) ||
+        (rc = balloc(ctx, in, &rhs64, s.n_dof)) || (rc = balloc(ctx, in, &a32, s.nnz)) ||
+        (rc = balloc(ctx, in, &d32, s.n_dof)) || (rc = balloc(ctx, in, &B.v[0], s.n_dof)) ||
+        (rc = balloc(ctx, in, &B.v[1], s.n_dof)) || (rc = balloc(ctx, in, (float **)&B.rhs, s.n_dof)) ||
+        (rc = balloc(ctx, in, &B.def, s.n_dof)))
+    {
+      free_inst(ctx, in);
+      return rc;
+    }
+    // assemble into this instance's arrays through the shared space
+    const int form = l == L - 1 ? disctype : coarse_disctype;
+    if (!tcd)
+      rc = assemble_to(ctx, s, form, *co, a64, a32, d64, d32, rhs64);
+    else
+    {
+      // mass matrix into temporaries, stiffness matrix into the instance's arrays, then the
+      // theta-scheme combinations
+      double *Mt = nullptr, *dt = nullptr, *rt = nullptr, *K = nullptr;
+      float *a32t = nullptr, *d32t = nullptr;
+      cudaError_t e = cudaMallocAsync((void **)&Mt, sizeof(double) * s.nnz, ctx->stream);
+      if (e == cudaSuccess) e = cudaMallocAsync((void **)&a32t, sizeof(float) * s.nnz, ctx->stream);
+      if (e == cudaSuccess) e = cudaMallocAsync((void **)&dt, sizeof(double) * s.n_dof, ctx->stream);
+      if (e == cudaSuccess) e = cudaMallocAsync((void **)&d32t, sizeof(float) * s.n_dof, ctx->stream);
+      if (e == cudaSuccess) e = cudaMallocAsync((void **)&rt, sizeof(double) * s.n_dof, ctx->stream);
+      if (e != cudaSuccess) { cudaGetLastError(); free_inst(ctx, in); return fail(ctx, CDGPU_ERR_OOM, "batch: device memory exhausted"); }
+      rc = assemble_to(ctx, s, CDGPU_MASS, *co, Mt, a32t, dt, d32t, rt);
+      if (!rc) rc = assemble_to(ctx, s, form, *co, a64, a32, d64, d32, rhs64);
+      if (!rc && l == L - 1) rc = balloc(ctx, in, &K, s.nnz);
+      if (!rc)
+      {
+        b_tcd_combine<<<(s.n_dof + 255) / 256, 256, 0, ctx->stream>>>(
+            s.n_dof, s.n_active, s.d_row_ptr, s.d_kcol, Mt, a64, a32, d64, d32, -tcd->tau * tcd->th2,
+            tcd->tau * tcd->th2 + tcd->tau * tcd->th1, K);
+        CD_LAUNCHED(ctx);
+        tcd_K = K;
+      }
+      void *tmp[] = {Mt, a32t, dt, d32t, rt};
+      for (void *q : tmp) cudaFreeAsync(q, ctx->stream);
+    }
+    if (rc) { free_inst(ctx, in); return rc; }
+    B.n = s.n_dof;
+    B.na = s.n_active;
+    B.rp = s.d_row_ptr;
+    B.kc = s.d_kcol;
+    B.dirst = s.d_dir_start;
+    B.color_rows = Lv.d_color_rows;
+    B.a32 = a32;
+    B.d32 = d32;
+    B.a64 = a64;
+    if (l > 0)
+    {
+      // this level is the fine one of the transfer to level l-1
+      const Space &c = *h.lev[l - 1].sp;
+      B.nc = c.n_dof;
+      B.nca = c.n_active;
+      B.prp = Lv.d_p_row; B.pkc = Lv.d_p_col; B.pv = Lv.d_p_val32;
+      B.rrp = Lv.d_r_row; B.rkc = Lv.d_r_col; B.rv = Lv.d_r_val32;
+    }
+    if (l == L - 1)
+    {
+      // FGMRES workspace and the right-hand side
+      BCtl c{};
+      c.state = ST_RUN;
+      c.action = A_START;
+      c.n = s.n_dof;
+      c.m = m;
+      c.rp = s.d_row_ptr;
+      c.kc = s.d_kcol;
+      c.a64 = a64;
+      if ((rc = balloc(ctx, in, &c.V, (size_t)(m + 1) * s.n_dof)) || (rc = balloc(ctx, in, &c.Z, (size_t)(m + 1) * s.n_dof)) ||
+          (rc = balloc(ctx, in, &c.w, s.n_dof)) || (rc = balloc(ctx, in, &c.x, s.n_dof)) ||
+          (rc = balloc(ctx, in, &c.H, (size_t)(m + 1) * m)))
+      {
+        free_inst(ctx, in);
+        return rc;
+      }
+      c.b = rhs64;
+      c.na = s.n_active;
+      if (tcd)
+      {
+        // idle until the first step; b is the step's right-hand side, f = (f, phi)
+        c.state = ST_DONE;
+        c.action = 0;
+        c.tcd = 1;
+        c.c3 = tcd->tau * tcd->th3;
+        c.c4 = tcd->tau * tcd->th4;
+        c.K = tcd_K;
+        c.f = rhs64;
+        if ((rc = balloc(ctx, in, &c.b, s.n_dof))) { free_inst(ctx, in); return rc; }
+        CD_CUDA(ctx, cudaMemcpyAsync(c.x, h_u0, sizeof(double) * s.n_dof, cudaMemcpyHostToDevice, ctx->stream));
+      }
+      else
+        CD_CUDA(ctx, cudaMemsetAsync(c.x, 0, sizeof(double) * s.n_dof, ctx->stream));
+      // initial guess: the Dirichlet values on Dirichlet rows (AssembleMRhs copies them from
+      // the right-hand side into the solution, SystemTCD2D.C:120)
+      if (s.n_dof > s.n_active)
+        CD_CUDA(ctx, cudaMemcpyAsync(c.x + s.n_active, rhs64 + s.n_active, sizeof(double) * (s.n_dof - s.n_active),
+                                     cudaMemcpyDeviceToDevice, ctx->stream));
+      b_init_ctl<<<1, 1, 0, ctx->stream>>>(b.d_ctl, sl, c);
+      CD_LAUNCHED(ctx);
+    }
+  }
+  // exact coarse solve: inverse of the coarsest level's active block
+  {
+    const Space &c = *h.lev[0].sp;
+    BLevel &B = lv[L - 1];
+    double *cinv;
+    int *piv, *flag;
+    const int na = c.n_active;
+    if ((rc = balloc(ctx, in, &cinv, (size_t)na * na)) || (rc = balloc(ctx, in, &piv, std::max(na, 1))) ||
+        (rc = balloc(ctx, in, &flag, 1)))
+    {
+      free_inst(ctx, in);
+      return rc;
+    }
+    if (na > 0)
+    {
+      b_dense_active<<<na, 128, 0, ctx->stream>>>(na, c.d_row_ptr, c.d_kcol, B.a64, cinv);
+      CD_LAUNCHED(ctx);
+      CD_CUDA(ctx, cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream));
+      b_coarse_inverse<<<1, 512, 0, ctx->stream>>>(cinv, na, piv, flag);
+      CD_LAUNCHED(ctx);
+    }
+    B.cinv = cinv;
+  }
+  // pageable host sources: the copy is staged before the call returns.  Assembly errors
+  // (a cell coupling missing from the pattern) are collected at the next advance.
+  CD_CUDA(ctx, cudaMemcpyAsync(b.d_lev + (size_t)sl * kMaxDepth, lv.data(), sizeof(BLevel) * kMaxDepth,
+                               cudaMemcpyHostToDevice, ctx->stream));
+  b.check_pending = true;
+  in.state = tcd ? ST_DONE : ST_RUN;
+  in.tcd = tcd != nullptr;
+  b.bytes += in.bytes;
+  b.dirty = true;
+  *slot = sl;
+  return CDGPU_OK;
+}

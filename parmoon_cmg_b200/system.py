@@ -343,6 +343,23 @@ class Batch:
                                                        disctype, cd, C.byref(slot)))
         return slot.value
 
+    def submit_tcd(self, structure, coeff, tau, theta1, theta2, theta3, theta4, u0, disctype=GALERKIN):
+        """A time-dependent instance (theta scheme) with initial solution u0."""
+        slot = C.c_int()
+        st = self.structures[structure]
+        u0 = _f64(u0)
+        self.ctx.check(self.ctx.lib.cdgpu_batch_submit_tcd(self.ctx.h, self.id, st["mg"], C.byref(coeff), disctype,
+                                                           tau, theta1, theta2, theta3, theta4, _p(u0),
+                                                           C.byref(slot)))
+        return slot.value
+
+    def tcd_step(self, iterations=4):
+        """One time step of every time-dependent instance; returns the iterations given to
+        the slowest one."""
+        out = C.c_int()
+        self.ctx.check(self.ctx.lib.cdgpu_batch_tcd_step(self.ctx.h, self.id, iterations, C.byref(out)))
+        return out.value
+
     def advance(self, iterations=1):
         running = C.c_int()
         self.ctx.check(self.ctx.lib.cdgpu_batch_advance(self.ctx.h, self.id, iterations, C.byref(running)))

@@ -117,3 +117,44 @@ def test_tcd_rejects_bad_use():
             ctx.check(ctx.lib.cdgpu_tcd_create(ctx.h, S.mg, _lib.SUPG, C.byref(C.c_int())))
     finally:
         ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("smoother", [1, 3])
+def test_batched_tcd_steps_vs_oracle(oracle_lib, smoother):
+    """Time-dependent instances in a batch (one graph per step) follow the oracle's
+    theta-scheme steps: Crank-Nicolson, rotating convection, Gaussian initial bump."""
+    from parmoon_cmg_b200 import _build
+    from parmoon_cmg_b200.system import Batch
+    _build.build()
+    tau, th = 1e-3, (0.5, 0.5, 0.5, 0.5)
+    ctx = Context(0)
+    try:
+        B = Batch(solver_params(smoother=smoother, omega=0.8 if smoother == 1 else 1.0, stop_rule=1,
+                                red_factor=1e-13, restart=30, maxit=200), ctx)
+        cases = []
+        for order, n0, L, eps in [(2, 2, 3, 1e-3), (1, 2, 4, 1e-4)]:
+            spaces, parents = mesh.structured_hierarchy(2, order, n0, L)
+            sid = B.add_structure(spaces, parents)
+            xy = mesh.dof_coords(spaces[-1])
+            u0 = np.exp(-((xy[:, 0] - 0.3) ** 2 + (xy[:, 1] - 0.3) ** 2) / (2 * 0.05 ** 2))
+            co = coeffs(_lib.COEFF_ROTATING, eps=eps, f=0.0)
+            slot = B.submit_tcd(sid, co, tau, *th, u0)
+            levels = oracle_levels(oracle_lib, spaces, parents, 2, order)
+            oco = oracle_lib.coeffs(_lib.COEFF_ROTATING, eps=eps, f=0.0)
+            M, f = oracle_forms(oracle_lib, spaces, levels, 2, order, MASS, oco)
+            A, f = oracle_forms(oracle_lib, spaces, levels, 2, order, 1, oco)
+            u = u0.copy()
+            u[spaces[-1]["n_active"]:] = f[spaces[-1]["n_active"]:]
+            cases.append(dict(slot=slot, levels=levels, M=M, A=A, f=f, u=u, n=spaces[-1]["n_dof"]))
+        prm_o = oracle_lib.solver_params(red_factor=1e-13, restart=32, maxit=200)
+        for step in range(4):
+            B.tcd_step(4)
+            for c in cases:
+                c["u"], its = oracle_lib.tcd_step(c["levels"], c["M"], c["A"], c["f"], c["f"], c["u"], tau, *th,
+                                                  prm_o)
+                x, info = B.fetch(c["slot"], c["n"])
+                assert info.status == 0
+                assert np.abs(x - c["u"]).max() <= 1e-9 * np.abs(c["u"]).max(), step
+    finally:
+        ctx.close()
