@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=200)
     ap.add_argument("--serving-rate", type=float, default=40.0, help="mean arrivals per second")
     ap.add_argument("--no-tcd", action="store_true", help="skip the time-dependent CD2D section")
+    ap.add_argument("--no-cd2d", action="store_true", help="skip the CD2D plain FP64 section")
     ap.add_argument("--tcd-instances", type=int, default=256)
     ap.add_argument("--tcd-steps", type=int, default=1000)
     return ap.parse_args()
@@ -532,6 +533,85 @@ def run_serving(ctx, args):
     return st
 
 
+DAT2D = """VERSION: 1
+LOGFILE: logfile
+OUTFILE: {out}
+BNDFILE: {mesh}/unit_square.PRM
+GEOFILE: {mesh}/unit_square.GEO
+MESH_TYPE: 0
+UNIFORM_STEPS: {steps}
+LEVELS: {levels}
+ANSATZ_ORDER: 1
+DISCTYPE: 2
+""" + DAT[DAT.index("SOLVER_TYPE"):]
+
+
+def run_cd2d(ctx, args):
+    """CD2D plain FP64: unit square 64 x 64 Q1, eps 1e-3, b = (1, 0.5), f = 1, Dirichlet 0,
+    SUPG with the reference's delta; assemble every level + FGMRES(30) with a 5-level V(2,2)
+    damped-Jacobi (0.8) cycle to the reference's relative residual 1e-10 (its own stopping
+    rule), every level and the cycle in FP64.  Inputs resident on the device, CUDA events;
+    the compiled reference solves the same problem on one host core."""
+    import torch
+    from parmoon_cmg_b200 import mesh
+    from parmoon_cmg_b200.system import SUPG, TSystemCD2D, coeffs, solver_params
+    spaces, parents = mesh.structured_hierarchy(2, 1, 4, 5)
+    S = TSystemCD2D(spaces, parents, disctype=SUPG, ctx=ctx)
+    S.Init(coeffs(0, eps=1e-3, b=(1.0, 0.5), f=1.0))
+    prm = solver_params(precision=0, coarse_smoother=17, stop_rule=0, red_factor=1e-10)
+    n = S.N_DOF
+    d_sol = torch.zeros(n, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream, device=d_sol.device)
+
+    def step():
+        ctx.assemble_hierarchy(S.mg, SUPG, SUPG)
+        d_rhs = ctx.rhs_device(S.sids[-1])
+        with torch.cuda.stream(stream):
+            d_sol.zero_()
+        info = ctx.solve_device(S.mg, prm, d_rhs, d_sol.data_ptr())
+        if info.status != 0:
+            raise RuntimeError(f"cd2d solve status {info.status}")
+        return info
+    for _ in range(max(3, args.warmup)):
+        step()
+    reps = 20
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        info = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    out = {"metric": "CD2D plain FP64 solves/s", "value": 1e3 / ms, "unit": "solves/s", "ms_per_solve": ms,
+           "n_dof": n, "fgmres_iterations": info.iterations, "form": "FP64 (drop-in)",
+           "config": "unit square 64x64 Q1, eps 1e-3, b=(1,0.5), f=1, Dirichlet 0, SUPG (reference delta); "
+                     "5 levels 4^2..64^2, FGMRES(30), V(2,2) damped Jacobi 0.8, rel. residual 1e-10"}
+    exe = os.path.join(ROOT, "oracle", "_ref", "cd2d_dump")
+    if not args.no_cpu_baseline and os.path.exists(exe):
+        tmp = tempfile.mkdtemp()
+        try:
+            dat = os.path.join(tmp, "c1.dat")
+            with open(dat, "w") as f:
+                f.write(DAT2D.format(out=os.path.join(tmp, "c1.out"), mesh=os.path.join(ROOT, "oracle", "meshes"),
+                                     steps=2, levels=5))
+            times = []
+            for _ in range(5):
+                p = subprocess.run([exe, dat, "-", "0", "1e-3", "1.0", "0.5", "0", "1"], cwd=tmp,
+                                   capture_output=True, text=True, check=True)
+                t = json.loads([l for l in p.stdout.splitlines() if l.startswith("{")][-1])
+                times.append(t["t_assemble"] + t["t_solve"])
+            out["cpu_baseline"] = {"value": 1.0 / float(np.median(times)), "unit": "solves/s", "cores": 1,
+                                   "kind": "reference", "iterations": t["iterations"],
+                                   "sample": "median of 5 assemble+solve runs of the same problem by the reference"}
+        except Exception as e:
+            out["cpu_baseline"] = {"value": None, "sample": f"unavailable: {e}"}
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+    return out
+
+
 def run_tcd(ctx, args):
     """Time-dependent CD2D: instances of 128^2 Q2 on the unit square, Crank-Nicolson with
     tau = 1e-3, rotating convection b = (0.5 - y, x - 0.5), eps log-uniform in [1e-5, 1e-2]
@@ -598,6 +678,8 @@ def main():
             run_reference_arm(args, rank, world)
             return
         result, ctx = run_ours(args, rank, world, local)
+        if not args.no_cd2d:
+            result["cd2d"] = run_cd2d(ctx, args)
         if not args.no_batched:
             result["batched"] = run_batched(ctx, args)
         if not args.no_serving:
