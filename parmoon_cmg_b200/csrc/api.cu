@@ -32,7 +32,7 @@ static Hierarchy *get_mg(cdgpu_ctx *ctx, int id)
 static void free_space(Space *s)
 {
   if (!s) return;
-  void *ptrs[] = {s->d_coords, s->d_gn,  s->d_row_ptr, s->d_kcol,     s->d_dir_start, s->d_inc_ptr,
+  void *ptrs[] = {s->d_coords, s->d_gn,  s->d_row_ptr, s->d_kcol,     s->d_dir_start, s->d_slot, s->d_inc_ptr,
                   s->d_inc,    s->d_a,   s->d_rhs,     s->d_diag,     s->d_a32,       s->d_diag32,
                   s->d_tab,    s->d_cellcoef, s->d_local, s->d_dir, s->d_ref, s->d_quadtab};
   for (void *p : ptrs)
@@ -207,7 +207,8 @@ static int install_pattern(cdgpu_ctx *ctx, Space &s)
   CD_CUDA(ctx, cudaMemcpy(s.d_kcol, s.h_kcol.data(), sizeof(int) * s.nnz, cudaMemcpyHostToDevice));
   CD_CUDA(ctx, cudaMemcpy(s.d_dir_start, dir_start.data(), sizeof(int) * s.n_dof, cudaMemcpyHostToDevice));
   s.shape = csr_shape(s.h_row_ptr.data(), s.n_dof);
-  // a new pattern invalidates values sized for the old one
+  // a new pattern invalidates values sized for the old one and the slot map
+  s.slot_pattern = -1;
   void **vals[] = {(void **)&s.d_a, (void **)&s.d_a32};
   for (void **p : vals)
     if (*p) { cudaFree(*p); *p = nullptr; }

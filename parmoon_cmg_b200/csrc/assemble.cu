@@ -351,14 +351,61 @@ __global__ void local_quad_kernel(LocalArgs a)
   }
 }
 
+// local matrices and right-hand sides of affine cells from their reference-tensor
+// coefficients: A_c[i][j] = sum_t coef_{c,t} R_t[i][j], F_c[i] = sum_u coef_{c,T+u} r_u[i]
+// (a [cells x T] x [T x nbf^2] product).  Each thread owns one entry q of the local layout
+// and keeps its tensor column R_q in registers; blocks walk a range of cells, so the cell
+// coefficients are broadcast loads and the writes are coalesced.
+__global__ void __launch_bounds__(256) affine_local_kernel(int n_cells, int nbf, int T, int Tr,
+                                                           const double *__restrict__ cellcoef,
+                                                           const double *__restrict__ R,
+                                                           const double *__restrict__ r, double *__restrict__ out,
+                                                           int cells_per_block)
+{
+  const int per = nbf * nbf + nbf;
+  const int q = blockIdx.y * blockDim.x + threadIdx.x;
+  const bool act = q < per;
+  double Rq[CD_MAXT];
+  int nt = 0, off = T;
+  if (act)
+  {
+    if (q < nbf * nbf)
+    {
+      nt = T;
+      off = 0;
+#pragma unroll
+      for (int u = 0; u < CD_MAXT; u++) Rq[u] = u < T ? R[(size_t)q * T + u] : 0.0;
+    }
+    else
+    {
+      nt = Tr;
+      const int i = q - nbf * nbf;
+#pragma unroll
+      for (int u = 0; u < CD_MAXT; u++) Rq[u] = u < Tr ? r[i * Tr + u] : 0.0;
+    }
+  }
+  const int c0 = blockIdx.x * cells_per_block, c1 = min(n_cells, c0 + cells_per_block);
+  for (int c = c0; c < c1; c++)
+  {
+    if (!act) continue;
+    const double *cf = cellcoef + (size_t)c * (T + Tr) + off;
+    double v = 0.0;
+#pragma unroll
+    for (int u = 0; u < CD_MAXT; u++)
+      if (u < nt) v += __ldg(cf + u) * Rq[u];
+    out[(size_t)c * per + q] = v;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // row gather: one group of GS threads per CSR row
 // ---------------------------------------------------------------------------
 struct GatherArgs
 {
-  int n_dof, n_active, nbf, T, Tr, mode; // mode 0 affine tensors, 1 stored local matrices
-  const int *row_ptr, *kcol, *inc_ptr, *inc, *gn;
-  const double *cellcoef, *local, *R, *r, *dir;
+  int n_dof, n_active, nbf;
+  const int *row_ptr, *kcol, *inc_ptr, *inc;
+  const unsigned char *slot; // slot map (ensure_slot_map)
+  const double *local, *dir; // local matrices + rhs per cell (n_cells x (nbf^2 + nbf))
   double *a, *rhs, *diag;
   float *a32, *diag32;
   int *err;
@@ -368,22 +415,14 @@ template <int GS, int MAXROW>
 __global__ void __launch_bounds__(256) row_gather_kernel(GatherArgs p)
 {
   extern __shared__ double smem[];
-  const int nbf = p.nbf, T = p.T, Tr = p.Tr;
-  double *Rs = smem;                                       // nbf*nbf*T (mode 0)
-  double *rs = Rs + (p.mode == 0 ? nbf * nbf * T : 0);     // nbf*Tr (mode 0)
-  double *accs = rs + (p.mode == 0 ? nbf * Tr : 0);        // groups x MAXROW
-  int *cols = (int *)(accs + (blockDim.x / GS) * MAXROW);  // groups x MAXROW
-  if (p.mode == 0)
-  {
-    for (int t = threadIdx.x; t < nbf * nbf * T; t += blockDim.x) Rs[t] = p.R[t];
-    for (int t = threadIdx.x; t < nbf * Tr; t += blockDim.x) rs[t] = p.r[t];
-  }
-  __syncthreads();
+  const int nbf = p.nbf;
+  double *accs = smem; // groups x MAXROW
   auto tile = cg::tiled_partition<GS>(cg::this_thread_block());
   const int lane = tile.thread_rank(), grp = threadIdx.x / GS;
   double *acc = accs + grp * MAXROW;
-  int *cl = cols + grp * MAXROW;
   const int ngroups = gridDim.x * (blockDim.x / GS);
+  const size_t per = (size_t)nbf * nbf + nbf;
+  constexpr int CH = GS < 4 ? GS : 4; // incidences per chunk (at most one per lane of the tile)
   for (int r = blockIdx.x * (blockDim.x / GS) + grp; r < p.n_dof; r += ngroups)
   {
     const int base = p.row_ptr[r], len = p.row_ptr[r + 1] - base;
@@ -409,55 +448,60 @@ __global__ void __launch_bounds__(256) row_gather_kernel(GatherArgs p)
       if (lane == 0) atomicExch(p.err, 2);
       continue;
     }
-    for (int s = lane; s < len; s += GS) { cl[s] = p.kcol[base + s]; acc[s] = 0.0; }
+    for (int s = lane; s < len; s += GS) acc[s] = 0.0;
     tile.sync();
     double racc = 0.0;
-    for (int t = p.inc_ptr[r]; t < p.inc_ptr[r + 1]; t++)
+    // local matrices with the slot map: every lane first loads its column's value and slot
+    // for up to CH incidences (independent loads in flight), then they are added in
+    // ascending cell order (the reference's order).  Trip counts are uniform over the tile
+    // (cnt is the row's, the column loop runs in whole tile widths), so every lane reaches
+    // every tile.sync.
+    const int t0 = p.inc_ptr[r], nt = p.inc_ptr[r + 1] - t0;
+    for (int q0 = 0; q0 < nt; q0 += CH)
     {
-      const int e = p.inc[t], K = e / nbf, i = e - K * nbf;
-      double cf[CD_MAXT];
-      if (p.mode == 0)
+      const int cnt = min(CH, nt - q0);
+      const int e_lane = lane < cnt ? __ldg(p.inc + t0 + q0 + lane) : 0;
+      double F_lane = 0.0;
+      if (lane < cnt)
       {
+        const int K = e_lane / nbf, i = e_lane - K * nbf;
+        F_lane = __ldg(p.local + (size_t)K * per + (size_t)nbf * nbf + i);
+      }
+      int eq[CH];
 #pragma unroll
-        for (int u = 0; u < CD_MAXT; u++) cf[u] = u < T ? __ldg(p.cellcoef + (size_t)K * (T + Tr) + u) : 0.0;
-      }
-      for (int j = lane; j < nbf; j += GS)
+      for (int q = 0; q < CH; q++) eq[q] = tile.shfl(e_lane, q);
+      for (int jb = 0; jb < nbf; jb += GS)
       {
-        const int col = __ldg(p.gn + (size_t)K * nbf + j);
-        int lo = 0, hi = len - 1, slot = -1;
-        while (lo <= hi)
-        {
-          int mid = (lo + hi) >> 1, v = cl[mid];
-          if (v == col) { slot = mid; break; }
-          if (v < col) lo = mid + 1; else hi = mid - 1;
-        }
-        if (slot < 0) { atomicExch(p.err, 1); continue; }
-        double v;
-        if (p.mode == 0)
-        {
-          const double *Rij = Rs + (i * nbf + j) * T;
-          v = 0.0;
+        const int j = jb + lane;
+        const bool act = j < nbf;
+        double v[CH];
+        int sl[CH];
 #pragma unroll
-          for (int u = 0; u < CD_MAXT; u++)
-            if (u < T) v += cf[u] * Rij[u];
-        }
-        else
-          v = __ldg(p.local + (size_t)K * (nbf * nbf + nbf) + i * nbf + j);
-        acc[slot] += v;
-      }
-      if (lane == 0)
-      {
-        double F;
-        if (p.mode == 0)
+        for (int q = 0; q < CH; q++)
         {
-          F = 0.0;
-          const double *rc = p.cellcoef + (size_t)K * (T + Tr) + T;
-          for (int u = 0; u < Tr; u++) F += __ldg(rc + u) * rs[i * Tr + u];
+          v[q] = 0.0;
+          sl[q] = 0;
+          if (act && q < cnt)
+          {
+            const int K = eq[q] / nbf, i = eq[q] - K * nbf;
+            v[q] = __ldg(p.local + (size_t)K * per + (size_t)i * nbf + j);
+            sl[q] = __ldg(p.slot + (size_t)(t0 + q0 + q) * nbf + j);
+          }
         }
-        else
-          F = __ldg(p.local + (size_t)K * (nbf * nbf + nbf) + nbf * nbf + i);
-        racc += F;
+#pragma unroll
+        for (int q = 0; q < CH; q++)
+          if (q < cnt)
+          {
+            if (act)
+            {
+              if (sl[q] >= len) atomicExch(p.err, 1);
+              else acc[sl[q]] += v[q];
+            }
+            tile.sync();
+          }
       }
+      // rhs in ascending cell order
+      for (int q = 0; q < cnt; q++) racc += tile.shfl(F_lane, q);
       tile.sync();
     }
     for (int s = lane; s < len; s += GS)
@@ -465,7 +509,7 @@ __global__ void __launch_bounds__(256) row_gather_kernel(GatherArgs p)
       double v = acc[s];
       p.a[base + s] = v;
       if (p.a32) p.a32[base + s] = (float)v;
-      if (cl[s] == r)
+      if (__ldg(p.kcol + base + s) == r)
       {
         p.diag[r] = v;
         if (p.diag32) p.diag32[r] = (float)v;
@@ -476,12 +520,57 @@ __global__ void __launch_bounds__(256) row_gather_kernel(GatherArgs p)
   }
 }
 
+// slot map: for every incidence t of an active row and local column j, the position of the
+// column within the row (binary search, once per pattern); 255 and the error flag when the
+// coupling is missing from the pattern
+__global__ void slot_map_kernel(int n_active, int nbf, const int *__restrict__ row_ptr, const int *__restrict__ kcol,
+                                const int *__restrict__ inc_ptr, const int *__restrict__ inc,
+                                const int *__restrict__ gn, unsigned char *__restrict__ slot, int *err)
+{
+  const int r = blockIdx.x;
+  if (r >= n_active) return;
+  const int base = row_ptr[r], len = row_ptr[r + 1] - base;
+  for (int t = inc_ptr[r]; t < inc_ptr[r + 1]; t++)
+  {
+    const int e = inc[t], K = e / nbf;
+    for (int j = threadIdx.x; j < nbf; j += blockDim.x)
+    {
+      const int col = gn[(size_t)K * nbf + j];
+      int lo = 0, hi = len - 1, pos = -1;
+      while (lo <= hi)
+      {
+        int mid = (lo + hi) >> 1, v = kcol[base + mid];
+        if (v == col) { pos = mid; break; }
+        if (v < col) lo = mid + 1; else hi = mid - 1;
+      }
+      if (pos < 0 || pos > 254) atomicExch(err, 1);
+      slot[(size_t)t * nbf + j] = (unsigned char)(pos < 0 || pos > 254 ? 255 : pos);
+    }
+  }
+}
+
+static int ensure_slot_map(cdgpu_ctx *ctx, Space &s)
+{
+  if (s.d_slot && s.slot_pattern == s.nnz) return CDGPU_OK;
+  // incidences of all DOFs = cells x nbf; the map is indexed by incidence position
+  const size_t n_inc = (size_t)s.n_cells * s.nbf;
+  int rc = dev_alloc(ctx, &s.d_slot, n_inc * s.nbf);
+  if (rc) return rc;
+  if (s.n_active > 0)
+  {
+    slot_map_kernel<<<s.n_active, 32, 0, ctx->stream>>>(s.n_active, s.nbf, s.d_row_ptr, s.d_kcol, s.d_inc_ptr,
+                                                         s.d_inc, s.d_gn, s.d_slot, ctx->d_err);
+    CD_LAUNCHED(ctx);
+  }
+  s.slot_pattern = s.nnz;
+  return CDGPU_OK;
+}
+
 template <int GS, int MAXROW>
 static int launch_gather(cdgpu_ctx *ctx, const GatherArgs &g, int n_dof)
 {
   int groups = 256 / GS;
-  size_t sm = (size_t)(g.mode == 0 ? g.nbf * g.nbf * g.T + g.nbf * g.Tr : 0) * sizeof(double) +
-              (size_t)groups * MAXROW * (sizeof(double) + sizeof(int));
+  size_t sm = (size_t)groups * MAXROW * sizeof(double);
   CD_CUDA(ctx, cudaFuncSetAttribute(row_gather_kernel<GS, MAXROW>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   int blocks_per_sm = 0;
@@ -568,6 +657,16 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, 
     CellCoefArgs a{s.dim, s.nv, s.n_cells, disctype, T, Tr, co, s.d_coords, s.d_cellcoef};
     cell_coef_kernel<<<(s.n_cells + 127) / 128, 128, 0, ctx->stream>>>(a);
     CD_LAUNCHED(ctx);
+    // local matrices of every cell, then the gather with prefetched loads
+    if (!s.d_local && (rc = dev_alloc(ctx, &s.d_local, (size_t)s.n_cells * (s.nbf * s.nbf + s.nbf))))
+      return rc;
+    const int per = s.nbf * s.nbf + s.nbf;
+    const int qblocks = (per + 255) / 256;
+    const int cpb = std::max(1, (int)((long)s.n_cells * qblocks / ((long)ctx->sm_count * 8)));
+    dim3 grid((s.n_cells + cpb - 1) / cpb, qblocks);
+    affine_local_kernel<<<grid, 256, 0, ctx->stream>>>(s.n_cells, s.nbf, T, Tr, s.d_cellcoef, s.d_ref,
+                                                       s.d_ref + (size_t)s.nbf * s.nbf * T, s.d_local, cpb);
+    CD_LAUNCHED(ctx);
   }
   else
   {
@@ -601,11 +700,12 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, 
     local_quad_kernel<<<s.n_cells, 256, sm, ctx->stream>>>(a);
     CD_LAUNCHED(ctx);
   }
+  if ((rc = ensure_slot_map(ctx, s))) return rc;
   GatherArgs g;
-  g.n_dof = s.n_dof; g.n_active = s.n_active; g.nbf = s.nbf; g.T = T; g.Tr = Tr; g.mode = fast ? 0 : 1;
-  g.row_ptr = s.d_row_ptr; g.kcol = s.d_kcol; g.inc_ptr = s.d_inc_ptr; g.inc = s.d_inc; g.gn = s.d_gn;
-  g.cellcoef = s.d_cellcoef; g.local = s.d_local; g.R = s.d_ref;
-  g.r = s.d_ref ? s.d_ref + (size_t)s.nbf * s.nbf * T : nullptr; g.dir = d_dir;
+  g.n_dof = s.n_dof; g.n_active = s.n_active; g.nbf = s.nbf;
+  g.slot = s.d_slot;
+  g.row_ptr = s.d_row_ptr; g.kcol = s.d_kcol; g.inc_ptr = s.d_inc_ptr; g.inc = s.d_inc;
+  g.local = s.d_local; g.dir = d_dir;
   g.a = s.d_a; g.rhs = s.d_rhs; g.diag = s.d_diag; g.a32 = s.d_a32; g.diag32 = s.d_diag32; g.err = ctx->d_err;
   if (s.dim == 2 && s.order == 1) rc = launch_gather<4, 16>(ctx, g, s.n_dof);
   else if (s.dim == 2) rc = launch_gather<16, 32>(ctx, g, s.n_dof);

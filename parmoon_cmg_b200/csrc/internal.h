@@ -60,6 +60,11 @@ struct Space
   CsrShape shape;
   // DOF -> (cell, local index) incidence, ascending cell per DOF
   int *d_inc_ptr = nullptr, *d_inc = nullptr;
+  // slot map of the row gather: for incidence t of an active row and local column j, the
+  // position of column gn[cell][j] within the row (rows are at most CD_MAXROW long); built
+  // from the pattern on the first assembly
+  unsigned char *d_slot = nullptr;
+  long slot_pattern = -1; // nnz of the pattern the slot map was built for
   // values
   double *d_a = nullptr, *d_rhs = nullptr, *d_diag = nullptr;
   float *d_a32 = nullptr, *d_diag32 = nullptr;
