@@ -329,15 +329,16 @@ __global__ void b_coarse(BTab t, const BCtl *__restrict__ ctl, const BLevel *__r
     const int n = L.n, na = L.na;
     for (int i = threadIdx.x; i < n; i += blockDim.x) sb[i] = (double)L.rhs[i];
     __syncthreads();
-    for (int i = threadIdx.x; i < na; i += blockDim.x)
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nw = blockDim.x / 32;
+    for (int i = warp; i < na; i += nw)
     {
-      double v = sb[i];
-      for (int j = L.dirst[i]; j < L.rp[i + 1]; j++) v -= L.a64[j] * sb[L.kc[j]];
-      sb[n + i] = v;
+      double v = 0.0;
+      for (int j = L.dirst[i] + lane; j < L.rp[i + 1]; j += 32) v += L.a64[j] * sb[L.kc[j]];
+      v = bsum<32>(v);
+      if (lane == 0) sb[n + i] = sb[i] - v;
     }
     for (int i = na + threadIdx.x; i < n; i += blockDim.x) L.v[out][i] = (float)sb[i];
     __syncthreads();
-    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nw = blockDim.x / 32;
     for (int r = warp; r < na; r += nw)
     {
       double s = 0;

@@ -61,6 +61,39 @@ __global__ void jacobi_first_kernel(int n, int n_active, const int *__restrict__
   xo[r] = omega * s / diag[r];
 }
 
+// start of a cycle on the finest level fused with its first damped-Jacobi sweep: the
+// right-hand side is the (FP64) input vector read through the pointer slot io[0]; the start
+// vector is zero on active rows and the right-hand side on Dirichlet rows
+// (MultiGridScaIte.C:79-85), so the sweep gives y = omega (f - A_D f_D) / a_rr on active rows
+// (A_D: the Dirichlet columns, from dir_start[r]) and y = f on Dirichlet rows.  8 threads
+// per row; rows visited warp by warp (every lane reaches every shuffle).
+template <typename T>
+__global__ void __launch_bounds__(256) mg_start_first_kernel(int n, int n_active, const int *__restrict__ rp,
+                                                             const int *__restrict__ kc,
+                                                             const int *__restrict__ dir_start,
+                                                             const T *__restrict__ a, const T *__restrict__ diag,
+                                                             double *const *__restrict__ io, T *__restrict__ rhs,
+                                                             T *__restrict__ y, T omega)
+{
+  const double *in = io[0];
+  const int lane = threadIdx.x % 8, sub = (threadIdx.x % 32) / 8;
+  const long nwarp = (long)gridDim.x * blockDim.x / 32;
+  for (long base = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32 * 4; base < n; base += nwarp * 4)
+  {
+    const int r = (int)base + sub;
+    T t = 0;
+    if (r < n_active)
+      for (int j = dir_start[r] + lane; j < rp[r + 1]; j += 8) t += a[j] * (T)in[kc[j]];
+    t = group_sum<8>(t);
+    if (r < n && lane == 0)
+    {
+      const T f = (T)in[r];
+      rhs[r] = f;
+      y[r] = r < n_active ? omega * (f - t) / diag[r] : f;
+    }
+  }
+}
+
 // exact coarse solve (SolveExact, MGLevel3D.C:839) with the explicit FP64 inverse of the
 // active block: Dirichlet rows are identity rows, so sol_D = rhs_D and
 // sol_A = inv(A_AA) (rhs_A - A_AD rhs_D); A_AD is read from the CSR values of each active
@@ -74,15 +107,18 @@ __global__ void coarse_exact_kernel(int n, int na, const int *__restrict__ rp, c
   extern __shared__ double b[];
   for (int i = threadIdx.x; i < n; i += blockDim.x) b[i] = (double)rhs[i];
   __syncthreads();
-  for (int i = threadIdx.x; i < na; i += blockDim.x)
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nw = blockDim.x / 32;
+  // one warp per active row for the Dirichlet columns (a row of the coarsest level can have
+  // ~100 of them)
+  for (int i = warp; i < na; i += nw)
   {
-    double v = b[i];
-    for (int j = dir_start[i]; j < rp[i + 1]; j++) v -= a[j] * b[kc[j]];
-    b[n + i] = v;
+    double v = 0.0;
+    for (int j = dir_start[i] + lane; j < rp[i + 1]; j += 32) v += a[j] * b[kc[j]];
+    v = group_sum<32>(v);
+    if (lane == 0) b[n + i] = b[i] - v;
   }
   for (int i = na + threadIdx.x; i < n; i += blockDim.x) sol[i] = (T)b[i];
   __syncthreads();
-  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nw = blockDim.x / 32;
   for (int r = warp; r < na; r += nw)
   {
     double s = 0;
@@ -470,6 +506,7 @@ struct CycleState
 {
   const cdgpu_solver_params *p;
   int rec[64];
+  int pre_done[64];    // pre-smoothing sweeps already done (fused into the cycle's start)
   bool sol_zero[64];   // active part and Dirichlet part zero
   bool active_zero[64];
 };
@@ -523,7 +560,8 @@ template <typename T> static int cycle(cdgpu_ctx *ctx, Hierarchy &h, CycleState 
   const Space &s = *L.sp, &sc = *C.sp;
   LevelVec<T> &v = vecs<T>(L), &vc = vecs<T>(C);
   int rc;
-  if ((rc = smooth<T>(ctx, h, cs, i, cs.p->pre))) return rc;
+  if ((rc = smooth<T>(ctx, h, cs, i, cs.p->pre - cs.pre_done[i]))) return rc;
+  cs.pre_done[i] = 0;
   csr_defect<T>(ctx, s, v.sol, v.rhs, v.def, nullptr, csr_grid(ctx, s.shape, s.n_dof));
   CD_LAUNCHED(ctx);
   csr_restrict<T>(ctx, L, sc, v.def, vc.rhs, vc.sol);
@@ -548,15 +586,35 @@ template <typename T> static int mg_record(cdgpu_ctx *ctx, Hierarchy &h, const c
   Level &F = h.lev[L - 1];
   LevelVec<T> &v = vecs<T>(F);
   int n = F.sp->n_dof;
-  mg_start_kernel<T><<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, F.sp->n_active, h.d_io, v.rhs, v.sol);
-  CD_LAUNCHED(ctx);
   CycleState cs;
   cs.p = &p;
   // SetRecursion(levels = L-1), MultiGrid3D.C:691-703
   cs.rec[1] = 1;
   for (int k = 2; k <= L - 1; k++) cs.rec[k] = p.cycle > 0 ? p.cycle : 2;
-  for (int k = 0; k < L; k++) cs.sol_zero[k] = cs.active_zero[k] = false;
-  cs.active_zero[L - 1] = true;
+  for (int k = 0; k < L; k++)
+  {
+    cs.sol_zero[k] = cs.active_zero[k] = false;
+    cs.pre_done[k] = 0;
+  }
+  if (L > 1 && p.pre >= 1)
+  {
+    // zero start and the first pre-smoothing sweep of the finest level in one kernel
+    const Space &s = *F.sp;
+    const long groups = (long)ctx->sm_count * 8 * (256 / 8);
+    const int grid = (int)std::max<long>(1, std::min<long>((n + 31) / 32, groups / 32));
+    mg_start_first_kernel<T><<<grid, 256, 0, ctx->stream>>>(n, s.n_active, s.d_row_ptr, s.d_kcol, s.d_dir_start,
+                                                           mat<T>(s), dg<T>(s), h.d_io, v.rhs, v.alt,
+                                                           (T)p.omega);
+    CD_LAUNCHED(ctx);
+    std::swap(v.sol, v.alt);
+    cs.pre_done[L - 1] = 1;
+  }
+  else
+  {
+    mg_start_kernel<T><<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, F.sp->n_active, h.d_io, v.rhs, v.sol);
+    CD_LAUNCHED(ctx);
+    cs.active_zero[L - 1] = true;
+  }
   int rc = cycle<T>(ctx, h, cs, L - 1);
   if (rc) return rc;
   mg_finish_kernel<T><<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, v.sol, h.d_io);
