@@ -639,6 +639,8 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, 
   const RefElement &re = s.re;
   bool fast = s.all_affine && s.co.kind == CDGPU_COEFF_CONSTANT;
   int T = n_tensors(s.dim, disctype), Tr = n_rhs_tensors(s.dim, disctype);
+  // the matrix-free operator follows the cell coefficients of an affine assembly only
+  s.mf_T = fast ? T : 0;
   Coef co = to_coef(s.co);
   if (fast)
   {

@@ -1218,6 +1218,7 @@ static int assemble_to(cdgpu_ctx *ctx, Space &s, int disctype, const cdgpu_coeff
   rc = assemble_space(ctx, s, disctype, nullptr, false);
   s.d_a = sa; s.d_rhs = srhs; s.d_diag = sd; s.d_a32 = sa32; s.d_diag32 = sd32;
   s.co = sco; s.co_set = sset; s.assembled = sasm;
+  s.mf_T = 0; // the cell coefficients now belong to the batch instance
   return rc;
 }
 

@@ -76,6 +76,13 @@ struct Space
   double *d_tab = nullptr;
   // assembly scratch
   double *d_cellcoef = nullptr; // affine path: n_cells x (T + Tr)
+  // matrix-free FP32 operator for the FP32 multigrid cycle (mf.cuh), available after an
+  // affine constant-coefficient assembly: mf_T = its number of reference tensors (0: none)
+  int mf_T = 0;
+  long mf_version = -1;         // assembly the FP32 copies were made from
+  float *d_cf32 = nullptr;      // n_cells x T cell coefficients
+  float *d_R32 = nullptr;       // T x nbf x nbf reference tensors, [t][i][j]
+  float *d_ybuf = nullptr;      // nbf x n_cells per-cell products
   double *d_local = nullptr;    // quadrature path: n_cells x (nbf*nbf + nbf)
   double *d_dir = nullptr;      // Dirichlet values
   double *d_ref = nullptr;      // reference tensors (affine path)
@@ -127,6 +134,7 @@ struct Hierarchy
   double *d_x = nullptr, *d_b = nullptr; // host-API staging vectors
   // captured multigrid cycle per precision (0 FP64, 1 FP32) and its in/out pointer slot
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  unsigned mf_mask = 0; // levels whose FP32 cycle in gexec[1] uses the matrix-free operator
   cdgpu_solver_params gparams[2] = {};
   long long graph_nodes[2] = {0, 0};
   double **d_io = nullptr;

@@ -24,8 +24,11 @@
 #include <cmath>
 #include <cstring>
 
+#include <type_traits>
+
 #include "internal.h"
 #include "csr.cuh"
+#include "mf.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -481,6 +484,18 @@ template <typename T> static int jacobi_sweep(cdgpu_ctx *ctx, Level &L, T omega)
 {
   LevelVec<T> &v = vecs<T>(L);
   const Space &s = *L.sp;
+  if constexpr (std::is_same<T, float>::value)
+  {
+    if (use_mf(s))
+    {
+      mf_apply_cells(ctx, s, v.sol);
+      CD_LAUNCHED(ctx);
+      mf_rows<MF_JACOBI>(ctx, s, v.sol, v.rhs, s.d_diag32, v.alt, omega);
+      CD_LAUNCHED(ctx);
+      std::swap(v.sol, v.alt);
+      return CDGPU_OK;
+    }
+  }
   csr_jacobi<T>(ctx, s, v.sol, v.rhs, v.alt, omega);
   CD_LAUNCHED(ctx);
   std::swap(v.sol, v.alt);
@@ -562,7 +577,18 @@ template <typename T> static int cycle(cdgpu_ctx *ctx, Hierarchy &h, CycleState 
   int rc;
   if ((rc = smooth<T>(ctx, h, cs, i, cs.p->pre - cs.pre_done[i]))) return rc;
   cs.pre_done[i] = 0;
-  csr_defect<T>(ctx, s, v.sol, v.rhs, v.def, nullptr, csr_grid(ctx, s.shape, s.n_dof));
+  bool done = false;
+  if constexpr (std::is_same<T, float>::value)
+  {
+    if (use_mf(s))
+    {
+      mf_apply_cells(ctx, s, v.sol);
+      CD_LAUNCHED(ctx);
+      mf_rows<MF_DEFECT>(ctx, s, v.sol, v.rhs, s.d_diag32, v.def, 0.f);
+      done = true;
+    }
+  }
+  if (!done) csr_defect<T>(ctx, s, v.sol, v.rhs, v.def, nullptr, csr_grid(ctx, s.shape, s.n_dof));
   CD_LAUNCHED(ctx);
   csr_restrict<T>(ctx, L, sc, v.def, vc.rhs, vc.sol);
   CD_LAUNCHED(ctx);
@@ -1090,6 +1116,44 @@ static int fixed_point(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &
   return CDGPU_OK;
 }
 
+// FP32 copies for the matrix-free operator of every level that has one; the captured FP32
+// cycle is recaptured when the set of such levels changes
+static int refresh_mf(cdgpu_ctx *ctx, Hierarchy &h)
+{
+  unsigned mask = 0;
+  for (size_t l = 0; l < h.lev.size(); l++)
+  {
+    Space &s = *h.lev[l].sp;
+    if (s.mf_T <= 0 || s.n_cells < kMfMinCells || !mf_shape_ok(s.nbf, s.mf_T)) continue;
+    int rc;
+    if (!s.d_ybuf)
+    {
+      if ((rc = dev_alloc(ctx, &s.d_cf32, (size_t)s.n_cells * CD_MAXT)) ||
+          (rc = dev_alloc(ctx, &s.d_R32, (size_t)CD_MAXT * s.nbf * s.nbf)) ||
+          (rc = dev_alloc(ctx, &s.d_ybuf, (size_t)s.nbf * s.n_cells)))
+        return rc;
+    }
+    if (s.mf_version != s.assembly_version)
+    {
+      const int T = s.mf_T, Tr = n_rhs_tensors(s.dim, s.ref_disctype);
+      const long total = (long)s.n_cells * T + (long)T * s.nbf * s.nbf;
+      const int grid = (int)std::min<long>((total + 255) / 256, (long)ctx->sm_count * 8);
+      mf_convert_kernel<<<grid, 256, 0, ctx->stream>>>(s.n_cells, T, Tr, s.nbf, s.d_cellcoef, s.d_ref, s.d_cf32,
+                                                        s.d_R32);
+      CD_LAUNCHED(ctx);
+      s.mf_version = s.assembly_version;
+    }
+    mask |= 1u << l;
+  }
+  if (mask != h.mf_mask && h.gexec[1])
+  {
+    cudaGraphExecDestroy(h.gexec[1]);
+    h.gexec[1] = nullptr;
+  }
+  h.mf_mask = mask;
+  return CDGPU_OK;
+}
+
 int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *d_rhs, double *d_sol,
               cdgpu_solve_info *info)
 {
@@ -1104,6 +1168,7 @@ int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const 
     return fail(ctx, CDGPU_ERR_UNSUPPORTED, "solve: coarse smoother loop needs a coarsest level below 6000 DOFs");
   int rc;
   if (p.coarse_smoother == 17 && (rc = refresh_coarse_inverse(ctx, h))) return rc;
+  if (p.precision == 1 && (rc = refresh_mf(ctx, h))) return rc;
   cdgpu_solve_info local{};
   if (!info) info = &local;
   if (p.solver == 11) rc = fixed_point(ctx, h, p, d_rhs, d_sol, info);

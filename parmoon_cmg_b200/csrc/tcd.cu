@@ -206,6 +206,7 @@ int cdgpu_tcd_step_device(cdgpu_ctx *ctx, int tcd_id, const cdgpu_solver_params 
   {
     Space &s = *h.lev[l].sp;
     if ((rc = matadd(ctx, s, -gamma + tau * theta1, t->A[l], t->M[l]))) return rc;
+    s.mf_T = 0; // the system matrix is a combination, not one affine assembly
     install_system_kernel<<<(s.n_dof + 255) / 256, 256, 0, ctx->stream>>>(s.n_dof, s.d_row_ptr, s.d_kcol, t->M[l],
                                                                         s.d_a, s.d_a32, s.d_diag, s.d_diag32);
     CD_LAUNCHED(ctx);

@@ -269,3 +269,22 @@ def test_errors_are_reported(ctx):
     bad["global_numbers"][0] = sp["n_dof"] + 5
     with pytest.raises(_lib.CdgpuError):
         ctx.upload_space(bad)
+
+
+def test_matrix_free_cycle_q2_hex(ctx):
+    """The mixed form's FP32 cycle applies the Q2-hexahedron operator matrix-free on levels of
+    at least 16,384 cells (per-cell products from the assembly's reference tensors); its
+    solution equals the FP64 form's (CSR throughout) within the mixed bar, with about the same
+    number of FGMRES iterations."""
+    co = coeffs(0, eps=1e-2, b=(0.57735026918962573,) * 3, f=1.0, delta0=1.0 / 3.0)
+    spaces, parents, sids, mg = structured_case(ctx, 3, 2, 2, 5, co, 1)
+    ctx.assemble_hierarchy(mg, 1, 2)
+    nd = spaces[-1]["n_dof"]
+    rhs = ctx.assemble(sids[-1], 1, nd, 1, want_entries=False)[1]
+    sol0 = np.zeros(nd)
+    prm = dict(stop_rule=1, red_factor=1e-12, maxit=200)
+    x64, i64 = ctx.solve(mg, solver_params(precision=0, **prm), rhs, sol0)
+    xm, im = ctx.solve(mg, solver_params(precision=1, **prm), rhs, sol0)
+    assert i64.status == 0 and im.status == 0
+    assert rel(xm, x64) <= TOL_MIXED
+    assert abs(im.iterations - i64.iterations) <= 2
