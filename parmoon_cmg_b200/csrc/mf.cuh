@@ -114,6 +114,164 @@ __global__ void __launch_bounds__(224) mf_cell27_kernel(int n_cells, const int *
   }
 }
 
+// ---------------------------------------------------------------------------
+// The same per-cell products on the 5th-generation tensor cores (tcgen05, kind::tf32):
+// for a tile of 128 cells, D[cell][t*32 + i] = sum_k X[cell][k] R_t[i][k] is one
+// 128 x 32T x 32 product (K = 27 local DOFs padded to 32), A = the gathered cell values and
+// B = the reference tensors, both K-major in shared memory in the no-swizzle core-matrix
+// layout (8 rows x 16 bytes per core matrix), the accumulator in tensor memory (TMEM).  One
+// thread issues 2 x 4 MMAs (two N halves of 16T columns, four K steps of 8) and commits them
+// to an mbarrier; after the (bounded) wait each of the 4 warps reads its 32 TMEM lanes (one
+// cell per thread) tensor by tensor with tcgen05.ld and contracts them with the cell's
+// coefficients: y[i] = sum_t coef_t D[t*32 + i].  Inputs are rounded to TF32 (10-bit
+// mantissa); only the FP32 multigrid cycle uses this operator.  Persistent CTAs, one per SM
+// (TMEM: 512 columns per CTA).
+__device__ __forceinline__ uint32_t mf_smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// byte offset of element (r, k) of an R-row, K = 32 K-major operand in core-matrix layout
+__device__ __forceinline__ int mf_core_off(int r, int k, int R)
+{
+  return (((k >> 2) * (R >> 3) + (r >> 3)) * 8 + (r & 7)) * 16 + (k & 3) * 4;
+}
+
+__device__ __forceinline__ uint64_t mf_sdesc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes)
+{
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46; // descriptor version of sm_100; layout type 0 = no swizzle
+  return d;
+}
+
+template <int T>
+__global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const int *__restrict__ gn,
+                                                              const float *__restrict__ cf32,
+                                                              const float *__restrict__ R32,
+                                                              const float *__restrict__ x, float *__restrict__ ybuf,
+                                                              int *__restrict__ err)
+{
+  constexpr int MT = 128, KP = 32, NB = 27, N = 32 * T, NH = N / 2;
+  extern __shared__ __align__(1024) unsigned char mf_sm[];
+  unsigned char *As = mf_sm;                    // 128 x 32 x 4 = 16 KB
+  unsigned char *Bs = mf_sm + MT * KP * 4;      // N x 32 x 4
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  // B = the tensors, zero-padded rows i >= 27 and columns k >= 27; A zero everywhere once
+  for (int e = tid; e < N * KP; e += blockDim.x)
+  {
+    const int n = e / KP, k = e % KP, t = n / 32, i = n % 32;
+    const float v = (i < NB && k < NB) ? R32[(t * NB + i) * NB + k] : 0.f;
+    *(float *)(Bs + mf_core_off(n, k, N)) = v;
+  }
+  for (int e = tid; e < MT * KP; e += blockDim.x) ((float *)As)[e] = 0.f;
+  if (warp == 0)
+  {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(mf_smem_u32(&tmem_base)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mf_smem_u32(&mbar)), "r"(1));
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(NH >> 3) << 17) | ((uint32_t)(MT >> 4) << 24);
+  const int n_tiles = (n_cells + MT - 1) / MT;
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
+  {
+    const int c0 = tile * MT;
+    // gather the tile's cell values, one cell per thread: all 27 DOF numbers, then all 27
+    // values in flight at once (k < 27; the padding stays zero)
+    {
+      const int r = tid, c = c0 + r;
+      int g[NB];
+      float v[NB];
+#pragma unroll
+      for (int k = 0; k < NB; k++) g[k] = c < n_cells ? __ldg(gn + (size_t)c * NB + k) : -1;
+#pragma unroll
+      for (int k = 0; k < NB; k++) v[k] = g[k] >= 0 ? __ldg(x + g[k]) : 0.f;
+#pragma unroll
+      for (int k = 0; k < NB; k++) *(float *)(As + mf_core_off(r, k, MT)) = v[k];
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0 && ok)
+    {
+      const uint32_t a0 = mf_smem_u32(As), b0 = mf_smem_u32(Bs);
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int s = 0; s < KP / 8; s++)
+        {
+          const uint64_t da = mf_sdesc(a0 + s * 2 * (MT / 8) * 128, (MT / 8) * 128, 128);
+          const uint64_t db = mf_sdesc(b0 + s * 2 * (N / 8) * 128 + h * (NH / 8) * 128, (N / 8) * 128, 128);
+          const uint32_t acc = s > 0 ? 1u : 0u;
+          asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + h * NH),
+                       "l"(da), "l"(db), "r"(idesc), "r"(acc));
+        }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       mf_smem_u32(&mbar))
+                   : "memory");
+    }
+    // bounded wait for this tile's products (an error flag instead of a hang)
+    uint32_t done = 0;
+    if (ok)
+      for (long it = 0; it < (1L << 24) && !done; it++)
+        asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, P1;\n\t}"
+                     : "=r"(done)
+                     : "r"(mf_smem_u32(&mbar)), "r"(phase)
+                     : "memory");
+    if (!done)
+    {
+      if (ok && lane == 0) atomicExch(err, 3);
+      ok = false;
+    }
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int c = c0 + warp * 32 + lane;
+    if (ok)
+    {
+      float y[NB];
+#pragma unroll
+      for (int i = 0; i < NB; i++) y[i] = 0.f;
+#pragma unroll 1
+      for (int t = 0; t < T; t++)
+      {
+        uint32_t v[32];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + t * 32;
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+                     "%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                     : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                       "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                       "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                       "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                       "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                     : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const float cf = c < n_cells ? __ldg(cf32 + (size_t)c * T + t) : 0.f;
+#pragma unroll
+        for (int i = 0; i < NB; i++) y[i] += cf * __uint_as_float(v[i]);
+      }
+      if (c < n_cells)
+#pragma unroll
+        for (int i = 0; i < NB; i++) ybuf[(size_t)i * n_cells + c] = y[i];
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+}
+
+template <int T> inline size_t mf_tc_smem() { return (size_t)128 * 32 * 4 + (size_t)32 * T * 32 * 4; }
+
 enum { MF_JACOBI = 0, MF_DEFECT = 1 };
 
 template <int NBF, int MODE>
@@ -173,6 +331,24 @@ inline bool use_mf(const Space &s)
 // y = A x per cell (phase 1)
 inline void mf_apply_cells(cdgpu_ctx *ctx, const Space &s, const float *x)
 {
+  if (s.nbf == 27 && ctx->d_err)
+  {
+    // tensor cores: persistent CTAs, one per SM (the shared memory request keeps a second CTA
+    // off the SM, so every CTA can allocate its 512 TMEM columns at once)
+    const int grid = std::max(1, std::min((s.n_cells + 127) / 128, ctx->sm_count));
+    if (s.mf_T == 10)
+    {
+      mf_cell27_tc_kernel<10><<<grid, 128, 120 * 1024, ctx->stream>>>(s.n_cells, s.d_gn, s.d_cf32, s.d_R32, x,
+                                                                      s.d_ybuf, ctx->d_err);
+      return;
+    }
+    if (s.mf_T == 13)
+    {
+      mf_cell27_tc_kernel<13><<<grid, 128, 120 * 1024, ctx->stream>>>(s.n_cells, s.d_gn, s.d_cf32, s.d_R32, x,
+                                                                      s.d_ybuf, ctx->d_err);
+      return;
+    }
+  }
   if (s.nbf == 27)
   {
     const int g27 = (s.n_cells + 63) / 64;

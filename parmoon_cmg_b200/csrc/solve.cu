@@ -1145,6 +1145,19 @@ static int refresh_mf(cdgpu_ctx *ctx, Hierarchy &h)
     }
     mask |= 1u << l;
   }
+  if (mask)
+  {
+    // shared memory of the tensor-core kernel (set outside any capture)
+    CD_CUDA(ctx, cudaFuncSetAttribute(mf_cell27_tc_kernel<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
+    CD_CUDA(ctx, cudaFuncSetAttribute(mf_cell27_tc_kernel<13>, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
+    if (!ctx->d_err)
+    {
+      int rc = dev_alloc(ctx, &ctx->d_err, 1);
+      if (rc) return rc;
+      CD_CUDA(ctx, cudaMallocHost((void **)&ctx->h_err, sizeof(int)));
+      CD_CUDA(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    }
+  }
   if (mask != h.mf_mask && h.gexec[1])
   {
     cudaGraphExecDestroy(h.gexec[1]);
