@@ -32,7 +32,7 @@ static Hierarchy *get_mg(cdgpu_ctx *ctx, int id)
 static void free_space(Space *s)
 {
   if (!s) return;
-  void *ptrs[] = {s->d_coords, s->d_gn,  s->d_row_ptr, s->d_kcol,     s->d_dir_start, s->d_slot, s->d_inc_ptr,
+  void *ptrs[] = {s->d_coords, s->d_gn,  s->d_row_ptr, s->d_kcol,     s->d_dir_start, s->d_dir_rows, s->d_slot, s->d_inc_ptr,
                   s->d_inc,    s->d_a,   s->d_rhs,     s->d_diag,     s->d_a32,       s->d_diag32,
                   s->d_tab,    s->d_cellcoef, s->d_local, s->d_dir, s->d_ref, s->d_quadtab,
                   s->d_cf32,   s->d_R32, s->d_ybuf};
@@ -60,6 +60,7 @@ static void free_mg(Hierarchy *h)
     if (p) cudaFree(p);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
   if (h->h_io) cudaFreeHost(h->h_io);
+  if (h->h_cflag) cudaFreeHost(h->h_cflag);
   delete h;
 }
 
@@ -194,19 +195,25 @@ static int install_pattern(cdgpu_ctx *ctx, Space &s)
 {
   int rc;
   s.nnz = s.h_row_ptr[s.n_dof];
-  std::vector<int> dir_start(s.n_dof);
+  std::vector<int> dir_start(s.n_dof), dir_rows;
   for (int r = 0; r < s.n_dof; r++)
   {
     int j = s.h_row_ptr[r + 1];
     while (j > s.h_row_ptr[r] && s.h_kcol[j - 1] >= s.n_active) j--;
     dir_start[r] = j;
+    if (r < s.n_active && j < s.h_row_ptr[r + 1]) dir_rows.push_back(r);
   }
+  if (s.d_dir_rows) { cudaFree(s.d_dir_rows); s.d_dir_rows = nullptr; }
+  s.n_dir_rows = (int)dir_rows.size();
   if ((rc = dev_alloc(ctx, &s.d_row_ptr, s.n_dof + 1)) || (rc = dev_alloc(ctx, &s.d_kcol, s.nnz)) ||
-      (rc = dev_alloc(ctx, &s.d_dir_start, s.n_dof)))
+      (rc = dev_alloc(ctx, &s.d_dir_start, s.n_dof)) ||
+      (rc = dev_alloc(ctx, &s.d_dir_rows, std::max<size_t>(1, dir_rows.size()))))
     return rc;
   CD_CUDA(ctx, cudaMemcpy(s.d_row_ptr, s.h_row_ptr.data(), sizeof(int) * (s.n_dof + 1), cudaMemcpyHostToDevice));
   CD_CUDA(ctx, cudaMemcpy(s.d_kcol, s.h_kcol.data(), sizeof(int) * s.nnz, cudaMemcpyHostToDevice));
   CD_CUDA(ctx, cudaMemcpy(s.d_dir_start, dir_start.data(), sizeof(int) * s.n_dof, cudaMemcpyHostToDevice));
+  if (!dir_rows.empty())
+    CD_CUDA(ctx, cudaMemcpy(s.d_dir_rows, dir_rows.data(), sizeof(int) * dir_rows.size(), cudaMemcpyHostToDevice));
   s.shape = csr_shape(s.h_row_ptr.data(), s.n_dof);
   // a new pattern invalidates values sized for the old one and the slot map
   s.slot_pattern = -1;

@@ -57,6 +57,8 @@ struct Space
   std::vector<int> h_row_ptr, h_kcol;
   int *d_row_ptr = nullptr, *d_kcol = nullptr;
   int *d_dir_start = nullptr; // first slot of each row whose column is a Dirichlet DOF
+  int *d_dir_rows = nullptr;  // the active rows that have Dirichlet columns
+  int n_dir_rows = 0;
   CsrShape shape;
   // DOF -> (cell, local index) incidence, ascending cell per DOF
   int *d_inc_ptr = nullptr, *d_inc = nullptr;
@@ -140,6 +142,8 @@ struct Hierarchy
   double **d_io = nullptr;
   double **h_io = nullptr; // pinned ring of 64 (in, out) pairs
   unsigned io_slot = 0;
+  int *h_cflag = nullptr;     // pinned copy of the coarse inversion's zero-pivot flag
+  bool cflag_pending = false; // copy enqueued, not yet checked
 };
 
 // ---------------------------------------------------------------------------

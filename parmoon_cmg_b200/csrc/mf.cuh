@@ -181,22 +181,30 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
   const int n_tiles = (n_cells + MT - 1) / MT;
   uint32_t phase = 0;
   bool ok = true;
+  // the next tile's cell values and coefficients, one cell per thread (thread r gathers and
+  // later contracts cell c0 + r): loaded before the current tile's products are awaited, so
+  // the gather latency overlaps the tensor-core work and the epilogue
+  float vn[NB], cn[T];
+  auto prefetch = [&](int tile) {
+    const int c = tile * MT + tid;
+    const bool in = tile < n_tiles && c < n_cells;
+    int g[NB];
+#pragma unroll
+    for (int k = 0; k < NB; k++) g[k] = in ? __ldg(gn + (size_t)c * NB + k) : -1;
+#pragma unroll
+    for (int t = 0; t < T; t++) cn[t] = in ? __ldg(cf32 + (size_t)c * T + t) : 0.f;
+#pragma unroll
+    for (int k = 0; k < NB; k++) vn[k] = g[k] >= 0 ? __ldg(x + g[k]) : 0.f;
+  };
+  prefetch(blockIdx.x);
   for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
   {
     const int c0 = tile * MT;
-    // gather the tile's cell values, one cell per thread: all 27 DOF numbers, then all 27
-    // values in flight at once (k < 27; the padding stays zero)
-    {
-      const int r = tid, c = c0 + r;
-      int g[NB];
-      float v[NB];
+    float cf[T];
 #pragma unroll
-      for (int k = 0; k < NB; k++) g[k] = c < n_cells ? __ldg(gn + (size_t)c * NB + k) : -1;
+    for (int t = 0; t < T; t++) cf[t] = cn[t];
 #pragma unroll
-      for (int k = 0; k < NB; k++) v[k] = g[k] >= 0 ? __ldg(x + g[k]) : 0.f;
-#pragma unroll
-      for (int k = 0; k < NB; k++) *(float *)(As + mf_core_off(r, k, MT)) = v[k];
-    }
+    for (int k = 0; k < NB; k++) *(float *)(As + mf_core_off(tid, k, MT)) = vn[k];
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -219,6 +227,7 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
                        mf_smem_u32(&mbar))
                    : "memory");
     }
+    prefetch(tile + gridDim.x);
     // bounded wait for this tile's products (an error flag instead of a hang)
     uint32_t done = 0;
     if (ok)
@@ -255,9 +264,11 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
                        "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                      : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        const float cf = c < n_cells ? __ldg(cf32 + (size_t)c * T + t) : 0.f;
+        float cft = cf[0];
 #pragma unroll
-        for (int i = 0; i < NB; i++) y[i] += cf * __uint_as_float(v[i]);
+        for (int u = 1; u < T; u++) cft = t == u ? cf[u] : cft;
+#pragma unroll
+        for (int i = 0; i < NB; i++) y[i] += cft * __uint_as_float(v[i]);
       }
       if (c < n_cells)
 #pragma unroll
@@ -287,10 +298,26 @@ __global__ void mf_row_kernel(int n, int na, int n_cells, const int *__restrict_
     out[r] = MODE == MF_JACOBI ? f[r] : f[r] - x[r];
     return;
   }
-  float s = 0.f;
-  for (int t = inc_ptr[r]; t < inc_ptr[r + 1]; t++)
+  // the first 8 incidences (every DOF of a structured hexahedral or quadrilateral mesh) are
+  // loaded at once, then added in ascending cell order; longer lists continue one by one
+  const int b = inc_ptr[r], e = inc_ptr[r + 1];
+  int ei[8];
+  float yv[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) ei[j] = b + j < e ? __ldg(inc + b + j) : -1;
+#pragma unroll
+  for (int j = 0; j < 8; j++)
   {
-    const int e = inc[t], K = e / NBF, li = e - K * NBF;
+    const int K = ei[j] / NBF, li = ei[j] - K * NBF;
+    yv[j] = ei[j] >= 0 ? __ldg(ybuf + (size_t)li * n_cells + K) : 0.f;
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int j = 0; j < 8; j++)
+    if (b + j < e) s += yv[j];
+  for (int t = b + 8; t < e; t++)
+  {
+    const int K = inc[t] / NBF, li = inc[t] - K * NBF;
     s += ybuf[(size_t)li * n_cells + K];
   }
   out[r] = MODE == MF_JACOBI ? x[r] + omega * (f[r] - s) / diag[r] : f[r] - s;

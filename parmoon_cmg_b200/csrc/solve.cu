@@ -68,10 +68,15 @@ __global__ void jacobi_first_kernel(int n, int n_active, const int *__restrict__
 // right-hand side is the (FP64) input vector read through the pointer slot io[0]; the start
 // vector is zero on active rows and the right-hand side on Dirichlet rows
 // (MultiGridScaIte.C:79-85), so the sweep gives y = omega (f - A_D f_D) / a_rr on active rows
-// (A_D: the Dirichlet columns, from dir_start[r]) and y = f on Dirichlet rows.  8 threads
-// per row; rows visited warp by warp (every lane reaches every shuffle).
+// (A_D: the Dirichlet columns, from dir_start[r]) and y = f on Dirichlet rows.
+// Blocks [0, nb1): one thread per row, every row's rhs, y on the rows without Dirichlet
+// columns; the remaining blocks: 8 threads per row of the list dir_rows (the active rows
+// with Dirichlet columns), each thread issuing its first 4 column/value loads at once.
+// Every lane of a warp of the second part reaches the shuffle.
 template <typename T>
-__global__ void __launch_bounds__(256) mg_start_first_kernel(int n, int n_active, const int *__restrict__ rp,
+__global__ void __launch_bounds__(256) mg_start_first_kernel(int n, int n_active, int nb1, int n_dir_rows,
+                                                             const int *__restrict__ dir_rows,
+                                                             const int *__restrict__ rp,
                                                              const int *__restrict__ kc,
                                                              const int *__restrict__ dir_start,
                                                              const T *__restrict__ a, const T *__restrict__ diag,
@@ -79,22 +84,42 @@ __global__ void __launch_bounds__(256) mg_start_first_kernel(int n, int n_active
                                                              T *__restrict__ y, T omega)
 {
   const double *in = io[0];
-  const int lane = threadIdx.x % 8, sub = (threadIdx.x % 32) / 8;
-  const long nwarp = (long)gridDim.x * blockDim.x / 32;
-  for (long base = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32 * 4; base < n; base += nwarp * 4)
+  if ((int)blockIdx.x < nb1)
   {
-    const int r = (int)base + sub;
-    T t = 0;
-    if (r < n_active)
-      for (int j = dir_start[r] + lane; j < rp[r + 1]; j += 8) t += a[j] * (T)in[kc[j]];
-    t = group_sum<8>(t);
-    if (r < n && lane == 0)
-    {
-      const T f = (T)in[r];
-      rhs[r] = f;
-      y[r] = r < n_active ? omega * (f - t) / diag[r] : f;
-    }
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const T f = (T)in[r];
+    rhs[r] = f;
+    if (r >= n_active)
+      y[r] = f;
+    else if (dir_start[r] == rp[r + 1])
+      y[r] = omega * (f - T(0)) / diag[r];
+    return;
   }
+  constexpr int U = 4;
+  const int lane = threadIdx.x % 8;
+  const int q = (int)(((long)(blockIdx.x - nb1) * blockDim.x + threadIdx.x) / 8);
+  const int r = q < n_dir_rows ? dir_rows[q] : -1;
+  T t = 0;
+  if (r >= 0)
+  {
+    const int b = dir_start[r], e = rp[r + 1];
+    int c[U];
+    T v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++)
+    {
+      const int j = b + lane + u * 8;
+      c[u] = j < e ? kc[j] : -1;
+      v[u] = j < e ? a[j] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (c[u] >= 0) t += v[u] * (T)in[c[u]];
+    for (int j = b + lane + U * 8; j < e; j += 8) t += a[j] * (T)in[kc[j]];
+  }
+  t = group_sum<8>(t);
+  if (r >= 0 && lane == 0) y[r] = omega * ((T)in[r] - t) / diag[r];
 }
 
 // exact coarse solve (SolveExact, MGLevel3D.C:839) with the explicit FP64 inverse of the
@@ -626,9 +651,9 @@ template <typename T> static int mg_record(cdgpu_ctx *ctx, Hierarchy &h, const c
   {
     // zero start and the first pre-smoothing sweep of the finest level in one kernel
     const Space &s = *F.sp;
-    const long groups = (long)ctx->sm_count * 8 * (256 / 8);
-    const int grid = (int)std::max<long>(1, std::min<long>((n + 31) / 32, groups / 32));
-    mg_start_first_kernel<T><<<grid, 256, 0, ctx->stream>>>(n, s.n_active, s.d_row_ptr, s.d_kcol, s.d_dir_start,
+    const int nb1 = (n + 255) / 256, nb2 = (int)(((long)s.n_dir_rows * 8 + 255) / 256);
+    mg_start_first_kernel<T><<<nb1 + nb2, 256, 0, ctx->stream>>>(n, s.n_active, nb1, s.n_dir_rows, s.d_dir_rows,
+                                                                s.d_row_ptr, s.d_kcol, s.d_dir_start,
                                                            mat<T>(s), dg<T>(s), h.d_io, v.rhs, v.alt,
                                                            (T)p.omega);
     CD_LAUNCHED(ctx);
@@ -850,7 +875,7 @@ static int refresh_coarse_inverse(cdgpu_ctx *ctx, Hierarchy &h)
   if (na > 4096)
     return fail(ctx, CDGPU_ERR_UNSUPPORTED, "exact coarse solve: more than 4096 active DOFs on the coarsest level");
   int rc;
-  if (h.cinv_version < 0 || !h.d_cinv)
+  if (!h.d_cinv)
   {
     if ((rc = dev_alloc(ctx, &h.d_cinv, (size_t)na * na)) || (rc = dev_alloc(ctx, &h.d_cpiv, na + 1)))
       return rc;
@@ -864,14 +889,16 @@ static int refresh_coarse_inverse(cdgpu_ctx *ctx, Hierarchy &h)
     int use_smem = sm <= 200 * 1024;
     if (use_smem)
       CD_CUDA(ctx, cudaFuncSetAttribute(gj_invert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    gj_invert_kernel<<<1, 1024, use_smem ? sm : 0, ctx->stream>>>(na, h.d_cinv, use_smem, h.d_cpiv,
-                                                                  h.d_cpiv + na);
+    // one warp per four rows (at most 32 warps): short barriers for small coarse levels
+    const int nt = std::min(1024, 32 * std::max(1, (na + 3) / 4));
+    gj_invert_kernel<<<1, nt, use_smem ? sm : 0, ctx->stream>>>(na, h.d_cinv, use_smem, h.d_cpiv, h.d_cpiv + na);
     CD_LAUNCHED(ctx);
   }
-  int flag = 0;
-  CD_CUDA(ctx, cudaMemcpyAsync(&flag, h.d_cpiv + na, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  if (flag) return fail(ctx, CDGPU_ERR_INVALID, "exact coarse solve: singular coarse matrix");
+  // the zero-pivot flag is copied back behind the inversion and checked after the solve,
+  // which synchronises anyway
+  if (!h.h_cflag) CD_CUDA(ctx, cudaMallocHost((void **)&h.h_cflag, sizeof(int)));
+  CD_CUDA(ctx, cudaMemcpyAsync(h.h_cflag, h.d_cpiv + na, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  h.cflag_pending = true;
   h.cinv_version = s.assembly_version;
   return CDGPU_OK;
 }
@@ -1187,5 +1214,16 @@ int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const 
   if (p.solver == 11) rc = fixed_point(ctx, h, p, d_rhs, d_sol, info);
   else if (p.solver == 16) rc = fgmres(ctx, h, p, d_rhs, d_sol, info);
   else return fail(ctx, CDGPU_ERR_UNSUPPORTED, "solve: SC_SOLVER_SCALAR must be 16 (FGMRES) or 11 (fixed point)");
+  if (h.cflag_pending)
+  {
+    h.cflag_pending = false;
+    CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (*h.h_cflag)
+    {
+      h.cinv_version = -2; // invert again on the next solve
+      return fail(ctx, CDGPU_ERR_INVALID, "exact coarse solve: singular coarse matrix");
+    }
+  }
+  if (rc == CDGPU_OK && p.precision == 1 && h.mf_mask) rc = assemble_check(ctx); // tensor-core wait flag
   return rc;
 }
