@@ -433,7 +433,7 @@ def run_ours(args, rank, world, local):
         "assembly": {"ms_all_levels": ms_asm, "mcells_per_s": n_cells_total / (ms_asm * 1e-3) / 1e6},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic,
-                     "kernel": "csr_kernel<double,8,16,SPMV> (finest level, the FGMRES matvec)",
+                     "kernel": "csr_kernel<double,8,16,SPMV,4> (finest level, the FGMRES matvec)",
                      "peak_source": peak_src, "spmv_ms": spmv_ms, "algorithmic_bytes": spmv_bytes},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 16 * n,
                 "d2h_bytes_per_step": 16 * n},

@@ -67,8 +67,8 @@ __device__ __forceinline__ void csr_epilogue(const CsrArgs<T> &p, int r, T s, do
   }
 }
 
-template <typename T, int GS, int U, int MODE>
-__global__ void __launch_bounds__(256) csr_kernel(CsrArgs<T> p)
+template <typename T, int GS, int U, int MODE, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) csr_kernel(CsrArgs<T> p)
 {
   constexpr int NT = 256;
   __shared__ double red[NT / 32];
@@ -120,8 +120,8 @@ __global__ void __launch_bounds__(256) csr_kernel(CsrArgs<T> p)
 // current chunk, so each row's dependent load chain overlaps the previous row's.  Used for
 // the FP32 multigrid levels with 8 threads per row, where it measured 31 us against 36 us
 // for the 32^3 Q2 product (FP64 gained nothing).
-template <typename T, int GS, int U, int MODE>
-__global__ void __launch_bounds__(256) csr_pipe_kernel(CsrArgs<T> p)
+template <typename T, int GS, int U, int MODE, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) csr_pipe_kernel(CsrArgs<T> p)
 {
   constexpr int NT = 256;
   __shared__ double red[NT / 32];
@@ -198,8 +198,12 @@ inline void launch_csr(cdgpu_ctx *ctx, const CsrShape &sh, const CsrArgs<T> &p, 
     case 2: csr_kernel<T, 2, 8, MODE><<<grid, 256, 0, ctx->stream>>>(p); break;
     case 4: csr_kernel<T, 4, 8, MODE><<<grid, 256, 0, ctx->stream>>>(p); break;
     case 8:
+      // FP64: at most 64 registers, so that 4 CTAs (32 warps) share an SM instead of 3; the
+      // 32^3 Q2 product went from 73 to 54 us with a cold L2
       if (sizeof(T) == 4 && (MODE == CM_JACOBI || MODE == CM_DEFECT))
         csr_pipe_kernel<T, 8, 8, MODE><<<grid, 256, 0, ctx->stream>>>(p);
+      else if (sizeof(T) == 8)
+        csr_kernel<T, 8, 16, MODE, 4><<<grid, 256, 0, ctx->stream>>>(p);
       else
         csr_kernel<T, 8, 16, MODE><<<grid, 256, 0, ctx->stream>>>(p);
       break;
