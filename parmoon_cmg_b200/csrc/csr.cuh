@@ -70,6 +70,7 @@ __device__ __forceinline__ void csr_epilogue(const CsrArgs<T> &p, int r, T s, do
 template <typename T, int GS, int U, int MODE, int MINB = 1>
 __global__ void __launch_bounds__(256, MINB) csr_kernel(CsrArgs<T> p)
 {
+  CD_PDL_ENTRY();
   constexpr int NT = 256;
   __shared__ double red[NT / 32];
   const int lane = threadIdx.x % GS, sub = (threadIdx.x % 32) / GS;
@@ -123,6 +124,7 @@ __global__ void __launch_bounds__(256, MINB) csr_kernel(CsrArgs<T> p)
 template <typename T, int GS, int U, int MODE, int MINB = 1>
 __global__ void __launch_bounds__(256, MINB) csr_pipe_kernel(CsrArgs<T> p)
 {
+  CD_PDL_ENTRY();
   constexpr int NT = 256;
   __shared__ double red[NT / 32];
   const int lane = threadIdx.x % GS, sub = (threadIdx.x % 32) / GS;
@@ -194,19 +196,19 @@ inline void launch_csr(cdgpu_ctx *ctx, const CsrShape &sh, const CsrArgs<T> &p, 
 {
   switch (sh.gs)
   {
-    case 1: csr_kernel<T, 1, 8, MODE><<<grid, 256, 0, ctx->stream>>>(p); break;
-    case 2: csr_kernel<T, 2, 8, MODE><<<grid, 256, 0, ctx->stream>>>(p); break;
-    case 4: csr_kernel<T, 4, 8, MODE><<<grid, 256, 0, ctx->stream>>>(p); break;
+    case 1: (void)cd_launch(csr_kernel<T, 1, 8, MODE>, grid, 256, 0, ctx->stream, p); break;
+    case 2: (void)cd_launch(csr_kernel<T, 2, 8, MODE>, grid, 256, 0, ctx->stream, p); break;
+    case 4: (void)cd_launch(csr_kernel<T, 4, 8, MODE>, grid, 256, 0, ctx->stream, p); break;
     case 8:
       // FP64: at most 64 registers, so that 4 CTAs (32 warps) share an SM instead of 3; the
       // 32^3 Q2 product went from 73 to 54 us with a cold L2
       if (sizeof(T) == 4 && (MODE == CM_JACOBI || MODE == CM_DEFECT))
-        csr_pipe_kernel<T, 8, 8, MODE><<<grid, 256, 0, ctx->stream>>>(p);
+        (void)cd_launch(csr_pipe_kernel<T, 8, 8, MODE>, grid, 256, 0, ctx->stream, p);
       else if (sizeof(T) == 8)
-        csr_kernel<T, 8, 16, MODE, 4><<<grid, 256, 0, ctx->stream>>>(p);
+        (void)cd_launch(csr_kernel<T, 8, 16, MODE, 4>, grid, 256, 0, ctx->stream, p);
       else
-        csr_kernel<T, 8, 16, MODE><<<grid, 256, 0, ctx->stream>>>(p);
+        (void)cd_launch(csr_kernel<T, 8, 16, MODE>, grid, 256, 0, ctx->stream, p);
       break;
-    default: csr_kernel<T, 32, 8, MODE><<<grid, 256, 0, ctx->stream>>>(p); break;
+    default: (void)cd_launch(csr_kernel<T, 32, 8, MODE>, grid, 256, 0, ctx->stream, p); break;
   }
 }

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/cdgpu.h"
@@ -183,6 +184,32 @@ int cuda_fail(cdgpu_ctx *ctx, cudaError_t e, const char *what);
     cudaError_t e_ = cudaGetLastError();                                  \
     if (e_ != cudaSuccess) return cuda_fail(ctx, e_, "kernel launch");   \
   } while (0)
+
+// Programmatic dependent launch (sm_90+): a kernel started with cd_launch may be scheduled
+// while the previous kernel of the stream (or captured graph) still runs.  Every kernel
+// launched that way begins with CD_PDL_ENTRY: it first lets its own successor be scheduled
+// (griddepcontrol.launch_dependents) and then waits until its predecessor has completed and
+// its memory is visible (griddepcontrol.wait), before its first global memory access.  Only
+// the launch and the CTA scheduling overlap, never the work.  Without the launch attribute
+// both instructions return at once.
+#define CD_PDL_ENTRY() asm volatile("griddepcontrol.launch_dependents;\n\tgriddepcontrol.wait;" ::: "memory")
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t cd_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                             Args &&...args)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 template <typename T> int dev_alloc(cdgpu_ctx *ctx, T **p, size_t n)
 {

@@ -24,6 +24,7 @@ __global__ void __launch_bounds__(128) mf_cell_kernel(int n_cells, const int *__
                                                       const float *__restrict__ R32, const float *__restrict__ x,
                                                       float *__restrict__ ybuf)
 {
+  CD_PDL_ENTRY();
   __shared__ float Rs[T * NBF * NBF];
   for (int i = threadIdx.x; i < T * NBF * NBF; i += blockDim.x) Rs[i] = R32[i];
   __syncthreads();
@@ -60,6 +61,7 @@ __global__ void __launch_bounds__(224) mf_cell27_kernel(int n_cells, const int *
                                                         const float *__restrict__ R32, const float *__restrict__ x,
                                                         float *__restrict__ ybuf)
 {
+  CD_PDL_ENTRY();
   constexpr int CB = 64, NB = 27;
   __shared__ float Rs[T * NB * NB];
   __shared__ float Xs[CB * NB];
@@ -151,6 +153,7 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
                                                               const float *__restrict__ x, float *__restrict__ ybuf,
                                                               int *__restrict__ err)
 {
+  CD_PDL_ENTRY();
   constexpr int MT = 128, KP = 32, NB = 27, N = 32 * T, NH = N / 2;
   extern __shared__ __align__(1024) unsigned char mf_sm[];
   unsigned char *As = mf_sm;                    // 128 x 32 x 4 = 16 KB
@@ -291,6 +294,7 @@ __global__ void mf_row_kernel(int n, int na, int n_cells, const int *__restrict_
                               const float *__restrict__ x, const float *__restrict__ f,
                               const float *__restrict__ diag, float *__restrict__ out, float omega)
 {
+  CD_PDL_ENTRY();
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
   if (r >= na)
@@ -365,28 +369,28 @@ inline void mf_apply_cells(cdgpu_ctx *ctx, const Space &s, const float *x)
     const int grid = std::max(1, std::min((s.n_cells + 127) / 128, ctx->sm_count));
     if (s.mf_T == 10)
     {
-      mf_cell27_tc_kernel<10><<<grid, 128, 120 * 1024, ctx->stream>>>(s.n_cells, s.d_gn, s.d_cf32, s.d_R32, x,
-                                                                      s.d_ybuf, ctx->d_err);
+      (void)cd_launch(mf_cell27_tc_kernel<10>, grid, 128, 120 * 1024, ctx->stream, s.n_cells, s.d_gn, s.d_cf32,
+                      s.d_R32, x, s.d_ybuf, ctx->d_err);
       return;
     }
     if (s.mf_T == 13)
     {
-      mf_cell27_tc_kernel<13><<<grid, 128, 120 * 1024, ctx->stream>>>(s.n_cells, s.d_gn, s.d_cf32, s.d_R32, x,
-                                                                      s.d_ybuf, ctx->d_err);
+      (void)cd_launch(mf_cell27_tc_kernel<13>, grid, 128, 120 * 1024, ctx->stream, s.n_cells, s.d_gn, s.d_cf32,
+                      s.d_R32, x, s.d_ybuf, ctx->d_err);
       return;
     }
   }
   if (s.nbf == 27)
   {
     const int g27 = (s.n_cells + 63) / 64;
-    if (s.mf_T == 10) { mf_cell27_kernel<10><<<g27, 224, 0, ctx->stream>>>(s.n_cells, s.d_gn, s.d_cf32, s.d_R32, x, s.d_ybuf); return; }
-    if (s.mf_T == 13) { mf_cell27_kernel<13><<<g27, 224, 0, ctx->stream>>>(s.n_cells, s.d_gn, s.d_cf32, s.d_R32, x, s.d_ybuf); return; }
+    if (s.mf_T == 10) { (void)cd_launch(mf_cell27_kernel<10>, g27, 224, 0, ctx->stream, s.n_cells, s.d_gn, s.d_cf32, s.d_R32, x, s.d_ybuf); return; }
+    if (s.mf_T == 13) { (void)cd_launch(mf_cell27_kernel<13>, g27, 224, 0, ctx->stream, s.n_cells, s.d_gn, s.d_cf32, s.d_R32, x, s.d_ybuf); return; }
   }
   const int grid = (s.n_cells + 127) / 128;
 #define CD_MF_CASE(NB, TT)                                                                              \
   if (s.nbf == NB && s.mf_T == TT)                                                                      \
   {                                                                                                     \
-    mf_cell_kernel<NB, TT><<<grid, 128, 0, ctx->stream>>>(s.n_cells, s.d_gn, s.d_cf32, s.d_R32, x, s.d_ybuf); \
+    (void)cd_launch(mf_cell_kernel<NB, TT>, grid, 128, 0, ctx->stream, s.n_cells, s.d_gn, s.d_cf32, s.d_R32, x, s.d_ybuf); \
     return;                                                                                             \
   }
   CD_MF_CASE(27, 10) CD_MF_CASE(27, 13) CD_MF_CASE(8, 10) CD_MF_CASE(8, 13)
@@ -401,9 +405,9 @@ inline void mf_rows(cdgpu_ctx *ctx, const Space &s, const float *x, const float 
   const int grid = (s.n_dof + 255) / 256;
   switch (s.nbf)
   {
-    case 27: mf_row_kernel<27, MODE><<<grid, 256, 0, ctx->stream>>>(s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega); break;
-    case 9: mf_row_kernel<9, MODE><<<grid, 256, 0, ctx->stream>>>(s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega); break;
-    case 8: mf_row_kernel<8, MODE><<<grid, 256, 0, ctx->stream>>>(s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega); break;
-    default: mf_row_kernel<4, MODE><<<grid, 256, 0, ctx->stream>>>(s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega); break;
+    case 27: (void)cd_launch(mf_row_kernel<27, MODE>, grid, 256, 0, ctx->stream, s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega); break;
+    case 9: (void)cd_launch(mf_row_kernel<9, MODE>, grid, 256, 0, ctx->stream, s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega); break;
+    case 8: (void)cd_launch(mf_row_kernel<8, MODE>, grid, 256, 0, ctx->stream, s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega); break;
+    default: (void)cd_launch(mf_row_kernel<4, MODE>, grid, 256, 0, ctx->stream, s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega); break;
   }
 }

@@ -55,6 +55,7 @@ __global__ void jacobi_first_kernel(int n, int n_active, const int *__restrict__
                                     const T *__restrict__ x, const T *__restrict__ f,
                                     T *__restrict__ xo, T omega, int x_all_zero)
 {
+  CD_PDL_ENTRY();
   int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
   if (r >= n_active) { xo[r] = f[r]; return; }
@@ -83,6 +84,7 @@ __global__ void __launch_bounds__(256) mg_start_first_kernel(int n, int n_active
                                                              double *const *__restrict__ io, T *__restrict__ rhs,
                                                              T *__restrict__ y, T omega)
 {
+  CD_PDL_ENTRY();
   const double *in = io[0];
   if ((int)blockIdx.x < nb1)
   {
@@ -132,6 +134,7 @@ __global__ void coarse_exact_kernel(int n, int na, const int *__restrict__ rp, c
                                     const double *__restrict__ cinv, const T *__restrict__ rhs,
                                     T *__restrict__ sol)
 {
+  CD_PDL_ENTRY();
   extern __shared__ double b[];
   for (int i = threadIdx.x; i < n; i += blockDim.x) b[i] = (double)rhs[i];
   __syncthreads();
@@ -165,6 +168,7 @@ __global__ void coarse_smooth_kernel(int n, int n_active, const int *__restrict_
                                      const T *__restrict__ f, T *__restrict__ sol, double omega,
                                      int mode, int maxit, double red_factor)
 {
+  CD_PDL_ENTRY();
   extern __shared__ double sh[];
   double *x = sh, *aux = sh + n;
   __shared__ double red[32];
@@ -265,6 +269,7 @@ __global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, const double *__
                                                          const double *__restrict__ coef,
                                                          double *__restrict__ partial)
 {
+  CD_PDL_ENTRY();
   constexpr int NS = MODE == GS_AXPY_NORM ? 1 : K;
   __shared__ double red[kBlock / 32][NS];
   double acc[NS];
@@ -316,7 +321,7 @@ static void launch_gs(int k, int grid, cudaStream_t st, int n, const double *Y, 
 {
   switch (k)
   {
-#define CD_GS_CASE(K) case K: gs_pass_kernel<K, MODE><<<grid, kBlock, 0, st>>>(n, Y, w, coef, partial); break;
+#define CD_GS_CASE(K) case K: (void)cd_launch(gs_pass_kernel<K, MODE>, grid, kBlock, 0, st, n, Y, w, coef, partial); break;
     CD_GS_CASE(1) CD_GS_CASE(2) CD_GS_CASE(3) CD_GS_CASE(4) CD_GS_CASE(5) CD_GS_CASE(6) CD_GS_CASE(7)
     CD_GS_CASE(8) CD_GS_CASE(9) CD_GS_CASE(10) CD_GS_CASE(11) CD_GS_CASE(12) CD_GS_CASE(13) CD_GS_CASE(14)
     CD_GS_CASE(15) CD_GS_CASE(16) CD_GS_CASE(17) CD_GS_CASE(18) CD_GS_CASE(19) CD_GS_CASE(20) CD_GS_CASE(21)
@@ -331,6 +336,7 @@ static void launch_gs(int k, int grid, cudaStream_t st, int n, const double *Y, 
 __global__ void reduce_partials_kernel(int nblocks, int nslots, const double *__restrict__ partial,
                                        double *__restrict__ out)
 {
+  CD_PDL_ENTRY();
   __shared__ double red[32];
   const int j = blockIdx.x;
   double t = 0;
@@ -365,6 +371,7 @@ __global__ void sum_blocks_kernel(int nblocks, const double *__restrict__ partia
 
 __global__ void scale_kernel(int n, double alpha, const double *__restrict__ x, double *__restrict__ y)
 {
+  CD_PDL_ENTRY();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) y[i] = alpha * x[i];
 }
@@ -400,6 +407,7 @@ template <typename T>
 __global__ void mg_start_kernel(int n, int n_active, double *const *__restrict__ io, T *__restrict__ rhs,
                                 T *__restrict__ sol)
 {
+  CD_PDL_ENTRY();
   const double *rhs_in = io[0];
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -411,6 +419,7 @@ __global__ void mg_start_kernel(int n, int n_active, double *const *__restrict__
 template <typename T>
 __global__ void mg_finish_kernel(int n, const T *__restrict__ sol, double *const *__restrict__ io)
 {
+  CD_PDL_ENTRY();
   double *out = io[1];
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = (double)sol[i];
@@ -531,7 +540,7 @@ template <typename T> static int jacobi_first(cdgpu_ctx *ctx, Level &L, T omega,
 {
   LevelVec<T> &v = vecs<T>(L);
   const Space &s = *L.sp;
-  jacobi_first_kernel<T><<<(s.n_dof + 255) / 256, 256, 0, ctx->stream>>>(
+  (void)cd_launch(jacobi_first_kernel<T>, (s.n_dof + 255) / 256, 256, 0, ctx->stream, 
       s.n_dof, s.n_active, s.d_row_ptr, s.d_kcol, s.d_dir_start, mat<T>(s), dg<T>(s), v.sol, v.rhs,
       v.alt, omega, all_zero);
   CD_LAUNCHED(ctx);
@@ -576,14 +585,14 @@ template <typename T> static int coarse_solve(cdgpu_ctx *ctx, Hierarchy &h, Cycl
   if (cs.p->coarse_smoother == 17)
   {
     size_t sm = sizeof(double) * (s.n_dof + s.n_active);
-    coarse_exact_kernel<T><<<1, 1024, sm, ctx->stream>>>(s.n_dof, s.n_active, s.d_row_ptr, s.d_kcol,
+    (void)cd_launch(coarse_exact_kernel<T>, 1, 1024, sm, ctx->stream, s.n_dof, s.n_active, s.d_row_ptr, s.d_kcol,
                                                          s.d_dir_start, s.d_a, h.d_cinv, v.rhs, v.sol);
     CD_LAUNCHED(ctx);
   }
   else
   {
     size_t sm = sizeof(double) * 2 * s.n_dof;
-    coarse_smooth_kernel<T><<<1, 256, sm, ctx->stream>>>(s.n_dof, s.n_active, s.d_row_ptr, s.d_kcol,
+    (void)cd_launch(coarse_smooth_kernel<T>, 1, 256, sm, ctx->stream, s.n_dof, s.n_active, s.d_row_ptr, s.d_kcol,
                                                          mat<T>(s), v.rhs, v.sol, cs.p->omega,
                                                          cs.p->coarse_smoother, cs.p->coarse_maxit,
                                                          cs.p->coarse_red);
@@ -652,7 +661,7 @@ template <typename T> static int mg_record(cdgpu_ctx *ctx, Hierarchy &h, const c
     // zero start and the first pre-smoothing sweep of the finest level in one kernel
     const Space &s = *F.sp;
     const int nb1 = (n + 255) / 256, nb2 = (int)(((long)s.n_dir_rows * 8 + 255) / 256);
-    mg_start_first_kernel<T><<<nb1 + nb2, 256, 0, ctx->stream>>>(n, s.n_active, nb1, s.n_dir_rows, s.d_dir_rows,
+    (void)cd_launch(mg_start_first_kernel<T>, nb1 + nb2, 256, 0, ctx->stream, n, s.n_active, nb1, s.n_dir_rows, s.d_dir_rows,
                                                                 s.d_row_ptr, s.d_kcol, s.d_dir_start,
                                                            mat<T>(s), dg<T>(s), h.d_io, v.rhs, v.alt,
                                                            (T)p.omega);
@@ -662,13 +671,13 @@ template <typename T> static int mg_record(cdgpu_ctx *ctx, Hierarchy &h, const c
   }
   else
   {
-    mg_start_kernel<T><<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, F.sp->n_active, h.d_io, v.rhs, v.sol);
+    (void)cd_launch(mg_start_kernel<T>, (n + 255) / 256, 256, 0, ctx->stream, n, F.sp->n_active, h.d_io, v.rhs, v.sol);
     CD_LAUNCHED(ctx);
     cs.active_zero[L - 1] = true;
   }
   int rc = cycle<T>(ctx, h, cs, L - 1);
   if (rc) return rc;
-  mg_finish_kernel<T><<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, v.sol, h.d_io);
+  (void)cd_launch(mg_finish_kernel<T>, (n + 255) / 256, 256, 0, ctx->stream, n, v.sol, h.d_io);
   CD_LAUNCHED(ctx);
   return CDGPU_OK;
 }
@@ -1016,7 +1025,7 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
   bool done = false;
   while (j <= maxite && !done)
   {
-    scale_kernel<<<blocks, 256, 0, ctx->stream>>>(n, 1.0 / beta, V(0), V(0));
+    (void)cd_launch(scale_kernel, blocks, 256, 0, ctx->stream, n, 1.0 / beta, V(0), V(0));
     CD_LAUNCHED(ctx);
     std::fill(sv.begin(), sv.end(), 0.0);
     sv[0] = beta;
@@ -1029,17 +1038,17 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
       // pass 1: h1 = V^T w
       launch_gs<GS_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, nullptr, h.d_partial);
       CD_LAUNCHED(ctx);
-      reduce_partials_kernel<<<k, 256, 0, ctx->stream>>>(pb, k, h.d_partial, h.d_ctl);
+      (void)cd_launch(reduce_partials_kernel, k, 256, 0, ctx->stream, pb, k, h.d_partial, h.d_ctl);
       CD_LAUNCHED(ctx);
       // pass 2: w -= V h1, h2 = V^T w
       launch_gs<GS_AXPY_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, h.d_ctl, h.d_partial);
       CD_LAUNCHED(ctx);
-      reduce_partials_kernel<<<k, 256, 0, ctx->stream>>>(pb, k, h.d_partial, h.d_ctl + 33);
+      (void)cd_launch(reduce_partials_kernel, k, 256, 0, ctx->stream, pb, k, h.d_partial, h.d_ctl + 33);
       CD_LAUNCHED(ctx);
       // w -= V h2, ||w||^2
       launch_gs<GS_AXPY_NORM>(k, pb, ctx->stream, n, h.d_V, h.d_w, h.d_ctl + 33, h.d_partial);
       CD_LAUNCHED(ctx);
-      reduce_partials_kernel<<<1, 256, 0, ctx->stream>>>(pb, 1, h.d_partial, h.d_ctl + 66);
+      (void)cd_launch(reduce_partials_kernel, 1, 256, 0, ctx->stream, pb, 1, h.d_partial, h.d_ctl + 66);
       CD_LAUNCHED(ctx);
       if ((rc = read_ctl(ctx, h, 67))) return rc;
       // the slot-0 reduction of the last pass holds ||w||^2 (slot 32 of the partials)
@@ -1048,7 +1057,7 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
       H[(size_t)(i + 1) * m + i] = hn;
       if (hn != 0)
       {
-        scale_kernel<<<blocks, 256, 0, ctx->stream>>>(n, 1.0 / hn, h.d_w, V(i + 1));
+        (void)cd_launch(scale_kernel, blocks, 256, 0, ctx->stream, n, 1.0 / hn, h.d_w, V(i + 1));
         CD_LAUNCHED(ctx);
       }
       for (int t = 0; t < i; t++) app_rot(H[(size_t)t * m + i], H[(size_t)(t + 1) * m + i], cs[t], sn[t]);
