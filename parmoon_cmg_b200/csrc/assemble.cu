@@ -129,6 +129,7 @@ struct CellCoefArgs
 
 __global__ void cell_coef_kernel(CellCoefArgs a)
 {
+  CD_PDL_ENTRY();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.n_cells) return;
   const int dim = a.dim;
@@ -362,6 +363,7 @@ __global__ void __launch_bounds__(256) affine_local_kernel(int n_cells, int nbf,
                                                            const double *__restrict__ r, double *__restrict__ out,
                                                            int cells_per_block)
 {
+  CD_PDL_ENTRY();
   const int per = nbf * nbf + nbf;
   const int q = blockIdx.y * blockDim.x + threadIdx.x;
   const bool act = q < per;
@@ -414,6 +416,7 @@ struct GatherArgs
 template <int GS, int MAXROW>
 __global__ void __launch_bounds__(256) row_gather_kernel(GatherArgs p)
 {
+  CD_PDL_ENTRY();
   extern __shared__ double smem[];
   const int nbf = p.nbf;
   double *accs = smem; // groups x MAXROW
@@ -580,7 +583,7 @@ static int launch_gather(cdgpu_ctx *ctx, const GatherArgs &g, int n_dof)
   long need = (n_dof + groups - 1) / groups;
   long grid = std::min<long>(need, (long)ctx->sm_count * blocks_per_sm);
   if (grid < 1) grid = 1;
-  row_gather_kernel<GS, MAXROW><<<(int)grid, 256, sm, ctx->stream>>>(g);
+  (void)cd_launch(row_gather_kernel<GS, MAXROW>, (int)grid, 256, sm, ctx->stream, g);
   CD_LAUNCHED(ctx);
   return CDGPU_OK;
 }
@@ -658,7 +661,7 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, 
     if (!s.d_cellcoef && (rc = dev_alloc(ctx, &s.d_cellcoef, (size_t)s.n_cells * (CD_MAXT + 4))))
       return rc;
     CellCoefArgs a{s.dim, s.nv, s.n_cells, disctype, T, Tr, co, s.d_coords, s.d_cellcoef};
-    cell_coef_kernel<<<(s.n_cells + 127) / 128, 128, 0, ctx->stream>>>(a);
+    (void)cd_launch(cell_coef_kernel, (s.n_cells + 127) / 128, 128, 0, ctx->stream, a);
     CD_LAUNCHED(ctx);
     // local matrices of every cell, then the gather with prefetched loads
     if (!s.d_local && (rc = dev_alloc(ctx, &s.d_local, (size_t)s.n_cells * (s.nbf * s.nbf + s.nbf))))
@@ -667,7 +670,7 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, 
     const int qblocks = (per + 255) / 256;
     const int cpb = std::max(1, (int)((long)s.n_cells * qblocks / ((long)ctx->sm_count * 8)));
     dim3 grid((s.n_cells + cpb - 1) / cpb, qblocks);
-    affine_local_kernel<<<grid, 256, 0, ctx->stream>>>(s.n_cells, s.nbf, T, Tr, s.d_cellcoef, s.d_ref,
+    (void)cd_launch(affine_local_kernel, grid, 256, 0, ctx->stream, s.n_cells, s.nbf, T, Tr, s.d_cellcoef, s.d_ref,
                                                        s.d_ref + (size_t)s.nbf * s.nbf * T, s.d_local, cpb);
     CD_LAUNCHED(ctx);
   }

@@ -195,6 +195,7 @@ __device__ __forceinline__ bool stepping(const BCtl &c) { return c.state == ST_R
 // zero start + Dirichlet nodes on depth 0 from the current basis vector V_j
 __global__ void b_mg_start(BTab t, const BCtl *__restrict__ ctl, const BLevel *__restrict__ lev)
 {
+  CD_PDL_ENTRY();
   for (int vb = blockIdx.x; vb < t.total; vb += gridDim.x)
   {
     const int k = find_item(t, vb), slot = t.item[k];
@@ -214,6 +215,7 @@ __global__ void b_mg_start(BTab t, const BCtl *__restrict__ ctl, const BLevel *_
 __global__ void b_jacobi(BTab t, const BCtl *__restrict__ ctl, const BLevel *__restrict__ lev, int depth, int src,
                          int first, float omega)
 {
+  CD_PDL_ENTRY();
   const int lane = threadIdx.x % 4;
   for (int vb = blockIdx.x; vb < t.total; vb += gridDim.x)
   {
@@ -247,6 +249,7 @@ __global__ void b_jacobi(BTab t, const BCtl *__restrict__ ctl, const BLevel *__r
 __global__ void b_color(BTab t, const BCtl *__restrict__ ctl, const BLevel *__restrict__ lev, int depth,
                         const int *__restrict__ cstart, float omega)
 {
+  CD_PDL_ENTRY();
   const int lane = threadIdx.x % 4;
   for (int vb = blockIdx.x; vb < t.total; vb += gridDim.x)
   {
@@ -266,6 +269,7 @@ __global__ void b_color(BTab t, const BCtl *__restrict__ ctl, const BLevel *__re
 // def = f - A v[src]
 __global__ void b_defect(BTab t, const BCtl *__restrict__ ctl, const BLevel *__restrict__ lev, int depth, int src)
 {
+  CD_PDL_ENTRY();
   const int lane = threadIdx.x % 4;
   for (int vb = blockIdx.x; vb < t.total; vb += gridDim.x)
   {
@@ -282,6 +286,7 @@ __global__ void b_defect(BTab t, const BCtl *__restrict__ ctl, const BLevel *__r
 // coarse rhs = R def on active coarse rows (zero elsewhere), coarse v[0] = 0
 __global__ void b_restrict(BTab t, const BCtl *__restrict__ ctl, const BLevel *__restrict__ lev, int depth)
 {
+  CD_PDL_ENTRY();
   const int lane = threadIdx.x % 4;
   for (int vb = blockIdx.x; vb < t.total; vb += gridDim.x)
   {
@@ -303,6 +308,7 @@ __global__ void b_restrict(BTab t, const BCtl *__restrict__ ctl, const BLevel *_
 __global__ void b_prolong(BTab t, const BCtl *__restrict__ ctl, const BLevel *__restrict__ lev, int depth, int fsrc,
                           int csrc, float damp)
 {
+  CD_PDL_ENTRY();
   const int lane = threadIdx.x % 4;
   for (int vb = blockIdx.x; vb < t.total; vb += gridDim.x)
   {
@@ -320,6 +326,7 @@ __global__ void b_prolong(BTab t, const BCtl *__restrict__ ctl, const BLevel *__
 // Dirichlet rows v = rhs and the active right-hand side corrected by A_AD rhs_D
 __global__ void b_coarse(BTab t, const BCtl *__restrict__ ctl, const BLevel *__restrict__ lev, int depth, int out)
 {
+  CD_PDL_ENTRY();
   extern __shared__ double sb[];
   for (int k = blockIdx.x; k < t.K; k += gridDim.x)
   {
@@ -353,6 +360,7 @@ __global__ void b_coarse(BTab t, const BCtl *__restrict__ ctl, const BLevel *__r
 // Z_j = v[src] of depth 0, in FP64
 __global__ void b_mg_finish(BTab t, const BCtl *__restrict__ ctl, const BLevel *__restrict__ lev, int src)
 {
+  CD_PDL_ENTRY();
   for (int vb = blockIdx.x; vb < t.total; vb += gridDim.x)
   {
     const int k = find_item(t, vb), slot = t.item[k];
@@ -371,6 +379,7 @@ __global__ void b_mg_finish(BTab t, const BCtl *__restrict__ ctl, const BLevel *
 // partial sums of its square
 __global__ void b_matvec(BTab t, const BCtl *__restrict__ ctl, int restart_phase, double *__restrict__ partial)
 {
+  CD_PDL_ENTRY();
   __shared__ double red[kNT / 32];
   const int lane = threadIdx.x % 4;
   for (int vb = blockIdx.x; vb < t.total; vb += gridDim.x)
@@ -415,6 +424,7 @@ __global__ void b_matvec(BTab t, const BCtl *__restrict__ ctl, int restart_phase
 // 2 axpy (dots2) + norm; per-virtual-block partials in partial[vb * 33 + t]
 __global__ void b_gs(BTab t, const BCtl *__restrict__ ctl, int mode, double *__restrict__ partial)
 {
+  CD_PDL_ENTRY();
   __shared__ double red[kNT / 32][kSlots];
   const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
   for (int vb = blockIdx.x; vb < t.total; vb += gridDim.x)
@@ -471,6 +481,7 @@ __global__ void b_gs(BTab t, const BCtl *__restrict__ ctl, int mode, double *__r
 __global__ void b_reduce(BTab t, BCtl *__restrict__ ctl, int which, int restart_phase,
                          const double *__restrict__ partial)
 {
+  CD_PDL_ENTRY();
   __shared__ double red[kNT / 32];
   for (int k = blockIdx.x; k < t.K; k += gridDim.x)
   {
@@ -528,6 +539,7 @@ __device__ void d_solve_y(BCtl &c, int k)
 // Hessenberg column j, rotations, residual, stopping tests (FgmresIte.C:410-530)
 __global__ void b_givens(BTab t, BCtl *__restrict__ ctl, int maxit, int minit, double div_factor)
 {
+  CD_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < t.K; k += gridDim.x * blockDim.x)
   {
     BCtl &c = ctl[t.item[k]];
@@ -577,6 +589,7 @@ __global__ void b_givens(BTab t, BCtl *__restrict__ ctl, int maxit, int minit, d
 // V_{j+1} = w / h_{j+1,j} (A_NEXT), or x += Z y (A_UPD_*)
 __global__ void b_next_update(BTab t, const BCtl *__restrict__ ctl)
 {
+  CD_PDL_ENTRY();
   for (int vb = blockIdx.x; vb < t.total; vb += gridDim.x)
   {
     const int k = find_item(t, vb), slot = t.item[k];
@@ -598,6 +611,7 @@ __global__ void b_next_update(BTab t, const BCtl *__restrict__ ctl)
 // end of an iteration: advance j, finish, or schedule the restart
 __global__ void b_post(BTab t, BCtl *__restrict__ ctl, int *__restrict__ state_out)
 {
+  CD_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < t.K; k += gridDim.x * blockDim.x)
   {
     const int slot = t.item[k];
@@ -615,6 +629,7 @@ __global__ void b_post(BTab t, BCtl *__restrict__ ctl, int *__restrict__ state_o
 // restart: beta = ||b - A x||, stopping test on it, s = (beta, 0, ...), j = 0
 __global__ void b_restart(BTab t, BCtl *__restrict__ ctl, int stop_rule, double red_factor, double res_norm_min)
 {
+  CD_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < t.K; k += gridDim.x * blockDim.x)
   {
     BCtl &c = ctl[t.item[k]];
@@ -639,6 +654,7 @@ __global__ void b_restart(BTab t, BCtl *__restrict__ ctl, int stop_rule, double 
 
 __global__ void b_scale0(BTab t, BCtl *__restrict__ ctl)
 {
+  CD_PDL_ENTRY();
   for (int vb = blockIdx.x; vb < t.total; vb += gridDim.x)
   {
     const int k = find_item(t, vb), slot = t.item[k];
@@ -651,6 +667,7 @@ __global__ void b_scale0(BTab t, BCtl *__restrict__ ctl)
 
 __global__ void b_begin_step(BTab t, BCtl *__restrict__ ctl)
 {
+  CD_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < t.K; k += gridDim.x * blockDim.x)
   {
     BCtl &c = ctl[t.item[k]];
@@ -781,6 +798,7 @@ __global__ void b_tcd_combine(int n, int na, const int *__restrict__ rp, const i
 // K u_old on active rows (f_old = f: coefficients constant in time), b = f on Dirichlet rows
 __global__ void b_tcd_rhs(BTab t, const BCtl *__restrict__ ctl)
 {
+  CD_PDL_ENTRY();
   const int lane = threadIdx.x % 4;
   for (int vb = blockIdx.x; vb < t.total; vb += gridDim.x)
   {
@@ -806,6 +824,7 @@ __global__ void b_tcd_rhs(BTab t, const BCtl *__restrict__ ctl)
 
 __global__ void b_tcd_begin(BTab t, BCtl *__restrict__ ctl)
 {
+  CD_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < t.K; k += gridDim.x * blockDim.x)
   {
     BCtl &c = ctl[t.item[k]];
@@ -1072,7 +1091,7 @@ static int batch_cycle(cdgpu_ctx *ctx, Batch &b)
   const int after_pre = jac ? pre % 2 : 0, after_post = jac ? (pre + post) % 2 : 0;
   const float omega = (float)p.omega, damp = (float)p.gmg_damp;
   cudaStream_t st = ctx->stream;
-  b_mg_start<<<grid_of(ctx, b.fine_vec.total), kNT, 0, st>>>(b.fine_vec, b.d_ctl, b.d_lev);
+  (void)cd_launch(b_mg_start, grid_of(ctx, b.fine_vec.total), kNT, 0, st, b.fine_vec, b.d_ctl, b.d_lev);
   CD_LAUNCHED(ctx);
   auto sweeps = [&](int d, int count, bool first_zero) -> int {
     const BTab &t = b.smooth[d];
@@ -1081,7 +1100,7 @@ static int batch_cycle(cdgpu_ctx *ctx, Batch &b)
       int src = first_zero ? 0 : after_pre;
       for (int s = 0; s < count; s++)
       {
-        b_jacobi<<<grid_of(ctx, t.total), kNT, 0, st>>>(t, b.d_ctl, b.d_lev, d, src, first_zero && s == 0 ? 1 : 0,
+        (void)cd_launch(b_jacobi, grid_of(ctx, t.total), kNT, 0, st, t, b.d_ctl, b.d_lev, d, src, first_zero && s == 0 ? 1 : 0,
                                                         omega);
         CD_LAUNCHED(ctx);
         src = 1 - src;
@@ -1097,7 +1116,7 @@ static int batch_cycle(cdgpu_ctx *ctx, Batch &b)
             const int c = pass == 0 ? q : nc - 1 - q;
             const BTab &ct = b.color[d][c];
             if (ct.K == 0) continue;
-            b_color<<<grid_of(ctx, ct.total), kNT, 0, st>>>(ct, b.d_ctl, b.d_lev, d, colour_start(ct), omega);
+            (void)cd_launch(b_color, grid_of(ctx, ct.total), kNT, 0, st, ct, b.d_ctl, b.d_lev, d, colour_start(ct), omega);
             CD_LAUNCHED(ctx);
           }
       }
@@ -1119,21 +1138,21 @@ static int batch_cycle(cdgpu_ctx *ctx, Batch &b)
       size_t sm = sizeof(double) * nmax;
       if (sm > 48 * 1024)
         CD_CUDA(ctx, cudaFuncSetAttribute(b_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      b_coarse<<<grid_of(ctx, b.coarse[d].K), 512, sm, st>>>(b.coarse[d], b.d_ctl, b.d_lev, d, after_post);
+      (void)cd_launch(b_coarse, grid_of(ctx, b.coarse[d].K), 512, sm, st, b.coarse[d], b.d_ctl, b.d_lev, d, after_post);
       CD_LAUNCHED(ctx);
     }
     if (b.smooth[d].K == 0) continue;
     int rc = sweeps(d, pre, true);
     if (rc) return rc;
-    b_defect<<<grid_of(ctx, b.smooth[d].total), kNT, 0, st>>>(b.smooth[d], b.d_ctl, b.d_lev, d, after_pre);
+    (void)cd_launch(b_defect, grid_of(ctx, b.smooth[d].total), kNT, 0, st, b.smooth[d], b.d_ctl, b.d_lev, d, after_pre);
     CD_LAUNCHED(ctx);
-    b_restrict<<<grid_of(ctx, b.restrict_[d].total), kNT, 0, st>>>(b.restrict_[d], b.d_ctl, b.d_lev, d);
+    (void)cd_launch(b_restrict, grid_of(ctx, b.restrict_[d].total), kNT, 0, st, b.restrict_[d], b.d_ctl, b.d_lev, d);
     CD_LAUNCHED(ctx);
   }
   for (int d = D - 2; d >= 0; d--)
   {
     if (b.smooth[d].K == 0) continue;
-    b_prolong<<<grid_of(ctx, b.smooth[d].total), kNT, 0, st>>>(b.smooth[d], b.d_ctl, b.d_lev, d, after_pre,
+    (void)cd_launch(b_prolong, grid_of(ctx, b.smooth[d].total), kNT, 0, st, b.smooth[d], b.d_ctl, b.d_lev, d, after_pre,
                                                                after_post, damp);
     CD_LAUNCHED(ctx);
     if (jac)
@@ -1141,7 +1160,7 @@ static int batch_cycle(cdgpu_ctx *ctx, Batch &b)
       int src = after_pre;
       for (int s = 0; s < post; s++)
       {
-        b_jacobi<<<grid_of(ctx, b.smooth[d].total), kNT, 0, st>>>(b.smooth[d], b.d_ctl, b.d_lev, d, src, 0, omega);
+        (void)cd_launch(b_jacobi, grid_of(ctx, b.smooth[d].total), kNT, 0, st, b.smooth[d], b.d_ctl, b.d_lev, d, src, 0, omega);
         CD_LAUNCHED(ctx);
         src = 1 - src;
       }
@@ -1152,7 +1171,7 @@ static int batch_cycle(cdgpu_ctx *ctx, Batch &b)
       if (rc) return rc;
     }
   }
-  b_mg_finish<<<grid_of(ctx, b.fine_vec.total), kNT, 0, st>>>(b.fine_vec, b.d_ctl, b.d_lev, after_post);
+  (void)cd_launch(b_mg_finish, grid_of(ctx, b.fine_vec.total), kNT, 0, st, b.fine_vec, b.d_ctl, b.d_lev, after_post);
   CD_LAUNCHED(ctx);
   return CDGPU_OK;
 }
@@ -1163,33 +1182,33 @@ static int batch_iteration(cdgpu_ctx *ctx, Batch &b)
   cudaStream_t st = ctx->stream;
   const int gi = std::max(1, std::min((b.items.K + 127) / 128, ctx->sm_count * 4));
   // restarts (and first starts): V_0 = b - A x, beta, V_0 /= beta
-  b_matvec<<<grid_of(ctx, b.fine_csr.total), kNT, 0, st>>>(b.fine_csr, b.d_ctl, 1, b.d_partial);
+  (void)cd_launch(b_matvec, grid_of(ctx, b.fine_csr.total), kNT, 0, st, b.fine_csr, b.d_ctl, 1, b.d_partial);
   CD_LAUNCHED(ctx);
-  b_reduce<<<grid_of(ctx, b.fine_csr.K), kNT, 0, st>>>(b.fine_csr, b.d_ctl, 2, 1, b.d_partial);
+  (void)cd_launch(b_reduce, grid_of(ctx, b.fine_csr.K), kNT, 0, st, b.fine_csr, b.d_ctl, 2, 1, b.d_partial);
   CD_LAUNCHED(ctx);
-  b_restart<<<gi, 128, 0, st>>>(b.items, b.d_ctl, p.stop_rule, p.red_factor, p.res_norm_min);
+  (void)cd_launch(b_restart, gi, 128, 0, st, b.items, b.d_ctl, p.stop_rule, p.red_factor, p.res_norm_min);
   CD_LAUNCHED(ctx);
-  b_scale0<<<grid_of(ctx, b.fine_vec.total), kNT, 0, st>>>(b.fine_vec, b.d_ctl);
+  (void)cd_launch(b_scale0, grid_of(ctx, b.fine_vec.total), kNT, 0, st, b.fine_vec, b.d_ctl);
   CD_LAUNCHED(ctx);
-  b_begin_step<<<gi, 128, 0, st>>>(b.items, b.d_ctl);
+  (void)cd_launch(b_begin_step, gi, 128, 0, st, b.items, b.d_ctl);
   CD_LAUNCHED(ctx);
   // one Arnoldi step: z = M^{-1} v_j, w = A z, CGS2, Givens
   int rc = batch_cycle(ctx, b);
   if (rc) return rc;
-  b_matvec<<<grid_of(ctx, b.fine_csr.total), kNT, 0, st>>>(b.fine_csr, b.d_ctl, 0, b.d_partial);
+  (void)cd_launch(b_matvec, grid_of(ctx, b.fine_csr.total), kNT, 0, st, b.fine_csr, b.d_ctl, 0, b.d_partial);
   CD_LAUNCHED(ctx);
   for (int mode = 0; mode < 3; mode++)
   {
-    b_gs<<<grid_of(ctx, b.fine_vec.total), kNT, 0, st>>>(b.fine_vec, b.d_ctl, mode, b.d_partial);
+    (void)cd_launch(b_gs, grid_of(ctx, b.fine_vec.total), kNT, 0, st, b.fine_vec, b.d_ctl, mode, b.d_partial);
     CD_LAUNCHED(ctx);
-    b_reduce<<<grid_of(ctx, b.fine_vec.K), kNT, 0, st>>>(b.fine_vec, b.d_ctl, mode, 0, b.d_partial);
+    (void)cd_launch(b_reduce, grid_of(ctx, b.fine_vec.K), kNT, 0, st, b.fine_vec, b.d_ctl, mode, 0, b.d_partial);
     CD_LAUNCHED(ctx);
   }
-  b_givens<<<gi, 128, 0, st>>>(b.items, b.d_ctl, p.maxit, p.minit, p.div_factor);
+  (void)cd_launch(b_givens, gi, 128, 0, st, b.items, b.d_ctl, p.maxit, p.minit, p.div_factor);
   CD_LAUNCHED(ctx);
-  b_next_update<<<grid_of(ctx, b.fine_vec.total), kNT, 0, st>>>(b.fine_vec, b.d_ctl);
+  (void)cd_launch(b_next_update, grid_of(ctx, b.fine_vec.total), kNT, 0, st, b.fine_vec, b.d_ctl);
   CD_LAUNCHED(ctx);
-  b_post<<<gi, 128, 0, st>>>(b.items, b.d_ctl, b.d_state);
+  (void)cd_launch(b_post, gi, 128, 0, st, b.items, b.d_ctl, b.d_state);
   CD_LAUNCHED(ctx);
   return CDGPU_OK;
 }
@@ -1371,11 +1390,11 @@ int cdgpu_batch_tcd_step(cdgpu_ctx *ctx, int batch_id, int iterations, int *max_
       CD_CUDA(ctx, cudaFuncSetAttribute(b_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     const long long before = ctx->launches;
     CD_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    b_tcd_rhs<<<std::max(1, std::min(b.tcd_csr.total, ctx->sm_count * 8)), kNT, 0, ctx->stream>>>(b.tcd_csr, b.d_ctl);
+    (void)cd_launch(b_tcd_rhs, std::max(1, std::min(b.tcd_csr.total, ctx->sm_count * 8)), kNT, 0, ctx->stream, b.tcd_csr, b.d_ctl);
     rc = cudaGetLastError() == cudaSuccess ? CDGPU_OK : CDGPU_ERR_CUDA;
     if (!rc)
     {
-      b_tcd_begin<<<1, 256, 0, ctx->stream>>>(b.tcd_items, b.d_ctl);
+      (void)cd_launch(b_tcd_begin, 1, 256, 0, ctx->stream, b.tcd_items, b.d_ctl);
       for (int it = 0; it < iterations && !rc; it++) rc = batch_iteration(ctx, b);
     }
     cudaGraph_t g = nullptr;

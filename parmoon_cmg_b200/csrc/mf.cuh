@@ -332,6 +332,7 @@ __global__ void mf_row_kernel(int n, int na, int n_cells, const int *__restrict_
 __global__ void mf_convert_kernel(int n_cells, int T, int Tr, int nbf, const double *__restrict__ cellcoef,
                                   const double *__restrict__ R, float *__restrict__ cf32, float *__restrict__ R32)
 {
+  CD_PDL_ENTRY();
   const long total_c = (long)n_cells * T, total_r = (long)T * nbf * nbf;
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total_c + total_r; e += (long)gridDim.x * blockDim.x)
   {

@@ -354,6 +354,7 @@ __global__ void reduce_partials_kernel(int nblocks, int nslots, const double *__
 
 __global__ void sum_blocks_kernel(int nblocks, const double *__restrict__ partial, double *out)
 {
+  CD_PDL_ENTRY();
   __shared__ double red[32];
   double t = 0;
   // fixed per-thread order, then fixed tree
@@ -380,6 +381,7 @@ __global__ void scale_kernel(int n, double alpha, const double *__restrict__ x, 
 __global__ void update_kernel(int n, int k, const double *__restrict__ c, const double *__restrict__ Z,
                               double *__restrict__ x)
 {
+  CD_PDL_ENTRY();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double s = 0;
@@ -389,6 +391,7 @@ __global__ void update_kernel(int n, int k, const double *__restrict__ c, const 
 
 __global__ void axpy_kernel(int n, double alpha, const double *__restrict__ x, double *__restrict__ y)
 {
+  CD_PDL_ENTRY();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) y[i] += alpha * x[i];
 }
@@ -779,6 +782,7 @@ int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m)
 __global__ void csr_to_dense_kernel(int na, const int *__restrict__ rp, const int *__restrict__ kc,
                                     const double *__restrict__ a, double *__restrict__ dense)
 {
+  CD_PDL_ENTRY();
   int r = blockIdx.x;
   for (int c = threadIdx.x; c < na; c += blockDim.x) dense[(size_t)r * na + c] = 0.0;
   __syncthreads();
@@ -792,6 +796,7 @@ __global__ void csr_to_dense_kernel(int na, const int *__restrict__ rp, const in
 __global__ void __launch_bounds__(1024) gj_invert_kernel(int n, double *__restrict__ g, int use_smem,
                                                          int *__restrict__ piv, int *__restrict__ flag)
 {
+  CD_PDL_ENTRY();
   extern __shared__ double sm[];
   double *A = use_smem ? sm : g;
   __shared__ double red_v[32];
@@ -892,7 +897,7 @@ static int refresh_coarse_inverse(cdgpu_ctx *ctx, Hierarchy &h)
   CD_CUDA(ctx, cudaMemsetAsync(h.d_cpiv + na, 0, sizeof(int), ctx->stream));
   if (na > 0)
   {
-    csr_to_dense_kernel<<<na, 128, 0, ctx->stream>>>(na, s.d_row_ptr, s.d_kcol, s.d_a, h.d_cinv);
+    (void)cd_launch(csr_to_dense_kernel, na, 128, 0, ctx->stream, na, s.d_row_ptr, s.d_kcol, s.d_a, h.d_cinv);
     CD_LAUNCHED(ctx);
     size_t sm = sizeof(double) * (size_t)na * na;
     int use_smem = sm <= 200 * 1024;
@@ -900,7 +905,7 @@ static int refresh_coarse_inverse(cdgpu_ctx *ctx, Hierarchy &h)
       CD_CUDA(ctx, cudaFuncSetAttribute(gj_invert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     // one warp per four rows (at most 32 warps): short barriers for small coarse levels
     const int nt = std::min(1024, 32 * std::max(1, (na + 3) / 4));
-    gj_invert_kernel<<<1, nt, use_smem ? sm : 0, ctx->stream>>>(na, h.d_cinv, use_smem, h.d_cpiv, h.d_cpiv + na);
+    (void)cd_launch(gj_invert_kernel, 1, nt, use_smem ? sm : 0, ctx->stream, na, h.d_cinv, use_smem, h.d_cpiv, h.d_cpiv + na);
     CD_LAUNCHED(ctx);
   }
   // the zero-pivot flag is copied back behind the inversion and checked after the solve,
@@ -922,7 +927,7 @@ static int finest_defect_norm(cdgpu_ctx *ctx, Hierarchy &h, const double *x, con
   const int grid = csr_grid(ctx, s.shape, s.n_dof); // <= 8 blocks per SM, within d_partial
   csr_defect<double>(ctx, s, x, f, d, h.d_partial, grid);
   CD_LAUNCHED(ctx);
-  sum_blocks_kernel<<<1, 256, 0, ctx->stream>>>(grid, h.d_partial, norm_out_dev);
+  (void)cd_launch(sum_blocks_kernel, 1, 256, 0, ctx->stream, grid, h.d_partial, norm_out_dev);
   CD_LAUNCHED(ctx);
   return CDGPU_OK;
 }
@@ -942,7 +947,7 @@ int defect64(cdgpu_ctx *ctx, const Space &s, const double *x, const double *f, d
   if ((rc = dev_alloc(ctx, &partial, grid)) || (rc = dev_alloc(ctx, &out, 1))) return rc;
   csr_defect<double>(ctx, s, x, f, d, partial, grid);
   CD_LAUNCHED(ctx);
-  sum_blocks_kernel<<<1, 256, 0, ctx->stream>>>(grid, partial, out);
+  (void)cd_launch(sum_blocks_kernel, 1, 256, 0, ctx->stream, grid, partial, out);
   CD_LAUNCHED(ctx);
   double r2 = 0;
   CD_CUDA(ctx, cudaMemcpyAsync(&r2, out, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1076,7 +1081,7 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
         }
         CD_CUDA(ctx, cudaMemcpyAsync(h.d_ctl + 100, y.data(), sizeof(double) * (i + 1), cudaMemcpyHostToDevice,
                                      ctx->stream));
-        update_kernel<<<blocks, 256, 0, ctx->stream>>>(n, i + 1, h.d_ctl + 100, h.d_Z, x);
+        (void)cd_launch(update_kernel, blocks, 256, 0, ctx->stream, n, i + 1, h.d_ctl + 100, h.d_Z, x);
         CD_LAUNCHED(ctx);
         ret = j;
         done = true;
@@ -1099,7 +1104,7 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
       for (int b = a - 1; b >= 0; b--) y[b] -= H[(size_t)b * m + a] * y[a];
     }
     CD_CUDA(ctx, cudaMemcpyAsync(h.d_ctl + 100, y.data(), sizeof(double) * m, cudaMemcpyHostToDevice, ctx->stream));
-    update_kernel<<<blocks, 256, 0, ctx->stream>>>(n, m, h.d_ctl + 100, h.d_Z, x);
+    (void)cd_launch(update_kernel, blocks, 256, 0, ctx->stream, n, m, h.d_ctl + 100, h.d_Z, x);
     CD_LAUNCHED(ctx);
     if ((rc = finest_defect_norm(ctx, h, x, f, V(0), h.d_ctl))) return rc;
     if ((rc = read_ctl(ctx, h, 1))) return rc;
@@ -1135,7 +1140,7 @@ static int fixed_point(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &
   for (i = 1; i <= maxite; i++)
   {
     if ((rc = precondition(ctx, h, p, d, z))) return rc;
-    axpy_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, 1.0, z, x);
+    (void)cd_launch(axpy_kernel, (n + 255) / 256, 256, 0, ctx->stream, n, 1.0, z, x);
     CD_LAUNCHED(ctx);
     if ((rc = finest_defect_norm(ctx, h, x, f, d, h.d_ctl))) return rc;
     if ((rc = read_ctl(ctx, h, 1))) return rc;
@@ -1174,7 +1179,7 @@ static int refresh_mf(cdgpu_ctx *ctx, Hierarchy &h)
       const int T = s.mf_T, Tr = n_rhs_tensors(s.dim, s.ref_disctype);
       const long total = (long)s.n_cells * T + (long)T * s.nbf * s.nbf;
       const int grid = (int)std::min<long>((total + 255) / 256, (long)ctx->sm_count * 8);
-      mf_convert_kernel<<<grid, 256, 0, ctx->stream>>>(s.n_cells, T, Tr, s.nbf, s.d_cellcoef, s.d_ref, s.d_cf32,
+      (void)cd_launch(mf_convert_kernel, grid, 256, 0, ctx->stream, s.n_cells, T, Tr, s.nbf, s.d_cellcoef, s.d_ref, s.d_cf32,
                                                         s.d_R32);
       CD_LAUNCHED(ctx);
       s.mf_version = s.assembly_version;

@@ -39,6 +39,7 @@ void free_tcd(Tcd *t)
 // y += alpha * x over the entries of the active rows [0, n_active_entries)
 __global__ void matadd_kernel(long n, double alpha, const double *__restrict__ x, double *__restrict__ y)
 {
+  CD_PDL_ENTRY();
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) y[i] += alpha * x[i];
 }
@@ -49,6 +50,7 @@ __global__ void tcd_rhs_kernel(int n, int n_active, const int *__restrict__ rp, 
                                const double *__restrict__ f, double c3, double c4, double *__restrict__ x,
                                double *__restrict__ B)
 {
+  CD_PDL_ENTRY();
   int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
   if (r >= n_active)
@@ -66,6 +68,7 @@ __global__ void tcd_rhs_kernel(int n, int n_active, const int *__restrict__ rp, 
 
 __global__ void dirichlet_copy_kernel(int n, int n_active, const double *__restrict__ f, double *__restrict__ x)
 {
+  CD_PDL_ENTRY();
   int r = n_active + blockIdx.x * blockDim.x + threadIdx.x;
   if (r < n) x[r] = f[r];
 }
@@ -75,6 +78,7 @@ __global__ void install_system_kernel(int n, const int *__restrict__ rp, const i
                                       const double *__restrict__ M, double *__restrict__ a, float *__restrict__ a32,
                                       double *__restrict__ diag, float *__restrict__ diag32)
 {
+  CD_PDL_ENTRY();
   int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
   for (int j = rp[r]; j < rp[r + 1]; j++)
@@ -90,7 +94,7 @@ static int matadd(cdgpu_ctx *ctx, const Space &s, double alpha, const double *x,
 {
   long n = s.h_row_ptr[s.n_active];
   if (n == 0) return CDGPU_OK;
-  matadd_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, alpha, x, y);
+  (void)cd_launch(matadd_kernel, (unsigned)((n + 255) / 256), 256, 0, ctx->stream, n, alpha, x, y);
   CD_LAUNCHED(ctx);
   return CDGPU_OK;
 }
@@ -191,13 +195,13 @@ int cdgpu_tcd_step_device(cdgpu_ctx *ctx, int tcd_id, const cdgpu_solver_params 
   for (int l = 0; l < L; l++)
     if ((rc = matadd(ctx, *h.lev[l].sp, -tau * theta2, t->A[l], t->M[l]))) return rc;
   const Space &f = *h.lev[L - 1].sp;
-  tcd_rhs_kernel<<<(f.n_dof + 255) / 256, 256, 0, ctx->stream>>>(f.n_dof, f.n_active, f.d_row_ptr, f.d_kcol,
+  (void)cd_launch(tcd_rhs_kernel, (f.n_dof + 255) / 256, 256, 0, ctx->stream, f.n_dof, f.n_active, f.d_row_ptr, f.d_kcol,
                                                                 t->M[L - 1], t->d_f_old, t->d_f, tau * theta3,
                                                                 tau * theta4, d_sol, t->d_B);
   CD_LAUNCHED(ctx);
   if (f.n_dof > f.n_active)
   {
-    dirichlet_copy_kernel<<<(f.n_dof - f.n_active + 255) / 256, 256, 0, ctx->stream>>>(f.n_dof, f.n_active, t->d_f,
+    (void)cd_launch(dirichlet_copy_kernel, (f.n_dof - f.n_active + 255) / 256, 256, 0, ctx->stream, f.n_dof, f.n_active, t->d_f,
                                                                                      d_sol);
     CD_LAUNCHED(ctx);
   }
@@ -207,7 +211,7 @@ int cdgpu_tcd_step_device(cdgpu_ctx *ctx, int tcd_id, const cdgpu_solver_params 
     Space &s = *h.lev[l].sp;
     if ((rc = matadd(ctx, s, -gamma + tau * theta1, t->A[l], t->M[l]))) return rc;
     s.mf_T = 0; // the system matrix is a combination, not one affine assembly
-    install_system_kernel<<<(s.n_dof + 255) / 256, 256, 0, ctx->stream>>>(s.n_dof, s.d_row_ptr, s.d_kcol, t->M[l],
+    (void)cd_launch(install_system_kernel, (s.n_dof + 255) / 256, 256, 0, ctx->stream, s.n_dof, s.d_row_ptr, s.d_kcol, t->M[l],
                                                                         s.d_a, s.d_a32, s.d_diag, s.d_diag32);
     CD_LAUNCHED(ctx);
     s.assembly_version++;
