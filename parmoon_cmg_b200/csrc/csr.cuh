@@ -24,6 +24,10 @@ template <typename T> struct CsrArgs
   T *y = nullptr, *y2 = nullptr;
   T omega = 0;
   double *partial = nullptr;
+  // 1: the kernel loads its first rows' pointers, columns and values before waiting for its
+  // predecessor (set for the kernels of the captured multigrid cycle, where no kernel writes
+  // a matrix; see CD_PDL_WAIT)
+  int pre = 0;
 };
 
 template <int G, typename T> __device__ __forceinline__ T csr_group_sum(T v)
@@ -67,40 +71,77 @@ __device__ __forceinline__ void csr_epilogue(const CsrArgs<T> &p, int r, T s, do
   }
 }
 
+// the pointers, columns and values of row r for a group of GS threads (U per thread,
+// predicated on the row length)
+template <typename T, int GS, int U> struct CsrRow
+{
+  int b, e;
+  int c[U];
+  T v[U];
+};
+template <typename T, int GS, int U>
+__device__ __forceinline__ void csr_load_row(const CsrArgs<T> &p, int r, int rows_end, int lane, CsrRow<T, GS, U> &w)
+{
+  w.b = 0;
+  w.e = 0;
+  if (r < rows_end)
+  {
+    w.b = p.rp[r];
+    w.e = p.rp[r + 1];
+  }
+#pragma unroll
+  for (int i = 0; i < U; i++)
+  {
+    const int j = w.b + lane + i * GS;
+    w.c[i] = j < w.e ? __ldcs(p.kc + j) : -1;
+    w.v[i] = j < w.e ? __ldcs(p.a + j) : T(0);
+  }
+}
+
+// gathers, group sum and epilogue of row r (every lane of the warp calls it)
+template <typename T, int GS, int U, int MODE>
+__device__ __forceinline__ void csr_do_row(const CsrArgs<T> &p, int r, int rows_end, int lane,
+                                           const CsrRow<T, GS, U> &w, double &acc)
+{
+  T s = 0;
+  if (r < rows_end)
+  {
+#pragma unroll
+    for (int i = 0; i < U; i++)
+      if (w.c[i] >= 0) s += w.v[i] * __ldg(p.x + w.c[i]);
+    for (int j = w.b + lane + U * GS; j < w.e; j += GS) s += p.a[j] * __ldg(p.x + p.kc[j]);
+  }
+  s = csr_group_sum<GS>(s);
+  if (r < rows_end && lane == 0) csr_epilogue<T, MODE>(p, r, s, acc);
+}
+
 template <typename T, int GS, int U, int MODE, int MINB = 1>
 __global__ void __launch_bounds__(256, MINB) csr_kernel(CsrArgs<T> p)
 {
-  CD_PDL_ENTRY();
   constexpr int NT = 256;
   __shared__ double red[NT / 32];
   const int lane = threadIdx.x % GS, sub = (threadIdx.x % 32) / GS;
   const long nwarp = (long)gridDim.x * NT / 32;
   const int rows_end = MODE == CM_PROLONG ? p.n_active : p.n;
+  const long step = nwarp * (32 / GS);
+  long base = ((long)blockIdx.x * NT + threadIdx.x) / 32 * (32 / GS);
   double acc = 0;
-  for (long base = ((long)blockIdx.x * NT + threadIdx.x) / 32 * (32 / GS); base < rows_end;
-       base += nwarp * (32 / GS))
+  if (p.pre && base < rows_end)
   {
-    const int r = (int)base + sub;
-    T s = 0;
-    if (r < rows_end)
-    {
-      const int b = p.rp[r], e = p.rp[r + 1];
-      int c[U];
-      T v[U];
-#pragma unroll
-      for (int i = 0; i < U; i++)
-      {
-        const int j = b + lane + i * GS;
-        c[i] = j < e ? __ldcs(p.kc + j) : -1;
-        v[i] = j < e ? __ldcs(p.a + j) : T(0);
-      }
-#pragma unroll
-      for (int i = 0; i < U; i++)
-        if (c[i] >= 0) s += v[i] * __ldg(p.x + c[i]);
-      for (int j = b + lane + U * GS; j < e; j += GS) s += p.a[j] * __ldg(p.x + p.kc[j]);
-    }
-    s = csr_group_sum<GS>(s);
-    if (r < rows_end && lane == 0) csr_epilogue<T, MODE>(p, r, s, acc);
+    // the first row's matrix data before the wait, its gathers after
+    CsrRow<T, GS, U> w;
+    csr_load_row<T, GS, U>(p, (int)base + sub, rows_end, lane, w);
+    CD_PDL_ENTRY();
+    csr_do_row<T, GS, U, MODE>(p, (int)base + sub, rows_end, lane, w, acc);
+    base += step;
+  }
+  else
+    CD_PDL_ENTRY();
+  for (; base < rows_end; base += step)
+  {
+    CsrRow<T, GS, U> w;
+    csr_load_row<T, GS, U>(p, (int)base + sub, rows_end, lane, w);
+    csr_do_row<T, GS, U, MODE>(p, (int)base + sub, rows_end, lane, w, acc);
   }
   if (MODE == CM_DEFECT && p.partial)
   {
@@ -110,7 +151,7 @@ __global__ void __launch_bounds__(256, MINB) csr_kernel(CsrArgs<T> p)
     if (threadIdx.x == 0)
     {
       double tot = 0;
-      for (int w = 0; w < NT / 32; w++) tot += red[w];
+      for (int wi = 0; wi < NT / 32; wi++) tot += red[wi];
       p.partial[blockIdx.x] = tot;
     }
   }
@@ -124,7 +165,7 @@ __global__ void __launch_bounds__(256, MINB) csr_kernel(CsrArgs<T> p)
 template <typename T, int GS, int U, int MODE, int MINB = 1>
 __global__ void __launch_bounds__(256, MINB) csr_pipe_kernel(CsrArgs<T> p)
 {
-  CD_PDL_ENTRY();
+  if (!p.pre) CD_PDL_ENTRY();
   constexpr int NT = 256;
   __shared__ double red[NT / 32];
   const int lane = threadIdx.x % GS, sub = (threadIdx.x % 32) / GS;
@@ -144,6 +185,7 @@ __global__ void __launch_bounds__(256, MINB) csr_pipe_kernel(CsrArgs<T> p)
     c[i] = j < e ? __ldcs(p.kc + j) : -1;
     v[i] = j < e ? __ldcs(p.a + j) : T(0);
   }
+  if (p.pre) CD_PDL_ENTRY(); // the first rows' matrix data is in flight
   double acc = 0;
   for (; base < rows_end; base += step)
   {
@@ -192,8 +234,10 @@ inline int csr_grid(const cdgpu_ctx *ctx, const CsrShape &sh, int rows)
 }
 
 template <typename T, int MODE>
-inline void launch_csr(cdgpu_ctx *ctx, const CsrShape &sh, const CsrArgs<T> &p, int grid)
+inline void launch_csr(cdgpu_ctx *ctx, const CsrShape &sh, const CsrArgs<T> &pa, int grid)
 {
+  CsrArgs<T> p = pa;
+  p.pre = ctx->pdl_pre ? 1 : 0;
   switch (sh.gs)
   {
     case 1: (void)cd_launch(csr_kernel<T, 1, 8, MODE>, grid, 256, 0, ctx->stream, p); break;

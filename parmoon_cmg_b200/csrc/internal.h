@@ -166,6 +166,9 @@ struct cdgpu_ctx
   long long launches = 0;
   std::vector<Space *> spaces;
   std::vector<Hierarchy *> mgs;
+  // set while the multigrid cycle is recorded into its graph: its kernels load the data that
+  // no kernel of the cycle writes before waiting for their predecessor
+  bool pdl_pre = false;
   int *d_err = nullptr; // assembly error flag (device) and its pinned host mirror
   int *h_err = nullptr;
 };
@@ -187,12 +190,21 @@ int cuda_fail(cdgpu_ctx *ctx, cudaError_t e, const char *what);
 
 // Programmatic dependent launch (sm_90+): a kernel started with cd_launch may be scheduled
 // while the previous kernel of the stream (or captured graph) still runs.  Every kernel
-// launched that way begins with CD_PDL_ENTRY: it first lets its own successor be scheduled
-// (griddepcontrol.launch_dependents) and then waits until its predecessor has completed and
-// its memory is visible (griddepcontrol.wait), before its first global memory access.  Only
-// the launch and the CTA scheduling overlap, never the work.  Without the launch attribute
-// both instructions return at once.
-#define CD_PDL_ENTRY() asm volatile("griddepcontrol.launch_dependents;\n\tgriddepcontrol.wait;" ::: "memory")
+// launched that way waits until its predecessor has completed and its memory is visible
+// (griddepcontrol.wait) before it reads or writes anything the predecessor may touch, and
+// only then lets its own successor be scheduled (griddepcontrol.launch_dependents).  So at
+// most two kernels of a chain are resident at once, and the later one runs only the part
+// before its wait: the launch, the CTA scheduling and, in kernels of the captured multigrid
+// cycle, loads of data that no kernel of the cycle writes (matrices, transfer operators,
+// incidence lists, reference tensors).  Without the launch attribute both instructions
+// return at once.
+#define CD_PDL_WAIT() asm volatile("griddepcontrol.wait;" ::: "memory")
+#define CD_PDL_TRIGGER() asm volatile("griddepcontrol.launch_dependents;" ::: "memory")
+#define CD_PDL_ENTRY() \
+  do {                 \
+    CD_PDL_WAIT();     \
+    CD_PDL_TRIGGER();  \
+  } while (0)
 
 template <typename... KArgs, typename... Args>
 inline cudaError_t cd_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,

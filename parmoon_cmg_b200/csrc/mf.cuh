@@ -151,9 +151,11 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
                                                               const float *__restrict__ cf32,
                                                               const float *__restrict__ R32,
                                                               const float *__restrict__ x, float *__restrict__ ybuf,
-                                                              int *__restrict__ err)
+                                                              int *__restrict__ err, int pre)
 {
-  CD_PDL_ENTRY();
+  // with pre, the tensors, the shared-memory set-up and the first tile's DOF numbers and
+  // coefficients (written by no kernel of the cycle) come before the wait for the predecessor
+  if (!pre) CD_PDL_ENTRY();
   constexpr int MT = 128, KP = 32, NB = 27, N = 32 * T, NH = N / 2;
   extern __shared__ __align__(1024) unsigned char mf_sm[];
   unsigned char *As = mf_sm;                    // 128 x 32 x 4 = 16 KB
@@ -169,37 +171,41 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
     *(float *)(Bs + mf_core_off(n, k, N)) = v;
   }
   for (int e = tid; e < MT * KP; e += blockDim.x) ((float *)As)[e] = 0.f;
+  if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mf_smem_u32(&mbar)), "r"(1));
+  const int n_tiles = (n_cells + MT - 1) / MT;
+  // the next tile's cell values and coefficients, one cell per thread (thread r gathers and
+  // later contracts cell c0 + r): loaded before the current tile's products are awaited, so
+  // the gather latency overlaps the tensor-core work and the epilogue
+  float vn[NB], cn[T];
+  int gq[NB];
+  auto prefetch_idx = [&](int tile) {
+    const int c = tile * MT + tid;
+    const bool in = tile < n_tiles && c < n_cells;
+#pragma unroll
+    for (int k = 0; k < NB; k++) gq[k] = in ? __ldg(gn + (size_t)c * NB + k) : -1;
+#pragma unroll
+    for (int t = 0; t < T; t++) cn[t] = in ? __ldg(cf32 + (size_t)c * T + t) : 0.f;
+  };
+  auto prefetch_x = [&]() {
+#pragma unroll
+    for (int k = 0; k < NB; k++) vn[k] = gq[k] >= 0 ? __ldg(x + gq[k]) : 0.f;
+  };
+  prefetch_idx(blockIdx.x);
+  if (pre) CD_PDL_ENTRY();
   if (warp == 0)
   {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(mf_smem_u32(&tmem_base)),
                  "r"(512));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
   }
-  if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mf_smem_u32(&mbar)), "r"(1));
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
   const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(NH >> 3) << 17) | ((uint32_t)(MT >> 4) << 24);
-  const int n_tiles = (n_cells + MT - 1) / MT;
   uint32_t phase = 0;
   bool ok = true;
-  // the next tile's cell values and coefficients, one cell per thread (thread r gathers and
-  // later contracts cell c0 + r): loaded before the current tile's products are awaited, so
-  // the gather latency overlaps the tensor-core work and the epilogue
-  float vn[NB], cn[T];
-  auto prefetch = [&](int tile) {
-    const int c = tile * MT + tid;
-    const bool in = tile < n_tiles && c < n_cells;
-    int g[NB];
-#pragma unroll
-    for (int k = 0; k < NB; k++) g[k] = in ? __ldg(gn + (size_t)c * NB + k) : -1;
-#pragma unroll
-    for (int t = 0; t < T; t++) cn[t] = in ? __ldg(cf32 + (size_t)c * T + t) : 0.f;
-#pragma unroll
-    for (int k = 0; k < NB; k++) vn[k] = g[k] >= 0 ? __ldg(x + g[k]) : 0.f;
-  };
-  prefetch(blockIdx.x);
+  prefetch_x();
   for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
   {
     const int c0 = tile * MT;
@@ -230,7 +236,8 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
                        mf_smem_u32(&mbar))
                    : "memory");
     }
-    prefetch(tile + gridDim.x);
+    prefetch_idx(tile + gridDim.x);
+    prefetch_x();
     // bounded wait for this tile's products (an error flag instead of a hang)
     uint32_t done = 0;
     if (ok)
@@ -292,23 +299,29 @@ template <int NBF, int MODE>
 __global__ void mf_row_kernel(int n, int na, int n_cells, const int *__restrict__ inc_ptr,
                               const int *__restrict__ inc, const float *__restrict__ ybuf,
                               const float *__restrict__ x, const float *__restrict__ f,
-                              const float *__restrict__ diag, float *__restrict__ out, float omega)
+                              const float *__restrict__ diag, float *__restrict__ out, float omega, int pre)
 {
-  CD_PDL_ENTRY();
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
+  // the first 8 incidences (every DOF of a structured hexahedral or quadrilateral mesh) are
+  // loaded at once, then added in ascending cell order; longer lists continue one by one.
+  // With pre, the incidence list (written by no kernel of the cycle) is read before the wait.
+  int b = 0, e = 0, ei[8];
+  auto load_inc = [&]() {
+    b = inc_ptr[r];
+    e = inc_ptr[r + 1];
+#pragma unroll
+    for (int j = 0; j < 8; j++) ei[j] = b + j < e ? __ldg(inc + b + j) : -1;
+  };
+  if (pre && r < na) load_inc();
+  CD_PDL_ENTRY();
   if (r >= na)
   {
     out[r] = MODE == MF_JACOBI ? f[r] : f[r] - x[r];
     return;
   }
-  // the first 8 incidences (every DOF of a structured hexahedral or quadrilateral mesh) are
-  // loaded at once, then added in ascending cell order; longer lists continue one by one
-  const int b = inc_ptr[r], e = inc_ptr[r + 1];
-  int ei[8];
+  if (!pre) load_inc();
   float yv[8];
-#pragma unroll
-  for (int j = 0; j < 8; j++) ei[j] = b + j < e ? __ldg(inc + b + j) : -1;
 #pragma unroll
   for (int j = 0; j < 8; j++)
   {
@@ -371,13 +384,13 @@ inline void mf_apply_cells(cdgpu_ctx *ctx, const Space &s, const float *x)
     if (s.mf_T == 10)
     {
       (void)cd_launch(mf_cell27_tc_kernel<10>, grid, 128, 120 * 1024, ctx->stream, s.n_cells, s.d_gn, s.d_cf32,
-                      s.d_R32, x, s.d_ybuf, ctx->d_err);
+                      s.d_R32, x, s.d_ybuf, ctx->d_err, ctx->pdl_pre ? 1 : 0);
       return;
     }
     if (s.mf_T == 13)
     {
       (void)cd_launch(mf_cell27_tc_kernel<13>, grid, 128, 120 * 1024, ctx->stream, s.n_cells, s.d_gn, s.d_cf32,
-                      s.d_R32, x, s.d_ybuf, ctx->d_err);
+                      s.d_R32, x, s.d_ybuf, ctx->d_err, ctx->pdl_pre ? 1 : 0);
       return;
     }
   }
@@ -406,9 +419,9 @@ inline void mf_rows(cdgpu_ctx *ctx, const Space &s, const float *x, const float 
   const int grid = (s.n_dof + 255) / 256;
   switch (s.nbf)
   {
-    case 27: (void)cd_launch(mf_row_kernel<27, MODE>, grid, 256, 0, ctx->stream, s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega); break;
-    case 9: (void)cd_launch(mf_row_kernel<9, MODE>, grid, 256, 0, ctx->stream, s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega); break;
-    case 8: (void)cd_launch(mf_row_kernel<8, MODE>, grid, 256, 0, ctx->stream, s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega); break;
-    default: (void)cd_launch(mf_row_kernel<4, MODE>, grid, 256, 0, ctx->stream, s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega); break;
+    case 27: (void)cd_launch(mf_row_kernel<27, MODE>, grid, 256, 0, ctx->stream, s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega, ctx->pdl_pre ? 1 : 0); break;
+    case 9: (void)cd_launch(mf_row_kernel<9, MODE>, grid, 256, 0, ctx->stream, s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega, ctx->pdl_pre ? 1 : 0); break;
+    case 8: (void)cd_launch(mf_row_kernel<8, MODE>, grid, 256, 0, ctx->stream, s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega, ctx->pdl_pre ? 1 : 0); break;
+    default: (void)cd_launch(mf_row_kernel<4, MODE>, grid, 256, 0, ctx->stream, s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega, ctx->pdl_pre ? 1 : 0); break;
   }
 }

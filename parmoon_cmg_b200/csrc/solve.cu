@@ -711,7 +711,9 @@ static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, 
     cudaGraph_t g = nullptr;
     const long long before = ctx->launches;
     CD_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    ctx->pdl_pre = true; // kernels of the cycle load matrix data before waiting (CD_PDL_WAIT)
     rc = k == 1 ? mg_record<float>(ctx, h, p) : mg_record<double>(ctx, h, p);
+    ctx->pdl_pre = false;
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
     h.graph_nodes[k] = ctx->launches - before; // kernels per replay; capturing runs none
     ctx->launches = before;
