@@ -61,6 +61,9 @@ static void free_mg(Hierarchy *h)
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
   if (h->h_io) cudaFreeHost(h->h_io);
   if (h->h_cflag) cudaFreeHost(h->h_cflag);
+  if (h->h_slot) cudaFreeHost(h->h_slot);
+  for (auto &e : h->ev_slot)
+    if (e) cudaEventDestroy(e);
   delete h;
 }
 

@@ -143,6 +143,8 @@ struct Hierarchy
   double **d_io = nullptr;
   double **h_io = nullptr; // pinned ring of 64 (in, out) pairs
   unsigned io_slot = 0;
+  double *h_slot = nullptr;            // pinned: two slots of an FGMRES iteration's control block
+  cudaEvent_t ev_slot[2] = {nullptr, nullptr}; // recorded behind each slot's copy
   int *h_cflag = nullptr;     // pinned copy of the coarse inversion's zero-pivot flag
   bool cflag_pending = false; // copy enqueued, not yet checked
 };

@@ -370,6 +370,17 @@ __global__ void sum_blocks_kernel(int nblocks, const double *__restrict__ partia
   }
 }
 
+// y = x / sqrt(*nrm2) unless *nrm2 == 0 (the next Arnoldi vector, scaled on the device so that
+// the host need not have read the norm yet)
+__global__ void scale_norm_kernel(int n, const double *__restrict__ nrm2, const double *__restrict__ x,
+                                  double *__restrict__ y)
+{
+  CD_PDL_ENTRY();
+  const double hn = sqrt(*nrm2);
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (hn != 0 && i < n) y[i] = (1.0 / hn) * x[i];
+}
+
 __global__ void scale_kernel(int n, double alpha, const double *__restrict__ x, double *__restrict__ y)
 {
   CD_PDL_ENTRY();
@@ -774,6 +785,8 @@ int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m)
         (rc = dev_alloc(ctx, &h.d_x, n)) || (rc = dev_alloc(ctx, &h.d_b, n)))
       return rc;
     CD_CUDA(ctx, cudaMallocHost((void **)&h.h_ctl, 256 * sizeof(double)));
+    CD_CUDA(ctx, cudaMallocHost((void **)&h.h_slot, 2 * 80 * sizeof(double)));
+    for (auto &e : h.ev_slot) CD_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     CD_CUDA(ctx, cudaMallocHost((void **)&h.h_io, 128 * sizeof(double *)));
     if ((rc = dev_alloc(ctx, &h.d_io, 2))) return rc;
   }
@@ -1036,11 +1049,18 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
     CD_LAUNCHED(ctx);
     std::fill(sv.begin(), sv.end(), 0.0);
     sv[0] = beta;
-    int i;
-    for (i = 0; i < m && j <= maxite; i++, j++)
-    {
-      if ((rc = precondition(ctx, h, p, V(i), Z(i)))) return rc;
-      if ((rc = spmv64(ctx, s, Z(i), h.d_w))) return rc;
+    // Iteration i on the device: the preconditioner on v_i, w = A z_i, the Gram-Schmidt passes,
+    // a copy of the control block to pinned slot i % 2 (and an event behind it), and
+    // v_{i+1} = w / ||w||, which needs no host value.  The host then applies the Givens
+    // rotations and the stopping tests.  While it waits for iteration i it has, as a rule,
+    // already enqueued iteration i + 1, so the device does not idle during the host's part;
+    // it does not when the residual predicted from the convergence so far is within a factor
+    // of 4 of the stopping threshold, because an iteration enqueued after the one that
+    // converges is wasted.  Which iterations are enqueued early changes no arithmetic.
+    auto enqueue = [&](int i) -> int {
+      int rc2;
+      if ((rc2 = precondition(ctx, h, p, V(i), Z(i)))) return rc2;
+      if ((rc2 = spmv64(ctx, s, Z(i), h.d_w))) return rc2;
       int k = i + 1, pb = h.partial_blocks;
       // pass 1: h1 = V^T w
       launch_gs<GS_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, nullptr, h.d_partial);
@@ -1057,16 +1077,32 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
       CD_LAUNCHED(ctx);
       (void)cd_launch(reduce_partials_kernel, 1, 256, 0, ctx->stream, pb, 1, h.d_partial, h.d_ctl + 66);
       CD_LAUNCHED(ctx);
-      if ((rc = read_ctl(ctx, h, 67))) return rc;
-      // the slot-0 reduction of the last pass holds ||w||^2 (slot 32 of the partials)
-      for (int t = 0; t < k; t++) H[(size_t)t * m + i] = h.h_ctl[t] + h.h_ctl[33 + t];
-      double hn = std::sqrt(h.h_ctl[66]);
-      H[(size_t)(i + 1) * m + i] = hn;
-      if (hn != 0)
+      CD_CUDA(ctx, cudaMemcpyAsync(h.h_slot + (i & 1) * 80, h.d_ctl, sizeof(double) * 67, cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+      CD_CUDA(ctx, cudaEventRecord(h.ev_slot[i & 1], ctx->stream));
+      (void)cd_launch(scale_norm_kernel, blocks, 256, 0, ctx->stream, n, h.d_ctl + 66, h.d_w, V(i + 1));
+      CD_LAUNCHED(ctx);
+      return CDGPU_OK;
+    };
+    const double thr = std::max(p.res_norm_min, p.red_factor * res0);
+    double last = beta, rate = 0.5;
+    int i;
+    if ((rc = enqueue(0))) return rc;
+    for (i = 0; i < m && j <= maxite; i++, j++)
+    {
+      bool next_enqueued = false;
+      if (i + 1 < m && j + 1 <= maxite && (j < p.minit || last * rate > 4.0 * thr))
       {
-        (void)cd_launch(scale_kernel, blocks, 256, 0, ctx->stream, n, 1.0 / hn, h.d_w, V(i + 1));
-        CD_LAUNCHED(ctx);
+        if ((rc = enqueue(i + 1))) return rc;
+        next_enqueued = true;
       }
+      CD_CUDA(ctx, cudaEventSynchronize(h.ev_slot[i & 1]));
+      const double *c = h.h_slot + (i & 1) * 80;
+      const int k = i + 1;
+      // the slot-0 reduction of the last pass holds ||w||^2 (slot 32 of the partials)
+      for (int t = 0; t < k; t++) H[(size_t)t * m + i] = c[t] + c[33 + t];
+      double hn = std::sqrt(c[66]);
+      H[(size_t)(i + 1) * m + i] = hn;
       for (int t = 0; t < i; t++) app_rot(H[(size_t)t * m + i], H[(size_t)(t + 1) * m + i], cs[t], sn[t]);
       gen_rot(H[(size_t)i * m + i], H[(size_t)(i + 1) * m + i], cs[i], sn[i]);
       app_rot(H[(size_t)i * m + i], H[(size_t)(i + 1) * m + i], cs[i], sn[i]);
@@ -1096,6 +1132,10 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
         done = true;
         break;
       }
+      // convergence rate so far in this restart cycle, for the next prediction
+      if (beta > 0 && res > 0) rate = std::pow(res / beta, 1.0 / (i + 1));
+      last = res;
+      if (!next_enqueued && i + 1 < m && j + 1 <= maxite && (rc = enqueue(i + 1))) return rc;
     }
     if (done) break;
     // restart: x += Z y over the full basis, new residual (FgmresIte.C:536-560)
