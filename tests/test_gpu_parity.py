@@ -234,6 +234,40 @@ def test_structured_solve_vs_oracle(ctx, oracle_lib, dim, order, n0, L, disc, ep
     assert abs(i1.iterations - its1) <= 2
 
 
+@pytest.mark.parametrize("restart,minit", [(4, 0), (5, 9)])
+def test_fgmres_restart_cycles_vs_oracle(ctx, oracle_lib, restart, minit):
+    """FGMRES over several restart cycles (FgmresIte.C:536-560) and with a minimum iteration
+    count: the device-side Arnoldi vectors, the iterations enqueued ahead of the host's Givens
+    step and the restart update give the oracle's iterates, in FP64 and in the mixed form."""
+    co = coeffs(0, eps=1e-3, b=(1.0, 0.5), f=1.0)
+    dim, order, disc = 2, 1, 2
+    spaces, parents, sids, mg = structured_case(ctx, dim, order, 4, 4, co, disc)
+    levels = []
+    for l, (sp, sid) in enumerate(zip(spaces, sids)):
+        rp, kc = oracle_lib.pattern(sp["global_numbers"], sp["begin_index"], sp["n_dof"], sp["n_active"])
+        ent, rhs = oracle_lib.assemble(dim, order, disc, sp["coords"], sp["global_numbers"],
+                                       sp["begin_index"], sp["n_dof"], sp["n_active"], rp, kc,
+                                       oracle_coeffs(oracle_lib, co))
+        lv = dict(n_dof=sp["n_dof"], n_active=sp["n_active"], row_ptr=rp, kcol=kc, entries=ent)
+        if l > 0:
+            lv["p_row"], lv["p_col"], lv["p_val"] = oracle_lib.prolongation(
+                dim, order, spaces[l - 1], dict(sp), parents[l])
+        levels.append(lv)
+        ctx.assemble(sid, disc, sp["n_dof"], len(kc), want_entries=False)
+    sol0 = np.zeros(spaces[-1]["n_dof"])
+    tight = dict(red_factor=0.0, res_norm_min=1e-12 * np.linalg.norm(rhs), maxit=400, restart=restart,
+                 minit=minit)
+    x_o, its_o, _, _ = oracle_lib.solve(levels, oracle_lib.solver_params(**tight), rhs, sol0)
+    assert its_o > restart  # several restart cycles
+    x, info = ctx.solve(mg, solver_params(coarse_smoother=3, **tight), rhs, sol0)
+    assert info.status == 0
+    assert abs(info.iterations - its_o) <= 2
+    assert rel(x, x_o) <= TOL_SOL
+    xm, infom = ctx.solve(mg, solver_params(precision=1, **tight), rhs, sol0)
+    assert infom.status == 0
+    assert rel(xm, x_o) <= TOL_MIXED
+
+
 def test_spmv_and_defect_vs_oracle(ctx, oracle_lib):
     co = coeffs(0, eps=1e-2, b=(0.2, 0.3, 0.4))
     spaces, parents, sids, mg = structured_case(ctx, 3, 2, 6, 1, co, 1)
