@@ -213,7 +213,7 @@ def solve(levels, prm, rhs, sol0):
     return sol, its, hist[:max(its, 0) + 1], fres.value
 
 
-def tcd_step(levels, M, A, f_old, f, sol, tau, th1, th2, th3, th4, prm):
+def tcd_step(levels, M, A, f_old, f, sol, tau, th1, th2, th3, th4, prm, fine_only_theta2=False):
     """One theta-scheme step of TSystemTCD2D on the oracle's CSR levels.
 
     levels: as for :func:`solve` (their ``entries`` are replaced by the system matrices);
@@ -222,10 +222,15 @@ def tcd_step(levels, M, A, f_old, f, sol, tau, th1, th2, th3, th4, prm):
     src/System/SystemTCD2D.C:231-277 (AssembleSystMat), 323-330 (Solve with GMG) and
     279-305 (RestoreMassMat): MatAdd acts on the active rows only (Blas2.C MatAdd),
     B = tau*th3*f_old + tau*th4*f + M_active u_old, Dirichlet entries of B and u from f.
-    Returns (new solution, iterations)."""
+    fine_only_theta2: the order of TSystemTCD3D (src/System/SystemTCD3D.C:257-278), where
+    M - tau*th2*A is formed on the finest level only and the coarser levels' system matrices
+    are M + tau*th1*A.  Returns (new solution, iterations)."""
     fine = levels[-1]
     na = int(fine["n_active"])
-    for lv, m, a in zip(levels, M, A):
+    L = len(levels)
+    for l, (lv, m, a) in enumerate(zip(levels, M, A)):
+        if fine_only_theta2 and l < L - 1:
+            continue
         k = int(lv["row_ptr"][lv["n_active"]])
         m[:k] += (-tau * th2) * a[:k]
     B = np.zeros(len(f))
@@ -238,9 +243,9 @@ def tcd_step(levels, M, A, f_old, f, sol, tau, th1, th2, th3, th4, prm):
     u[na:] = f[na:]
     gamma = -tau * th2
     sys_levels = []
-    for lv, m, a in zip(levels, M, A):
+    for l, (lv, m, a) in enumerate(zip(levels, M, A)):
         k = int(lv["row_ptr"][lv["n_active"]])
-        m[:k] += (-gamma + tau * th1) * a[:k]
+        m[:k] += (tau * th1 if fine_only_theta2 and l < L - 1 else -gamma + tau * th1) * a[:k]
         d = dict(lv)
         d["entries"] = m.copy()
         sys_levels.append(d)

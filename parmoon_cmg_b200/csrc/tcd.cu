@@ -191,10 +191,13 @@ int cdgpu_tcd_step_device(cdgpu_ctx *ctx, int tcd_id, const cdgpu_solver_params 
   Hierarchy &h = *t->h;
   const int L = (int)h.lev.size();
   int rc;
-  // M <- M - tau theta2 A on every level (the coarse levels get the same system matrices)
-  for (int l = 0; l < L; l++)
-    if ((rc = matadd(ctx, *h.lev[l].sp, -tau * theta2, t->A[l], t->M[l]))) return rc;
   const Space &f = *h.lev[L - 1].sp;
+  // 2D (SystemTCD2D.C): M <- M - tau theta2 A on every level, so that the coarse levels get
+  // the finest level's sequence of updates; 3D (SystemTCD3D.C:257-278): on the finest level
+  // only, the coarser levels' system matrices are M + tau theta1 A
+  const bool fine_only = f.dim == 3;
+  for (int l = 0; l < L; l++)
+    if (!(fine_only && l < L - 1) && (rc = matadd(ctx, *h.lev[l].sp, -tau * theta2, t->A[l], t->M[l]))) return rc;
   (void)cd_launch(tcd_rhs_kernel, (f.n_dof + 255) / 256, 256, 0, ctx->stream, f.n_dof, f.n_active, f.d_row_ptr, f.d_kcol,
                                                                 t->M[L - 1], t->d_f_old, t->d_f, tau * theta3,
                                                                 tau * theta4, d_sol, t->d_B);
@@ -209,7 +212,8 @@ int cdgpu_tcd_step_device(cdgpu_ctx *ctx, int tcd_id, const cdgpu_solver_params 
   for (int l = 0; l < L; l++)
   {
     Space &s = *h.lev[l].sp;
-    if ((rc = matadd(ctx, s, -gamma + tau * theta1, t->A[l], t->M[l]))) return rc;
+    const double c = fine_only && l < L - 1 ? tau * theta1 : -gamma + tau * theta1;
+    if ((rc = matadd(ctx, s, c, t->A[l], t->M[l]))) return rc;
     s.mf_T = 0; // the system matrix is a combination, not one affine assembly
     (void)cd_launch(install_system_kernel, (s.n_dof + 255) / 256, 256, 0, ctx->stream, s.n_dof, s.d_row_ptr, s.d_kcol, t->M[l],
                                                                         s.d_a, s.d_a32, s.d_diag, s.d_diag32);

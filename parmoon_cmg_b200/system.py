@@ -295,6 +295,15 @@ class TSystemTCD2D:
         return info
 
 
+class TSystemTCD3D(TSystemTCD2D):
+    """Mirror of TSystemTCD3D (src/System/SystemTCD3D.C:176-330) for theta schemes on the GPU,
+    driven like 3DPrograms/TCD3D_ParMooN.C: AssembleMRhs, then per step the old right-hand
+    side saved, AssembleARhs, AssembleSystMat + Solve + RestoreMassMat (``Step``).  The device
+    path is the 2D one; for a 3D hierarchy it follows the 3D reference's order of the matrix
+    updates: M - tau*theta2*A on the finest level only, the coarser levels' system matrices
+    M + tau*theta1*A (SystemTCD3D.C:257-278)."""
+
+
 class TSystemCD2D(TSystemCD3D):
     """2D counterpart.  The reference's TSystemCD2D takes one space and has no multigrid
     branch (src/System/SystemCD2D.C:191-193); here it takes every level's space and

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from parmoon_cmg_b200 import _lib, mesh
-from parmoon_cmg_b200.system import Context, TSystemTCD2D, coeffs, solver_params
+from parmoon_cmg_b200.system import Context, TSystemTCD2D, TSystemTCD3D, coeffs, solver_params
 
 TOL_SOL = 1e-10
 MASS = 10
@@ -95,6 +95,49 @@ def test_tcd_steps_vs_oracle(oracle_lib, order, scheme):
             info = S.Step(sol, tau, *th, params=prm)
             assert info.status == 0
             u, its = oracle_lib.tcd_step(levels, M, A, f_old, f, u, tau, *th, prm_o)
+            assert its >= 0
+            assert np.abs(sol - u).max() <= TOL_SOL * np.abs(u).max()
+    finally:
+        ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order", [1, 2])
+def test_tcd3d_steps_vs_oracle(oracle_lib, order):
+    """TSystemTCD3D: Crank-Nicolson steps on a 3D hierarchy with the 3D reference's order of
+    the matrix updates (the oracle's tcd_step with fine_only_theta2) agree with the oracle
+    within the FP64 solution bar."""
+    from parmoon_cmg_b200 import _build
+    _build.build()
+    th, tau = (0.5, 0.5, 0.5, 0.5), 0.05
+    spaces, parents = mesh.structured_hierarchy(3, order, 2, 2)
+    ctx = Context(0)
+    try:
+        S = TSystemTCD3D(spaces, parents, ctx=ctx)
+        b = (0.57735026918962573,) * 3
+        co_steps = [coeffs(0, eps=0.05, b=b, c=0.1, f=1.0 + 0.5 * k) for k in range(4)]
+        S.Init(co_steps[0])
+        sol = np.zeros(spaces[-1]["n_dof"])
+        S.AssembleMRhs(sol)
+        levels = oracle_levels(oracle_lib, spaces, parents, 3, order)
+
+        def oco(c):
+            return oracle_lib.coeffs(0, eps=c.eps, b=(c.b1, c.b2, c.b3), c=c.c, f=c.f)
+
+        M, f = oracle_forms(oracle_lib, spaces, levels, 3, order, MASS, oco(co_steps[0]))
+        assert np.abs(S.rhs() - f).max() <= 1e-12 * np.abs(f).max()
+        u = sol.copy()
+        prm_o = oracle_lib.solver_params(red_factor=1e-13, restart=32, maxit=200)
+        prm = solver_params(coarse_smoother=3, red_factor=1e-13, restart=32, maxit=200)
+        for k in range(1, 4):
+            for sid in S.sids:
+                ctx.set_coeffs(sid, co_steps[k])
+            f_old = f
+            S.AssembleARhs()
+            A, f = oracle_forms(oracle_lib, spaces, levels, 3, order, 1, oco(co_steps[k]))
+            info = S.Step(sol, tau, *th, params=prm)
+            assert info.status == 0
+            u, its = oracle_lib.tcd_step(levels, M, A, f_old, f, u, tau, *th, prm_o, fine_only_theta2=True)
             assert its >= 0
             assert np.abs(sol - u).max() <= TOL_SOL * np.abs(u).max()
     finally:
