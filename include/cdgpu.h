@@ -140,6 +140,15 @@ int cdgpu_set_coeffs(cdgpu_ctx *ctx, int space_id, const cdgpu_coeffs *coeffs,
  * CDGPU_COEFF_TABLE must be evaluated; *n_quad receives the points per cell. */
 int cdgpu_quadrature_points(cdgpu_ctx *ctx, int space_id, double *h_xyz, int *n_quad);
 
+/* --- error evaluation ---------------------------------------------------------
+ * Replaces TFEFunction2D::GetErrors (src/FE/FEFunction2D.C:73) for the exact solution of
+ * the SineLaplace example, u = sin(pi x) sin(pi y) (Examples/CD_2D/SineLaplace.h:27-30):
+ * *l2 = ||u_h - u||_L2, *h1semi = |u_h - u|_H1 with the assembly's Gauss rule on every cell,
+ * computed on the device.  h_sol: the full solution vector (n_dof values).  Only 2D spaces
+ * whose coefficients are of kind CDGPU_COEFF_SINE have this exact solution; others return
+ * CDGPU_ERR_UNSUPPORTED. */
+int cdgpu_errors(cdgpu_ctx *ctx, int space_id, const double *h_sol, double *l2, double *h1semi);
+
 /* --- assembly ---------------------------------------------------------------
  * Replaces TSystemCD3D::Assemble / TAssembleMat3D::Reset + Assemble3D
  * (src/System/SystemCD3D.C:314-339, src/System/AssembleMat3D.C:230-505) and

@@ -64,6 +64,7 @@ SIGNATURES = {
     "cdgpu_add_neumann": (_I, [_P, _I, _I, _P, _P, _P, _P]),
     "cdgpu_spmv": (_I, [_P, _I, _P, _P]),
     "cdgpu_defect": (_I, [_P, _I, _P, _P, _P, C.POINTER(C.c_double)]),
+    "cdgpu_errors": (_I, [_P, _I, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "cdgpu_spmv_device": (_I, [_P, _I, _P, _P]),
     "cdgpu_defect_noalloc": (_I, [_P, _I, _P, _P, _P, C.POINTER(C.c_double)]),
     "cdgpu_hierarchy": (_I, [_P, _I, _P, _P, C.POINTER(_I)]),

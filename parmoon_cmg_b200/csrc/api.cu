@@ -386,6 +386,21 @@ int cdgpu_spmv(cdgpu_ctx *ctx, int space_id, const double *h_x, double *h_y)
   return rc;
 }
 
+int cdgpu_errors(cdgpu_ctx *ctx, int space_id, const double *h_sol, double *l2, double *h1semi)
+{
+  Space *s = get_space(ctx, space_id);
+  if (!s || !h_sol || !l2 || !h1semi) return fail(ctx, CDGPU_ERR_INVALID, "errors: bad argument");
+  cudaSetDevice(ctx->device);
+  double *du = nullptr;
+  int rc;
+  if ((rc = dev_alloc(ctx, &du, s->n_dof))) return rc;
+  cudaError_t e = cudaMemcpyAsync(du, h_sol, sizeof(double) * s->n_dof, cudaMemcpyHostToDevice, ctx->stream);
+  rc = e == cudaSuccess ? space_errors_sine(ctx, *s, du, l2, h1semi) : cuda_fail(ctx, e, "errors: copy");
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(du);
+  return rc;
+}
+
 int cdgpu_defect(cdgpu_ctx *ctx, int space_id, const double *h_x, const double *h_f, double *h_d, double *res)
 {
   Space *s = get_space(ctx, space_id);

@@ -87,6 +87,56 @@ __device__ __forceinline__ double d_invert(int dim, const double *J, double *Ji)
   return det;
 }
 
+// reference -> physical map of a quadrilateral / hexahedron at xi: x and J[r*dim + b] =
+// dx_r/dxi_b; affine cells from three (four) vertices, others multilinear
+// (TQuadAffin / TQuadBilinear::GetOrigFromRef, src/FE/QuadAffin.C, src/FE/QuadBilinear.C, and
+// their hexahedron counterparts)
+__device__ __forceinline__ void d_ref_map(int dim, int nv, bool affine, const double *V, const double *xi,
+                                          double *x, double *J)
+{
+  for (int k = 0; k < 3; k++) x[k] = 0.0;
+  for (int k = 0; k < 9; k++) J[k] = 0.0;
+  if (affine)
+  {
+    for (int r = 0; r < dim; r++)
+    {
+      double c1 = (V[1 * dim + r] - V[r]) * 0.5, c2 = (V[3 * dim + r] - V[r]) * 0.5;
+      if (dim == 2)
+      {
+        x[r] = (V[1 * dim + r] + V[3 * dim + r]) * 0.5 + c1 * xi[0] + c2 * xi[1];
+        J[r * 2] = c1; J[r * 2 + 1] = c2;
+      }
+      else
+      {
+        double c3 = (V[4 * dim + r] - V[r]) * 0.5;
+        x[r] = (V[1 * dim + r] + V[3 * dim + r] + V[4 * dim + r] - V[r]) * 0.5 + c1 * xi[0] +
+               c2 * xi[1] + c3 * xi[2];
+        J[r * 3] = c1; J[r * 3 + 1] = c2; J[r * 3 + 2] = c3;
+      }
+    }
+  }
+  else
+  {
+    const double r2[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
+    for (int v = 0; v < nv; v++)
+    {
+      double rv[3];
+      if (dim == 2) { rv[0] = r2[v][0]; rv[1] = r2[v][1]; }
+      else { rv[0] = r2[v & 3][0]; rv[1] = r2[v & 3][1]; rv[2] = v < 4 ? -1.0 : 1.0; }
+      double f[3], N = 1;
+      for (int b = 0; b < dim; b++) { f[b] = 0.5 * (1 + rv[b] * xi[b]); N *= f[b]; }
+      for (int b = 0; b < dim; b++)
+      {
+        double dN = 0.5 * rv[b];
+        for (int e = 0; e < dim; e++)
+          if (e != b) dN *= f[e];
+        for (int r = 0; r < dim; r++) J[r * dim + b] += dN * V[v * dim + r];
+      }
+      for (int r = 0; r < dim; r++) x[r] += N * V[v * dim + r];
+    }
+  }
+}
+
 __device__ __forceinline__ double d_diameter(int dim, const double *V)
 {
   double best = 0;
@@ -233,47 +283,8 @@ __global__ void local_quad_kernel(LocalArgs a)
   for (int q = threadIdx.x; q < nq; q += blockDim.x)
   {
     const double *xi = a.qx + q * dim;
-    double x[3] = {0, 0, 0}, J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Ji[9];
-    bool affine = a.affine_all;
-    if (affine)
-    {
-      for (int r = 0; r < dim; r++)
-      {
-        double c1 = (V[1 * dim + r] - V[r]) * 0.5, c2 = (V[3 * dim + r] - V[r]) * 0.5;
-        if (dim == 2)
-        {
-          x[r] = (V[1 * dim + r] + V[3 * dim + r]) * 0.5 + c1 * xi[0] + c2 * xi[1];
-          J[r * 2] = c1; J[r * 2 + 1] = c2;
-        }
-        else
-        {
-          double c3 = (V[4 * dim + r] - V[r]) * 0.5;
-          x[r] = (V[1 * dim + r] + V[3 * dim + r] + V[4 * dim + r] - V[r]) * 0.5 + c1 * xi[0] +
-                 c2 * xi[1] + c3 * xi[2];
-          J[r * 3] = c1; J[r * 3 + 1] = c2; J[r * 3 + 2] = c3;
-        }
-      }
-    }
-    else
-    {
-      const double r2[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
-      for (int v = 0; v < a.nv; v++)
-      {
-        double rv[3];
-        if (dim == 2) { rv[0] = r2[v][0]; rv[1] = r2[v][1]; }
-        else { rv[0] = r2[v & 3][0]; rv[1] = r2[v & 3][1]; rv[2] = v < 4 ? -1.0 : 1.0; }
-        double f[3], N = 1;
-        for (int b = 0; b < dim; b++) { f[b] = 0.5 * (1 + rv[b] * xi[b]); N *= f[b]; }
-        for (int b = 0; b < dim; b++)
-        {
-          double dN = 0.5 * rv[b];
-          for (int e = 0; e < dim; e++)
-            if (e != b) dN *= f[e];
-          for (int r = 0; r < dim; r++) J[r * dim + b] += dN * V[v * dim + r];
-        }
-        for (int r = 0; r < dim; r++) x[r] += N * V[v * dim + r];
-      }
-    }
+    double x[3], J[9], Ji[9];
+    d_ref_map(dim, a.nv, a.affine_all, V, xi, x, J);
     double det = d_invert(dim, J, Ji);
     mult[q] = a.qw[q] * fabs(det);
     for (int k = 0; k < dim * dim; k++) Jis[q * dim * dim + k] = Ji[k];
@@ -606,6 +617,117 @@ int assemble_check(cdgpu_ctx *ctx)
   return CDGPU_OK;
 }
 
+// the assembly's quadrature rule and basis tables on the device: qx, qw, phi, dphi, hphi
+static int ensure_quadtab(cdgpu_ctx *ctx, Space &s)
+{
+  if (s.d_quadtab) return CDGPU_OK;
+  const RefElement &re = s.re;
+  std::vector<double> packed;
+  packed.insert(packed.end(), re.qx.begin(), re.qx.end());
+  packed.insert(packed.end(), re.qw.begin(), re.qw.end());
+  packed.insert(packed.end(), re.phi.begin(), re.phi.end());
+  packed.insert(packed.end(), re.dphi.begin(), re.dphi.end());
+  packed.insert(packed.end(), re.hphi.begin(), re.hphi.end());
+  int rc = dev_alloc(ctx, &s.d_quadtab, packed.size());
+  if (rc) return rc;
+  CD_CUDA(ctx, cudaMemcpy(s.d_quadtab, packed.data(), packed.size() * sizeof(double), cudaMemcpyHostToDevice));
+  return CDGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// L2 and H1-semi errors of a 2D solution against the SineLaplace solution
+// u = sin(pi x) sin(pi y) (Examples/CD_2D/SineLaplace.h:27-30), as TFEFunction2D::GetErrors
+// (src/FE/FEFunction2D.C:73) computes them: the assembly's Gauss rule on every cell, the
+// squared errors summed per thread over its cells, per block in a fixed tree, and the block
+// partials on the host in block order.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) errors_sine_kernel(int n_cells, int nbf, int nq, int nv, int affine_all,
+                                                          const double *__restrict__ coords,
+                                                          const int *__restrict__ gn, const double *__restrict__ qx,
+                                                          const double *__restrict__ qw,
+                                                          const double *__restrict__ phi,
+                                                          const double *__restrict__ dphi,
+                                                          const double *__restrict__ u, double *__restrict__ partial)
+{
+  CD_PDL_ENTRY();
+  __shared__ double red[2][8];
+  double e0 = 0.0, e1 = 0.0;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cells; c += gridDim.x * blockDim.x)
+  {
+    double V[8];
+    for (int k = 0; k < nv * 2; k++) V[k] = coords[(size_t)c * nv * 2 + k];
+    for (int q = 0; q < nq; q++)
+    {
+      double x[3], J[9], Ji[9];
+      d_ref_map(2, nv, affine_all != 0, V, qx + 2 * q, x, J);
+      const double det = d_invert(2, J, Ji);
+      double uh = 0.0, ux = 0.0, uy = 0.0;
+      for (int b = 0; b < nbf; b++)
+      {
+        const double *gr = dphi + (size_t)(q * nbf + b) * 2;
+        const double gx = Ji[0] * gr[0] + Ji[2] * gr[1], gy = Ji[1] * gr[0] + Ji[3] * gr[1];
+        const double ub = u[gn[(size_t)c * nbf + b]];
+        uh += ub * phi[q * nbf + b];
+        ux += ub * gx;
+        uy += ub * gy;
+      }
+      const double ex = sin(M_PI * x[0]) * sin(M_PI * x[1]);
+      const double exx = M_PI * cos(M_PI * x[0]) * sin(M_PI * x[1]);
+      const double exy = M_PI * sin(M_PI * x[0]) * cos(M_PI * x[1]);
+      const double w = qw[q] * fabs(det);
+      e0 += w * (uh - ex) * (uh - ex);
+      e1 += w * ((ux - exx) * (ux - exx) + (uy - exy) * (uy - exy));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1)
+  {
+    e0 += __shfl_xor_sync(0xffffffffu, e0, o);
+    e1 += __shfl_xor_sync(0xffffffffu, e1, o);
+  }
+  if (threadIdx.x % 32 == 0)
+  {
+    red[0][threadIdx.x / 32] = e0;
+    red[1][threadIdx.x / 32] = e1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < 8; w++) { a += red[0][w]; b += red[1][w]; }
+    partial[2 * blockIdx.x] = a;
+    partial[2 * blockIdx.x + 1] = b;
+  }
+}
+
+int space_errors_sine(cdgpu_ctx *ctx, Space &s, const double *d_u, double *l2, double *h1semi)
+{
+  if (s.dim != 2 || !s.co_set || s.co.kind != CDGPU_COEFF_SINE)
+    return fail(ctx, CDGPU_ERR_UNSUPPORTED, "errors: only 2D spaces with the sine coefficients (SineLaplace) have an exact solution");
+  int rc;
+  if ((rc = ensure_quadtab(ctx, s))) return rc;
+  const RefElement &re = s.re;
+  const double *qx = s.d_quadtab, *qw = qx + re.qx.size(), *phi = qw + re.qw.size(), *dphi = phi + re.phi.size();
+  const int grid = std::max(1, std::min((s.n_cells + 255) / 256, ctx->sm_count * 4));
+  double *d_partial = nullptr;
+  if ((rc = dev_alloc(ctx, &d_partial, (size_t)2 * grid))) return rc;
+  (void)cd_launch(errors_sine_kernel, grid, 256, 0, ctx->stream, s.n_cells, s.nbf, re.nq, s.nv,
+                  s.all_affine ? 1 : 0, (const double *)s.d_coords, (const int *)s.d_gn, qx, qw, phi, dphi, d_u,
+                  d_partial);
+  cudaError_t e = cudaGetLastError();
+  std::vector<double> part((size_t)2 * grid);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(part.data(), d_partial, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d_partial);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "errors");
+  CD_LAUNCHED(ctx);
+  double a = 0.0, b = 0.0;
+  for (int i = 0; i < grid; i++) { a += part[2 * i]; b += part[2 * i + 1]; }
+  *l2 = std::sqrt(a);
+  *h1semi = std::sqrt(b);
+  return CDGPU_OK;
+}
+
 int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, bool check)
 {
   if (s.nnz < 0) return fail(ctx, CDGPU_ERR_INVALID, "assemble: no pattern (call cdgpu_build_pattern)");
@@ -676,17 +798,7 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, 
   }
   else
   {
-    if (!s.d_quadtab)
-    {
-      std::vector<double> packed;
-      packed.insert(packed.end(), re.qx.begin(), re.qx.end());
-      packed.insert(packed.end(), re.qw.begin(), re.qw.end());
-      packed.insert(packed.end(), re.phi.begin(), re.phi.end());
-      packed.insert(packed.end(), re.dphi.begin(), re.dphi.end());
-      packed.insert(packed.end(), re.hphi.begin(), re.hphi.end());
-      if ((rc = dev_alloc(ctx, &s.d_quadtab, packed.size()))) return rc;
-      CD_CUDA(ctx, cudaMemcpy(s.d_quadtab, packed.data(), packed.size() * sizeof(double), cudaMemcpyHostToDevice));
-    }
+    if ((rc = ensure_quadtab(ctx, s))) return rc;
     const double *d_tab = nullptr;
     if (s.co.kind == CDGPU_COEFF_TABLE)
     {

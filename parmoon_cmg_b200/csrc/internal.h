@@ -248,6 +248,8 @@ bool dense_inverse(int n, std::vector<double> &a); // in place, row-major; false
 // device entry points (assemble.cu / solve.cu)
 // assemble one space; with check = false the error flag is left for assemble_check
 int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, bool check = true);
+// L2 and H1-semi errors against the SineLaplace solution (2D, coefficient kind SINE)
+int space_errors_sine(cdgpu_ctx *ctx, Space &s, const double *d_u, double *l2, double *h1semi);
 int assemble_check(cdgpu_ctx *ctx);
 int add_neumann(cdgpu_ctx *ctx, Space &s, int n_edges, const int *cell, const int *edge,
                 const double *g);

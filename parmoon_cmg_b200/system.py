@@ -109,6 +109,12 @@ class Context:
         self.check(self.lib.cdgpu_assemble(self.h, sid, disctype, _p(d), _p(ent), _p(rhs)))
         return ent, rhs
 
+    def errors(self, sid, sol):
+        """(L2, H1-semi) errors of ``sol`` against the SineLaplace solution, on the device."""
+        l2, h1 = C.c_double(), C.c_double()
+        self.check(self.lib.cdgpu_errors(self.h, sid, _p(_f64(sol)), C.byref(l2), C.byref(h1)))
+        return l2.value, h1.value
+
     def add_neumann(self, sid, cells, edges, g, n_dof=None):
         """Add Neumann data; returns the updated right-hand side when n_dof is given."""
         cells, edges, g = _i32(cells), _i32(edges), _f64(g)

@@ -127,6 +127,18 @@ def test_sine_known_answer_gpu(ctx, oracle_lib):
     sol, info = ctx.solve(mg, prm, rhs, sol0)
     e = oracle_lib.errors_sine(1, fin["coords"], fin["global_numbers"], fin["begin_index"], sol)
     assert f"{e[0]:.6e}" == "4.751079e-04" and f"{e[1]:.6e}" == "6.295197e-02"
+    # the same errors evaluated on the device (GetErrors)
+    g = ctx.errors(sids[-1], sol)
+    assert f"{g[0]:.6e}" == "4.751079e-04" and f"{g[1]:.6e}" == "6.295197e-02"
+    assert abs(g[0] - e[0]) <= 1e-12 * e[0] and abs(g[1] - e[1]) <= 1e-12 * e[1]
+    # no exact solution for other coefficient kinds
+    sp3 = mesh.structured_space(3, 1, 2)
+    sid3 = ctx.upload_space(sp3)
+    ctx.build_pattern(sid3)
+    ctx.set_coeffs(sid3, coeffs(0, eps=1.0))
+    with pytest.raises(_lib.CdgpuError) as err:
+        ctx.errors(sid3, np.zeros(sp3["n_dof"]))
+    assert err.value.status == _lib.ERR_UNSUPPORTED
 
 
 def structured_case(ctx, dim, order, n_coarse, n_levels, co, disc):
