@@ -210,7 +210,11 @@ int cdgpu_solve_device(cdgpu_ctx *ctx, int mg_id, const cdgpu_solver_params *par
 /* assemble every level of a hierarchy, as TSystemCD3D::Assemble loops over all levels
  * (src/System/SystemCD3D.C:314-339).  disctype is used on the finest level,
  * coarse_disctype on the others (the reference uses one DISCTYPE for all levels; a SUPG
- * coarse-grid operator under a Galerkin fine level only changes the preconditioner). */
+ * coarse-grid operator under a Galerkin fine level only changes the preconditioner).
+ * The device-side checks of an assembly (every cell coupling present in the pattern, rows
+ * within the kernel's length) depend on the pattern only, so the call waits for the device
+ * and reports them on the first assembly of each level's pattern; later calls return as
+ * soon as the work is enqueued on the library's stream. */
 int cdgpu_assemble_hierarchy(cdgpu_ctx *ctx, int mg_id, int disctype, int coarse_disctype);
 /* device pointer of the assembled right-hand side of a space */
 int cdgpu_rhs_device(cdgpu_ctx *ctx, int space_id, double **d_rhs);

@@ -220,6 +220,7 @@ static int install_pattern(cdgpu_ctx *ctx, Space &s)
   s.shape = csr_shape(s.h_row_ptr.data(), s.n_dof);
   // a new pattern invalidates values sized for the old one and the slot map
   s.slot_pattern = -1;
+  s.pattern_checked = false;
   void **vals[] = {(void **)&s.d_a, (void **)&s.d_a32};
   for (void **p : vals)
     if (*p) { cudaFree(*p); *p = nullptr; }
@@ -504,13 +505,19 @@ int cdgpu_assemble_hierarchy(cdgpu_ctx *ctx, int mg_id, int disctype, int coarse
   Hierarchy *h = get_mg(ctx, mg_id);
   if (!h) return fail(ctx, CDGPU_ERR_INVALID, "assemble_hierarchy: bad id");
   cudaSetDevice(ctx->device);
+  bool need_check = false;
   for (size_t l = 0; l < h->lev.size(); l++)
   {
     int d = l + 1 == h->lev.size() ? disctype : coarse_disctype;
     int rc = assemble_space(ctx, *h->lev[l].sp, d, nullptr, false);
     if (rc) return rc;
+    need_check = need_check || !h->lev[l].sp->pattern_checked;
   }
-  return assemble_check(ctx);
+  if (!need_check) return CDGPU_OK; // the checks depend on the patterns only
+  int rc = assemble_check(ctx);
+  if (!rc)
+    for (auto &L : h->lev) L.sp->pattern_checked = true;
+  return rc;
 }
 
 int cdgpu_solve_device(cdgpu_ctx *ctx, int mg_id, const cdgpu_solver_params *p, const double *d_rhs, double *d_sol,

@@ -606,9 +606,16 @@ int assemble_check(cdgpu_ctx *ctx)
 {
   CD_CUDA(ctx, cudaMemcpyAsync(ctx->h_err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return err_flag_status(ctx);
+}
+
+// the status of the error flag already copied to ctx->h_err (the flag is cleared when set)
+int err_flag_status(cdgpu_ctx *ctx)
+{
   int e = *ctx->h_err;
   if (e)
   {
+    *ctx->h_err = 0;
     CD_CUDA(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
     if (e == 1) return fail(ctx, CDGPU_ERR_PATTERN, "assemble: a cell coupling is missing from the CSR pattern");
     if (e == 3) return fail(ctx, CDGPU_ERR_CUDA, "multigrid: a tensor-core product did not complete in time");

@@ -68,6 +68,7 @@ struct Space
   // from the pattern on the first assembly
   unsigned char *d_slot = nullptr;
   long slot_pattern = -1; // nnz of the pattern the slot map was built for
+  bool pattern_checked = false; // an assembly with this pattern passed the device-side checks
   // values
   double *d_a = nullptr, *d_rhs = nullptr, *d_diag = nullptr;
   float *d_a32 = nullptr, *d_diag32 = nullptr;
@@ -251,6 +252,7 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, 
 // L2 and H1-semi errors against the SineLaplace solution (2D, coefficient kind SINE)
 int space_errors_sine(cdgpu_ctx *ctx, Space &s, const double *d_u, double *l2, double *h1semi);
 int assemble_check(cdgpu_ctx *ctx);
+int err_flag_status(cdgpu_ctx *ctx);
 int add_neumann(cdgpu_ctx *ctx, Space &s, int n_edges, const int *cell, const int *edge,
                 const double *g);
 int spmv64(cdgpu_ctx *ctx, const Space &s, const double *x, double *y);

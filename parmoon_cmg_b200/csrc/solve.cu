@@ -1158,6 +1158,8 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
     ret = j > maxite ? maxite : j;
     if (res > p.res_norm_min && res > res0 * p.red_factor) status = CDGPU_ERR_NOT_CONVERGED;
   }
+  if (ctx->d_err && ctx->h_err)
+    CD_CUDA(ctx, cudaMemcpyAsync(ctx->h_err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   info->iterations = ret;
   info->final_residual = res;
@@ -1280,6 +1282,8 @@ int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const 
       return fail(ctx, CDGPU_ERR_INVALID, "exact coarse solve: singular coarse matrix");
     }
   }
-  if (rc == CDGPU_OK && p.precision == 1 && h.mf_mask) rc = assemble_check(ctx); // tensor-core wait flag
+  // tensor-core wait flag: FGMRES copied it back with its last synchronisation
+  if (rc == CDGPU_OK && p.precision == 1 && h.mf_mask)
+    rc = p.solver == 16 && ctx->h_err ? err_flag_status(ctx) : assemble_check(ctx);
   return rc;
 }
