@@ -216,6 +216,10 @@ int cdgpu_solve_device(cdgpu_ctx *ctx, int mg_id, const cdgpu_solver_params *par
  * and reports them on the first assembly of each level's pattern; later calls return as
  * soon as the work is enqueued on the library's stream. */
 int cdgpu_assemble_hierarchy(cdgpu_ctx *ctx, int mg_id, int disctype, int coarse_disctype);
+/* copy of a space's assembled right-hand side (n_dof values), the rhs array that
+ * TSystemCD3D::Assemble leaves on the host (src/System/SystemCD3D.C:314-339); waits for the
+ * device */
+int cdgpu_get_rhs(cdgpu_ctx *ctx, int space_id, double *h_rhs);
 /* device pointer of the assembled right-hand side of a space */
 int cdgpu_rhs_device(cdgpu_ctx *ctx, int space_id, double **d_rhs);
 

@@ -71,6 +71,7 @@ SIGNATURES = {
     "cdgpu_solve": (_I, [_P, _I, C.POINTER(SolverParams), _P, _P, C.POINTER(SolveInfo)]),
     "cdgpu_solve_device": (_I, [_P, _I, C.POINTER(SolverParams), _P, _P, C.POINTER(SolveInfo)]),
     "cdgpu_assemble_hierarchy": (_I, [_P, _I, _I, _I]),
+    "cdgpu_get_rhs": (_I, [_P, _I, _P]),
     "cdgpu_rhs_device": (_I, [_P, _I, C.POINTER(C.c_void_p)]),
     "cdgpu_tcd_create": (_I, [_P, _I, _I, C.POINTER(_I)]),
     "cdgpu_tcd_assemble_mass": (_I, [_P, _I]),

@@ -359,6 +359,16 @@ int cdgpu_rhs_device(cdgpu_ctx *ctx, int space_id, double **d_rhs)
   return CDGPU_OK;
 }
 
+int cdgpu_get_rhs(cdgpu_ctx *ctx, int space_id, double *h_rhs)
+{
+  Space *s = get_space(ctx, space_id);
+  if (!s || !h_rhs || !s->assembled) return fail(ctx, CDGPU_ERR_INVALID, "get_rhs: not assembled");
+  cudaSetDevice(ctx->device);
+  CD_CUDA(ctx, cudaMemcpyAsync(h_rhs, s->d_rhs, sizeof(double) * s->n_dof, cudaMemcpyDeviceToHost, ctx->stream));
+  CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CDGPU_OK;
+}
+
 int cdgpu_spmv_device(cdgpu_ctx *ctx, int space_id, const double *d_x, double *d_y)
 {
   Space *s = get_space(ctx, space_id);

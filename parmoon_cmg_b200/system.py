@@ -31,6 +31,12 @@ def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
+def _is_f64_out(a, n):
+    """a can receive n float64 values in place (a writable C-contiguous float64 ndarray)"""
+    return (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous and
+            a.flags.writeable and a.size == n)
+
+
 class Context:
     """One libcdgpu context (device + CUDA stream)."""
 
@@ -224,6 +230,17 @@ class TSystemCD3D:
     def Assemble(self, sol=None, rhs=None, dirichlet=None, entries=False):
         """Assemble all levels (SystemCD3D.C:314-339); returns the finest (entries, rhs) and
         copies the Dirichlet part of rhs into sol like SystemCD3D.C:330."""
+        if dirichlet is None and not entries:
+            # every level in one call; the finest rhs is copied straight into ``rhs`` when it
+            # is a contiguous float64 array
+            self.ctx.assemble_hierarchy(self.mg, self.disctype, self.coarse_disctype)
+            r = rhs if _is_f64_out(rhs, self.N_DOF) else np.zeros(self.N_DOF)
+            self.ctx.check(self.ctx.lib.cdgpu_get_rhs(self.ctx.h, self.sids[-1], _p(r)))
+            if rhs is not None and r is not rhs:
+                rhs[:] = r
+            if sol is not None:
+                sol[self.N_Active:] = r[self.N_Active:]
+            return None, r
         out = None
         for i, sid in enumerate(self.sids):
             sp = self.spaces[i]
@@ -243,8 +260,14 @@ class TSystemCD3D:
     def Solve(self, sol, rhs, params=None):
         """FGMRES / fixed point with one multigrid cycle as preconditioner (SystemCD3D.C:342-368)."""
         params = params or solver_params()
-        x, info = self.ctx.solve(self.mg, params, rhs, sol)
-        sol[:] = x
+        if _is_f64_out(sol, self.N_DOF):
+            # the library reads the initial guess from and writes the solution into ``sol``
+            info = SolveInfo()
+            self.ctx.check(self.ctx.lib.cdgpu_solve(self.ctx.h, self.mg, C.byref(params), _p(_f64(rhs)),
+                                                    _p(sol), C.byref(info)))
+        else:
+            x, info = self.ctx.solve(self.mg, params, rhs, sol)
+            sol[:] = x
         if info.status == _lib.ERR_DIVERGED:
             raise CdgpuError(info.status, "fgmres iteration diverges")
         return info

@@ -13,7 +13,7 @@ from conftest import golden, golden_names
 import refdump
 
 from parmoon_cmg_b200 import _lib, mesh
-from parmoon_cmg_b200.system import Context, coeffs, solver_params
+from parmoon_cmg_b200.system import Context, TSystemCD2D, TSystemCD3D, coeffs, solver_params
 
 pytestmark = pytest.mark.gpu
 
@@ -278,6 +278,34 @@ def test_fgmres_restart_cycles_vs_oracle(ctx, oracle_lib, restart, minit):
     xm, infom = ctx.solve(mg, solver_params(precision=1, **tight), rhs, sol0)
     assert infom.status == 0
     assert rel(xm, x_o) <= TOL_MIXED
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_facade_assemble_and_solve(ctx, dim):
+    """The TSystemCD3D / TSystemCD2D mirror: Assemble over the whole hierarchy in one call
+    (rhs copied straight into the caller's array) gives the per-level assembly's rhs, and
+    Solve in place into the caller's array gives the same solution as the copying path."""
+    order, n0, L = (1, 4, 3) if dim == 2 else (2, 2, 2)
+    spaces, parents = mesh.structured_hierarchy(dim, order, n0, L)
+    b = (1.0, 0.5) if dim == 2 else (0.57735026918962573,) * 3
+    cls = TSystemCD2D if dim == 2 else TSystemCD3D
+    S = cls(spaces, parents, ctx=ctx)
+    S.Init(coeffs(0, eps=1e-1, b=b, f=1.0))
+    n = S.N_DOF
+    sol, rhs = np.zeros(n), np.zeros(n)
+    _, r = S.Assemble(sol, rhs)
+    assert r is rhs
+    ent2, r2 = S.Assemble(entries=True)          # per-level path with a copy of the entries
+    assert np.array_equal(rhs, r2) and ent2 is not None
+    prm = solver_params(precision=1, red_factor=1e-10)
+    sol_a = np.zeros(n)
+    sol_a[S.N_Active:] = rhs[S.N_Active:]
+    sol_b = np.zeros(2 * n)[::2]                 # not contiguous: the copying path
+    sol_b[S.N_Active:] = rhs[S.N_Active:]
+    ia = S.Solve(sol_a, rhs, prm)
+    ib = S.Solve(sol_b, rhs, prm)
+    assert ia.status == 0 and ib.status == 0 and ia.iterations == ib.iterations
+    assert np.array_equal(sol_a, sol_b)
 
 
 def test_spmv_and_defect_vs_oracle(ctx, oracle_lib):
