@@ -654,6 +654,68 @@ void cdo_errors_sine(int order, int n_cells, const double *coords, const int *gn
   err2[1] = sqrt(e1);
 }
 
+/* L2 and H1-semi errors against u = amp sin(k pi x) sin(k pi y) (2D): the TCD2D example exp.h
+ * (Examples/TCD_2D/exp.h:31-41, amp = exp(t), k = 2) through TFEFunction2D::GetErrors
+ * (src/FE/FEFunction2D.C:73) with the assembly's Gauss rule, as cdo_errors_sine */
+void cdo_errors_sinsin(int order, int n_cells, const double *coords, const int *gn, const int *bi,
+                       const double *u, double k, double amp, double *err2)
+{
+  int nbf = cdo_nbf(2, order);
+  double qx[2 * MAXQ], qw[MAXQ];
+  int nq = cdo_quadrature(2, cdo_gauss_points(order), qx, qw);
+  double e0 = 0, e1 = 0;
+  for (int c = 0; c < n_cells; c++)
+  {
+    const double *V = coords + (size_t)c * 8;
+    int affine = cell_is_affine(2, V);
+    const int *dof = gn + bi[c];
+    for (int q = 0; q < nq; q++)
+    {
+      double x[2], J[4], Ji[4], val[MAXBF], gr[MAXBF * 2];
+      ref_map(2, affine, V, qx + 2 * q, x, J);
+      double det = inv(2, J, Ji);
+      cdo_basis(2, order, qx + 2 * q, val, gr, NULL);
+      double uh = 0, ux = 0, uy = 0;
+      for (int b = 0; b < nbf; b++)
+      {
+        double gx = Ji[0] * gr[2 * b] + Ji[2] * gr[2 * b + 1];
+        double gy = Ji[1] * gr[2 * b] + Ji[3] * gr[2 * b + 1];
+        uh += u[dof[b]] * val[b];
+        ux += u[dof[b]] * gx;
+        uy += u[dof[b]] * gy;
+      }
+      double sx = sin(k * M_PI * x[0]), sy = sin(k * M_PI * x[1]);
+      double ex = amp * sx * sy;
+      double exx = amp * k * M_PI * cos(k * M_PI * x[0]) * sy;
+      double exy = amp * k * M_PI * sx * cos(k * M_PI * x[1]);
+      double w = qw[q] * fabs(det);
+      e0 += w * (uh - ex) * (uh - ex);
+      e1 += w * ((ux - exx) * (ux - exx) + (uy - exy) * (uy - exy));
+    }
+  }
+  err2[0] = sqrt(e0);
+  err2[1] = sqrt(e1);
+}
+
+/* physical quadrature points of every cell (n_cells x n_quad x dim), in the order the
+ * assembly reads a CDGPU_COEFF_TABLE (kind 3) */
+void cdo_quad_points(int dim, int order, int n_cells, const double *coords, double *xyz)
+{
+  double qx[3 * MAXQ], qw[MAXQ];
+  int nq = cdo_quadrature(dim, cdo_gauss_points(order), qx, qw), nv = nverts(dim);
+  for (int c = 0; c < n_cells; c++)
+  {
+    const double *V = coords + (size_t)c * nv * dim;
+    int affine = cell_is_affine(dim, V);
+    for (int q = 0; q < nq; q++)
+    {
+      double x[3], J[9];
+      ref_map(dim, affine, V, qx + dim * q, x, J);
+      for (int a = 0; a < dim; a++) xyz[((size_t)c * nq + q) * dim + a] = x[a];
+    }
+  }
+}
+
 /* physical coordinates of every DOF (any cell containing it gives the same point) */
 void cdo_dof_coords(int dim, int order, int n_cells, const double *coords, const int *gn,
                     const int *bi, int n_dof, double *xyz)

@@ -87,6 +87,8 @@ def _declare(L):
                                _P, _P, C.POINTER(Coeffs), _P, _P, _P, _P]
     L.cdo_neumann_sine.argtypes = [C.c_int, C.c_int, _P, _P, _P, C.c_int, C.c_double, _P]
     L.cdo_errors_sine.argtypes = [C.c_int, C.c_int, _P, _P, _P, _P, _P]
+    L.cdo_errors_sinsin.argtypes = [C.c_int, C.c_int, _P, _P, _P, _P, C.c_double, C.c_double, _P]
+    L.cdo_quad_points.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P]
     L.cdo_dof_coords.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P, _P, C.c_int, _P]
     L.cdo_prolongation.restype = C.c_long
     L.cdo_prolongation.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P, _P, C.c_int, C.c_int, _P,
@@ -145,6 +147,28 @@ def errors_sine(order, coords, gn, bi, u):
     out = np.zeros(2)
     lib().cdo_errors_sine(order, len(bi) - 1, _p(coords), _p(gn), _p(bi), _p(u), _p(out))
     return out
+
+
+def errors_sinsin(order, coords, gn, bi, u, k, amp):
+    """L2 and H1-semi errors of a 2D solution against amp*sin(k pi x)*sin(k pi y)."""
+    coords, gn, bi, u = _f64(coords), _i32(gn), _i32(bi), _f64(u)
+    out = np.zeros(2)
+    lib().cdo_errors_sinsin(order, len(bi) - 1, _p(coords), _p(gn), _p(bi), _p(u), k, amp, _p(out))
+    return out
+
+
+def quad_points(dim, order, coords, n_cells):
+    """Physical quadrature points (n_cells x n_quad x dim) in the oracle's table order."""
+    coords = _f64(coords)
+    nq = cdo_nq(dim, order)
+    out = np.zeros((n_cells, nq, dim))
+    lib().cdo_quad_points(dim, order, n_cells, _p(coords), _p(out))
+    return out
+
+
+def cdo_nq(dim, order):
+    n1 = 3 if order == 1 else 4
+    return n1 ** dim
 
 
 def dof_coords(dim, order, coords, gn, bi, n_dof):

@@ -145,6 +145,46 @@ def test_tcd3d_steps_vs_oracle(oracle_lib, order):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_tcd2d_known_answer_gpu(oracle_lib, precision):
+    """ReadIn/tcd2d.out:485-543 on the GPU: TSystemTCD2D with the exp.h coefficients evaluated
+    at the library's quadrature points every step (CDGPU_COEFF_TABLE), 32x32 Q1,
+    Crank-Nicolson, tau 0.05: the reference's printed L2 and H1-semi errors after each of 10
+    steps, in the FP64 and in the mixed form."""
+    import tcd_exp
+    from parmoon_cmg_b200 import _build
+    _build.build()
+    spaces, parents = mesh.structured_hierarchy(2, 1, 4, 4)
+    fin = spaces[-1]
+    ctx = Context(0)
+    try:
+        S = TSystemTCD2D(spaces, parents, ctx=ctx)
+
+        def set_time(t):
+            for sid, sp in zip(S.sids, spaces):
+                xq = ctx.quadrature_points(sid, len(sp["begin_index"]) - 1, 2)
+                ctx.set_coeffs(sid, coeffs(_lib.COEFF_TABLE), tcd_exp.coeff_table(xq, t))
+
+        xyz = oracle_lib.dof_coords(2, 1, fin["coords"], fin["global_numbers"], fin["begin_index"], fin["n_dof"])
+        sol = tcd_exp.initial(xyz)
+        set_time(0.0)
+        S.AssembleMRhs(sol)
+        prm = solver_params(precision=precision, coarse_smoother=3, red_factor=0.0, res_norm_min=1e-13,
+                            maxit=300)
+        for k in range(1, len(tcd_exp.KNOWN)):
+            t = tcd_exp.KNOWN[k][0]
+            set_time(t)
+            S.AssembleARhs()
+            info = S.Step(sol, tcd_exp.TAU, *tcd_exp.THETA, params=prm)
+            assert info.status == 0
+            e = oracle_lib.errors_sinsin(1, fin["coords"], fin["global_numbers"], fin["begin_index"], sol,
+                                         2.0, np.exp(t))
+            assert tcd_exp.fmt(e) == tcd_exp.KNOWN[k][1:], t
+    finally:
+        ctx.close()
+
+
+@pytest.mark.gpu
 def test_tcd_rejects_bad_use():
     from parmoon_cmg_b200 import _build
     _build.build()

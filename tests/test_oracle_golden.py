@@ -108,6 +108,52 @@ def test_sine_known_answer(oracle_lib):
     assert f"{float(d['err_h1']):.6e}" == "6.295197e-02"
 
 
+def test_tcd2d_known_answer(oracle_lib):
+    """ReadIn/tcd2d.out:485-543: the oracle's theta-scheme step (oracle.tcd_step, the
+    restatement of SystemTCD2D.C:154-210) on exp.h, 32x32 Q1, Crank-Nicolson, tau 0.05, gives
+    the reference's printed L2 and H1-semi errors at t = 0 and after each of 10 steps."""
+    import tcd_exp
+    from parmoon_cmg_b200 import mesh
+    spaces, parents = mesh.structured_hierarchy(2, 1, 4, 4)
+    fin = spaces[-1]
+    assert (fin["n_dof"], fin["n_active"]) == (1089, 961)
+    levels = []
+    for l, sp in enumerate(spaces):
+        rp, kc = oracle_lib.pattern(sp["global_numbers"], sp["begin_index"], sp["n_dof"], sp["n_active"])
+        lv = dict(n_dof=sp["n_dof"], n_active=sp["n_active"], row_ptr=rp, kcol=kc)
+        if l > 0:
+            lv["p_row"], lv["p_col"], lv["p_val"] = oracle_lib.prolongation(2, 1, spaces[l - 1], dict(sp), parents[l])
+        levels.append(lv)
+    co = oracle_lib.coeffs(3)
+
+    def forms(disc, t):
+        out, r = [], None
+        for sp, lv in zip(spaces, levels):
+            xq = oracle_lib.quad_points(2, 1, sp["coords"], len(sp["begin_index"]) - 1)
+            e, r = oracle_lib.assemble(2, 1, disc, sp["coords"], sp["global_numbers"], sp["begin_index"],
+                                       sp["n_dof"], sp["n_active"], lv["row_ptr"], lv["kcol"], co,
+                                       coeff_tab=tcd_exp.coeff_table(xq, t))
+            out.append(e)
+        return out, r
+
+    def errors(u, t):
+        return tcd_exp.fmt(oracle_lib.errors_sinsin(1, fin["coords"], fin["global_numbers"],
+                                                    fin["begin_index"], u, 2.0, np.exp(t)))
+
+    M, f = forms(10, 0.0)
+    xyz = oracle_lib.dof_coords(2, 1, fin["coords"], fin["global_numbers"], fin["begin_index"], fin["n_dof"])
+    u = tcd_exp.initial(xyz)
+    assert errors(u, 0.0) == tcd_exp.KNOWN[0][1:]
+    prm = oracle_lib.solver_params(red_factor=0.0, res_norm_min=1e-13, maxit=300)
+    for k in range(1, len(tcd_exp.KNOWN)):
+        t = tcd_exp.KNOWN[k][0]
+        A, fnew = forms(1, t)
+        u, its = oracle_lib.tcd_step(levels, M, A, f, fnew, u, tcd_exp.TAU, *tcd_exp.THETA, prm)
+        assert its > 0
+        f = fnew
+        assert errors(u, t) == tcd_exp.KNOWN[k][1:], t
+
+
 def test_mg_preconditioner_matches_reference(oracle_lib):
     """One multigrid application equals the reference's (cd3d dump 'prec_rhs')."""
     d = golden("cd3d_q1_gal_4")
