@@ -22,8 +22,9 @@ def default_params():
 
 
 class Server:
-    def __init__(self, ctx, budget_bytes, params=None, iterations_per_round=4):
-        self.batch = Batch(params or default_params(), ctx)
+    def __init__(self, ctx, budget_bytes, params=None, iterations_per_round=4, batch=None):
+        # batch: an existing Batch (or an object with its methods) instead of a new one
+        self.batch = batch if batch is not None else Batch(params or default_params(), ctx)
         self.cache = StructureCache(self.batch)
         self.budget = budget_bytes
         self.k = iterations_per_round
