@@ -5,7 +5,7 @@ log-uniform in [16, 256], Q1 or Q2 with equal probability, eps log-uniform in [1
 convection angle uniform in [0, 2 pi) with |b| = 1, f = 1, Dirichlet 0.  The multigrid
 hierarchy of an N x N mesh has L = floor(log2(N / 2)) + 1 levels on a coarsest mesh of
 n0 = round(N / 2^(L-1)) in {2, 3, 4} cells per side (a small exact coarse solve), so N is
-rounded to n0 * 2^(L-1) (within 15 %); the rounded N is recorded with every instance.
+rounded to n0 * 2^(L-1) (within 20 %); the rounded N is recorded with every instance.
 
 ``serving_stream``: Poisson arrivals of CD2D/CD3D requests (70 % 2D, 30 % 3D, Q1/Q2 50/50),
 DOF counts log-uniform in [1e3, 2e6] mapped to the nearest admissible N, eps log-uniform in
