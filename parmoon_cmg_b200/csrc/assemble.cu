@@ -585,12 +585,19 @@ static int launch_gather(cdgpu_ctx *ctx, const GatherArgs &g, int n_dof)
 {
   int groups = 256 / GS;
   size_t sm = (size_t)groups * MAXROW * sizeof(double);
-  CD_CUDA(ctx, cudaFuncSetAttribute(row_gather_kernel<GS, MAXROW>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const void *key = (const void *)row_gather_kernel<GS, MAXROW>;
   int blocks_per_sm = 0;
-  CD_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm,
-                                                             row_gather_kernel<GS, MAXROW>, 256, sm));
-  if (blocks_per_sm < 1) blocks_per_sm = 1;
+  for (auto &e : ctx->occupancy)
+    if (e.first == key) blocks_per_sm = e.second;
+  if (!blocks_per_sm)
+  {
+    CD_CUDA(ctx, cudaFuncSetAttribute(row_gather_kernel<GS, MAXROW>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    CD_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm,
+                                                               row_gather_kernel<GS, MAXROW>, 256, sm));
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+    ctx->occupancy.push_back({key, blocks_per_sm});
+  }
   long need = (n_dof + groups - 1) / groups;
   long grid = std::min<long>(need, (long)ctx->sm_count * blocks_per_sm);
   if (grid < 1) grid = 1;

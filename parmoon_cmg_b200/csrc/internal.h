@@ -169,6 +169,9 @@ struct cdgpu_ctx
   long long launches = 0;
   std::vector<Space *> spaces;
   std::vector<Hierarchy *> mgs;
+  // resident CTAs per SM of kernels launched with a dynamic shared-memory attribute, found
+  // once per context (the attribute is set at the same time)
+  std::vector<std::pair<const void *, int>> occupancy;
   // set while the multigrid cycle is recorded into its graph: its kernels load the data that
   // no kernel of the cycle writes before waiting for their predecessor
   bool pdl_pre = false;
