@@ -59,6 +59,28 @@ def test_oracle_backward_euler_reaches_steady_state(oracle_lib):
         assert np.abs(m - m0).max() <= 1e-12 * np.abs(m0).max()
 
 
+def test_oracle_backward_euler_reaches_steady_state_3d(oracle_lib):
+    """The 3D order of the updates (fine_only_theta2, SystemTCD3D.C:257-278) keeps the
+    property: implicit Euler with long steps converges to the stationary solution, and
+    RestoreMassMat brings every level's M back up to rounding."""
+    spaces, parents = mesh.structured_hierarchy(3, 1, 2, 2)
+    levels = oracle_levels(oracle_lib, spaces, parents, 3, 1)
+    co = oracle_lib.coeffs(0, eps=0.1, b=(1.0, 0.5, 0.25), f=1.0)
+    M, fm = oracle_forms(oracle_lib, spaces, levels, 3, 1, MASS, co)
+    A, f = oracle_forms(oracle_lib, spaces, levels, 3, 1, 1, co)
+    prm = oracle_lib.solver_params(red_factor=1e-13, restart=32, maxit=200)
+    M0 = [m.copy() for m in M]
+    u = np.zeros(spaces[-1]["n_dof"])
+    for _ in range(12):
+        u, its = oracle_lib.tcd_step(levels, M, A, f, f, u, 1e3, 1.0, 0.0, 0.0, 1.0, prm, fine_only_theta2=True)
+        assert its >= 0
+    steady = [dict(lv, entries=a) for lv, a in zip(levels, A)]
+    us, _, _, _ = oracle_lib.solve(steady, prm, f, np.zeros_like(f))
+    assert np.abs(u - us).max() <= 1e-8 * np.abs(us).max()
+    for m, m0 in zip(M, M0):
+        assert np.abs(m - m0).max() <= 1e-12 * np.abs(m0).max()
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("order,scheme", [(1, "crank_nicolson"), (2, "backward_euler")])
 def test_tcd_steps_vs_oracle(oracle_lib, order, scheme):
