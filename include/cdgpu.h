@@ -231,7 +231,10 @@ int cdgpu_rhs_device(cdgpu_ctx *ctx, int space_id, double **d_rhs);
  * the reference's, so every step rounds like the reference.  The solve is the multigrid
  * FGMRES of cdgpu_solve on the system matrices M + tau*theta1*A of every level.
  * cdgpu_tcd_assemble_stiffness first saves the current right-hand side as the old one
- * (the time loop's memcpy(oldrhs, rhs)).  Galerkin forms only. */
+ * (the time loop's memcpy(oldrhs, rhs)).  Galerkin forms only.  On a 3D hierarchy the
+ * steps follow TSystemTCD3D (src/System/SystemTCD3D.C:228-305, 3DPrograms/TCD3D_ParMooN.C):
+ * M - tau*theta2*A is formed on the finest level only and the coarser levels' system
+ * matrices are M + tau*theta1*A. */
 int cdgpu_tcd_create(cdgpu_ctx *ctx, int mg_id, int disctype, int *tcd_id);
 int cdgpu_tcd_assemble_mass(cdgpu_ctx *ctx, int tcd_id);
 int cdgpu_tcd_assemble_stiffness(cdgpu_ctx *ctx, int tcd_id);
