@@ -175,14 +175,24 @@ int cdgpu_spmv(cdgpu_ctx *ctx, int space_id, const double *h_x, double *h_y);
 int cdgpu_defect(cdgpu_ctx *ctx, int space_id, const double *h_x, const double *h_f, double *h_d,
                  double *res);
 int cdgpu_spmv_device(cdgpu_ctx *ctx, int space_id, const double *d_x, double *d_y);
+/* y = A x with an FP32 form of the assembled operator, the forms the mixed multigrid cycle
+ * applies (TMGLevel3D's MatVect/Defect on the FP32 levels, src/FE/MGLevel3D.C:194-252):
+ * form 0 the FP32 copy of the CSR entries; 1 the matrix-free per-cell products
+ * A_c x_c = sum_t coef_{c,t} R_t x_c on CUDA cores; 2 the same products on the tensor cores
+ * (tcgen05, TF32 inputs, FP32 accumulation).  Dirichlet rows are identity rows.  Forms 1 and 2
+ * need Q2 hexahedra assembled from affine cells with constant coefficients
+ * (CDGPU_ERR_UNSUPPORTED otherwise).  h_x, h_y: host arrays of n_dof floats. */
+int cdgpu_apply_fp32(cdgpu_ctx *ctx, int space_id, int form, const float *h_x, float *h_y);
 /* The defect d = f - A x and *h_res = ||d||, like cdgpu_defect, for callers that cannot
  * allocate device memory (for example while another allocator holds the whole device, or
  * where the device synchronisation of cudaFree is not acceptable).  No counterpart in the
  * reference.  d_x, d_f, d_d: device vectors of the space's length; h_res: host (nullable).
  * Allocates nothing: the partial sums live in a fixed 32 KB array of the library, so at most
- * 8,388,608 rows (CDGPU_ERR_UNSUPPORTED beyond).  The first call on a device looks up that
- * array's address and should come before any stream capture; calls that overlap on the GPU
- * share the array and race. */
+ * 8,388,608 rows (CDGPU_ERR_UNSUPPORTED beyond).  cdgpu_create looks up that array's address
+ * on its device (which, under lazy module loading, also loads it), so create the context
+ * before another allocator takes the device; if that lookup failed, the first call repeats it
+ * and should then come before any stream capture.  Calls that overlap on the GPU share the
+ * array and race. */
 int cdgpu_defect_noalloc(cdgpu_ctx *ctx, int space_id, const double *d_x, const double *d_f,
                          double *d_d, double *h_res);
 
@@ -245,6 +255,11 @@ int cdgpu_tcd_step_device(cdgpu_ctx *ctx, int tcd_id, const cdgpu_solver_params 
                           double theta1, double theta2, double theta3, double theta4, double *d_sol,
                           cdgpu_solve_info *info);
 int cdgpu_tcd_rhs(cdgpu_ctx *ctx, int tcd_id, double *h_rhs);
+/* copies (nnz values of level `level`, 0 = coarsest; each pointer nullable) of the mass matrix
+ * M as updated in place by the steps, the stiffness matrix A, and the system matrix the last
+ * step solved with: the sqmatrixM / sqmatrixA members of TSystemTCD2D / TSystemTCD3D
+ * (include/System/SystemTCD2D.h, SystemTCD3D.h) after RestoreMassMat. */
+int cdgpu_tcd_matrices(cdgpu_ctx *ctx, int tcd_id, int level, double *h_M, double *h_A, double *h_S);
 
 /* --- batched solves and serving ---------------------------------------------
  * No single reference function: the reference solves one system per process

@@ -492,11 +492,18 @@ int cdo_assemble(int dim, int order, int disctype, int n_cells, const double *co
         lap[b] = 0;
         if (dim == 2 && disctype == 2)
         {
-          /* physical second derivatives of an affine map: D2 = Ji^T H Ji */
+          /* physical second derivatives D2 = Ji^T (H - G) Ji.  G is zero for an affine map; for
+             the bilinear map x = c0 + c1 xi + c2 eta + c3 xi eta its off-diagonal entries are
+             grad(phi) . c3, the term the D11 row of the reference's 5x5 system carries
+             (xc3, yc3 in src/FE/QuadBilinear.C:531-549) */
+          double gm = 0;
+          if (!affine)
+            for (int a = 0; a < 2; a++)
+              gm += g[b][a] * 0.25 * (V[0 * 2 + a] - V[1 * 2 + a] + V[2 * 2 + a] - V[3 * 2 + a]);
           for (int a = 0; a < 2; a++)
             for (int e = 0; e < 2; e++)
               for (int f = 0; f < 2; f++)
-                lap[b] += Ji[e * 2 + a] * Ji[f * 2 + a] * hphi[q][b * 4 + e * 2 + f];
+                lap[b] += Ji[e * 2 + a] * Ji[f * 2 + a] * (hphi[q][b * 4 + e * 2 + f] - (e != f ? gm : 0.0));
         }
       }
       coeff_at(co, coeff_tab ? coeff_tab + ((size_t)c * nq + q) * 6 : NULL, x, k);

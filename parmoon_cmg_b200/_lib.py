@@ -66,6 +66,7 @@ SIGNATURES = {
     "cdgpu_defect": (_I, [_P, _I, _P, _P, _P, C.POINTER(C.c_double)]),
     "cdgpu_errors": (_I, [_P, _I, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "cdgpu_spmv_device": (_I, [_P, _I, _P, _P]),
+    "cdgpu_apply_fp32": (_I, [_P, _I, _I, _P, _P]),
     "cdgpu_defect_noalloc": (_I, [_P, _I, _P, _P, _P, C.POINTER(C.c_double)]),
     "cdgpu_hierarchy": (_I, [_P, _I, _P, _P, C.POINTER(_I)]),
     "cdgpu_solve": (_I, [_P, _I, C.POINTER(SolverParams), _P, _P, C.POINTER(SolveInfo)]),
@@ -81,6 +82,7 @@ SIGNATURES = {
     "cdgpu_tcd_step_device": (_I, [_P, _I, C.POINTER(SolverParams), C.c_double, C.c_double,
                                    C.c_double, C.c_double, C.c_double, _P, C.POINTER(SolveInfo)]),
     "cdgpu_tcd_rhs": (_I, [_P, _I, _P]),
+    "cdgpu_tcd_matrices": (_I, [_P, _I, _I, _P, _P, _P]),
     "cdgpu_batch_create": (_I, [_P, C.POINTER(SolverParams), C.POINTER(_I)]),
     "cdgpu_batch_submit": (_I, [_P, _I, _I, C.POINTER(Coeffs), _I, _I, C.POINTER(_I)]),
     "cdgpu_batch_advance": (_I, [_P, _I, _I, C.POINTER(_I)]),

@@ -89,6 +89,7 @@ int cdgpu_create(cdgpu_ctx **out, int device)
     delete ctx;
     return CDGPU_ERR_CUDA;
   }
+  noalloc_prepare(device);
   *out = ctx;
   return CDGPU_OK;
 }
@@ -392,6 +393,33 @@ int cdgpu_spmv(cdgpu_ctx *ctx, int space_id, const double *h_x, double *h_y)
     CD_CUDA(ctx, cudaMemcpyAsync(h_y, dy, sizeof(double) * s->n_dof, cudaMemcpyDeviceToHost, ctx->stream));
     CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
+  cudaFree(dx);
+  cudaFree(dy);
+  return rc;
+}
+
+int cdgpu_apply_fp32(cdgpu_ctx *ctx, int space_id, int form, const float *h_x, float *h_y)
+{
+  Space *s = get_space(ctx, space_id);
+  if (!s || !s->assembled || !h_x || !h_y || form < 0 || form > 2)
+    return fail(ctx, CDGPU_ERR_INVALID, "apply_fp32: bad argument");
+  cudaSetDevice(ctx->device);
+  float *dx = nullptr, *dy = nullptr;
+  int rc;
+  if ((rc = dev_alloc(ctx, &dx, s->n_dof)) || (rc = dev_alloc(ctx, &dy, s->n_dof)))
+  {
+    if (dx) cudaFree(dx);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpyAsync(dx, h_x, sizeof(float) * s->n_dof, cudaMemcpyHostToDevice, ctx->stream);
+  rc = e == cudaSuccess ? apply_fp32_form(ctx, *s, form, dx, dy) : cuda_fail(ctx, e, "apply_fp32: copy");
+  if (!rc)
+  {
+    e = cudaMemcpyAsync(h_y, dy, sizeof(float) * s->n_dof, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "apply_fp32: copy back");
+  }
+  cudaStreamSynchronize(ctx->stream);
   cudaFree(dx);
   cudaFree(dy);
   return rc;

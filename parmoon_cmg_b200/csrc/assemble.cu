@@ -311,10 +311,18 @@ __global__ void local_quad_kernel(LocalArgs a)
     double l = 0;
     if (dim == 2 && a.disctype == CDGPU_SUPG)
     {
+      // physical second derivatives Ji^T (H - G) Ji: on a bilinear cell
+      // x = c0 + c1 xi + c2 eta + c3 xi eta the mixed reference derivative also carries
+      // grad(phi) . c3 (the D11 row of the 5x5 system of QuadBilinear::GetOrigValues,
+      // src/FE/QuadBilinear.C:531-549); an affine map has c3 = 0
       const double *hp = a.hphi + (size_t)(q * nbf + b) * 4;
+      double gm = 0;
+      if (!a.affine_all)
+        for (int r = 0; r < 2; r++)
+          gm += g[(q * nbf + b) * dim + r] * 0.25 * (V[r] - V[2 + r] + V[4 + r] - V[6 + r]);
       for (int r = 0; r < 2; r++)
         for (int e = 0; e < 2; e++)
-          for (int f = 0; f < 2; f++) l += Ji[e * 2 + r] * Ji[f * 2 + r] * hp[e * 2 + f];
+          for (int f = 0; f < 2; f++) l += Ji[e * 2 + r] * Ji[f * 2 + r] * (hp[e * 2 + f] - (e != f ? gm : 0.0));
     }
     lap[q * nbf + b] = l;
   }

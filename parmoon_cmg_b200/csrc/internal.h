@@ -264,3 +264,6 @@ int defect64(cdgpu_ctx *ctx, const Space &s, const double *x, const double *f, d
 int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m);
 int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *d_rhs,
               double *d_sol, cdgpu_solve_info *info);
+int apply_fp32_form(cdgpu_ctx *ctx, Space &s, int form, const float *d_x, float *d_y);
+// looks up the allocation-free defect's scratch array on a device (noalloc.cu)
+void noalloc_prepare(int device);

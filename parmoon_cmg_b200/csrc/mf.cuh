@@ -146,6 +146,19 @@ __device__ __forceinline__ uint64_t mf_sdesc(uint32_t addr, uint32_t lbo_bytes, 
   return d;
 }
 
+// poll the mbarrier for completion of the given phase at most `limit` times; 1 when it completed
+__device__ __forceinline__ uint32_t mf_wait_parity(uint64_t *mbar, uint32_t phase, long limit)
+{
+  uint32_t done = 0;
+  for (long it = 0; it < limit && !done; it++)
+    asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                 "selp.b32 %0, 1, 0, P1;\n\t}"
+                 : "=r"(done)
+                 : "r"(mf_smem_u32(mbar)), "r"(phase)
+                 : "memory");
+  return done;
+}
+
 template <int T>
 __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const int *__restrict__ gn,
                                                               const float *__restrict__ cf32,
@@ -203,8 +216,8 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
   const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(NH >> 3) << 17) | ((uint32_t)(MT >> 4) << 24);
-  uint32_t phase = 0;
-  bool ok = true;
+  uint32_t phase = 0, pend_phase = 0;
+  bool ok = true, pending = false;
   prefetch_x();
   for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
   {
@@ -238,19 +251,16 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
     }
     prefetch_idx(tile + gridDim.x);
     prefetch_x();
-    // bounded wait for this tile's products (an error flag instead of a hang)
-    uint32_t done = 0;
-    if (ok)
-      for (long it = 0; it < (1L << 24) && !done; it++)
-        asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-                     "selp.b32 %0, 1, 0, P1;\n\t}"
-                     : "=r"(done)
-                     : "r"(mf_smem_u32(&mbar)), "r"(phase)
-                     : "memory");
-    if (!done)
+    // bounded wait for this tile's products (an error flag instead of a hang); the outcome is
+    // made CTA-uniform, so the warp-collective TMEM loads below run with every lane or none
+    const uint32_t done = ok ? mf_wait_parity(&mbar, phase, 1L << 24) : 0u;
+    const int all_done = __syncthreads_and(done != 0);
+    if (ok && !all_done)
     {
-      if (ok && lane == 0) atomicExch(err, 3);
+      if (tid == 0) atomicExch(err, 3);
       ok = false;
+      pending = true; // the committed products may still write TMEM
+      pend_phase = phase;
     }
     phase ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -287,13 +297,20 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
   }
+  // after a timed-out wait, wait once more (bounded) for the products still in flight before
+  // the accumulator columns are released
+  if (pending)
+  {
+    const uint32_t late = tid == 0 ? mf_wait_parity(&mbar, pend_phase, 1L << 26) : 1u;
+    __syncthreads_or(late == 0);
+  }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
 }
 
 template <int T> inline size_t mf_tc_smem() { return (size_t)128 * 32 * 4 + (size_t)32 * T * 32 * 4; }
 
-enum { MF_JACOBI = 0, MF_DEFECT = 1 };
+enum { MF_JACOBI = 0, MF_DEFECT = 1, MF_SPMV = 2 };
 
 template <int NBF, int MODE>
 __global__ void mf_row_kernel(int n, int na, int n_cells, const int *__restrict__ inc_ptr,
@@ -317,7 +334,8 @@ __global__ void mf_row_kernel(int n, int na, int n_cells, const int *__restrict_
   CD_PDL_ENTRY();
   if (r >= na)
   {
-    out[r] = MODE == MF_JACOBI ? f[r] : f[r] - x[r];
+    // Dirichlet rows are identity rows
+    out[r] = MODE == MF_JACOBI ? f[r] : MODE == MF_DEFECT ? f[r] - x[r] : x[r];
     return;
   }
   if (!pre) load_inc();
@@ -337,7 +355,7 @@ __global__ void mf_row_kernel(int n, int na, int n_cells, const int *__restrict_
     const int K = inc[t] / NBF, li = inc[t] - K * NBF;
     s += ybuf[(size_t)li * n_cells + K];
   }
-  out[r] = MODE == MF_JACOBI ? x[r] + omega * (f[r] - s) / diag[r] : f[r] - s;
+  out[r] = MODE == MF_JACOBI ? x[r] + omega * (f[r] - s) / diag[r] : MODE == MF_DEFECT ? f[r] - s : s;
 }
 
 // FP32 copies of the cell coefficients (first T of each cell's T + Tr) and of the tensors
@@ -373,10 +391,10 @@ inline bool use_mf(const Space &s)
          mf_shape_ok(s.nbf, s.mf_T);
 }
 
-// y = A x per cell (phase 1)
-inline void mf_apply_cells(cdgpu_ctx *ctx, const Space &s, const float *x)
+// y = A x per cell (phase 1); tensor_cores = false keeps Q2 hexahedra on the CUDA-core kernel
+inline void mf_apply_cells(cdgpu_ctx *ctx, const Space &s, const float *x, bool tensor_cores = true)
 {
-  if (s.nbf == 27 && ctx->d_err)
+  if (s.nbf == 27 && ctx->d_err && tensor_cores)
   {
     // tensor cores: persistent CTAs, one per SM (the shared memory request keeps a second CTA
     // off the SM, so every CTA can allocate its 512 TMEM columns at once)

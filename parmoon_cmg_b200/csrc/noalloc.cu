@@ -13,9 +13,12 @@
 // call writes every slot it reads, so nothing has to start at zero.  Calls that overlap on
 // the GPU (two streams, two host threads, two contexts on one device) race on the array.
 //
-// Set-up: the first call on a device looks up the array's device address with
-// cudaGetSymbolAddress, with that device current; later calls reuse it.  That first call
-// should come before any stream capture.
+// Set-up: cdgpu_create looks up the array's device address with cudaGetSymbolAddress, with the
+// context's device current, once per device (noalloc_prepare below); under lazy module loading
+// that lookup is what loads this file's kernels and the array, so it happens while the context
+// is made, before another allocator can have taken the device.  Should that lookup have failed,
+// the entry point's first call on the device repeats it; that call should then come before any
+// stream capture.
 #include <mutex>
 
 #include "internal.h"
@@ -93,6 +96,30 @@ __global__ void noalloc_total_kernel(int nblocks, double *__restrict__ partial)
   }
 }
 
+// the device address of the scratch array on `device` (the current device), looked up once
+static cudaError_t noalloc_scratch(int device, double **out)
+{
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_ptr[device])
+  {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_defect_scratch);
+    if (e != cudaSuccess) return e;
+    g_scratch_ptr[device] = (double *)p;
+  }
+  *out = g_scratch_ptr[device];
+  return cudaSuccess;
+}
+
+// called by cdgpu_create with the context's device current; a failure is left for the entry
+// point to report
+void noalloc_prepare(int device)
+{
+  if (device < 0 || device >= kMaxDevices) return;
+  double *p = nullptr;
+  if (noalloc_scratch(device, &p) != cudaSuccess) cudaGetLastError();
+}
+
 extern "C" int cdgpu_defect_noalloc(cdgpu_ctx *ctx, int space_id, const double *d_x, const double *d_f,
                                     double *d_d, double *h_res)
 {
@@ -107,18 +134,14 @@ extern "C" int cdgpu_defect_noalloc(cdgpu_ctx *ctx, int space_id, const double *
   if (ctx->device < 0 || ctx->device >= kMaxDevices)
     return fail(ctx, CDGPU_ERR_UNSUPPORTED, "defect_noalloc: device index beyond 63");
   CD_CUDA(ctx, cudaSetDevice(ctx->device));
-  double *scratch;
+  if (s.n_dof <= 0)
   {
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[ctx->device])
-    {
-      void *p = nullptr;
-      cudaError_t e = cudaGetSymbolAddress(&p, g_defect_scratch);
-      if (e != cudaSuccess) return cuda_fail(ctx, e, "defect_noalloc: cudaGetSymbolAddress");
-      g_scratch_ptr[ctx->device] = (double *)p;
-    }
-    scratch = g_scratch_ptr[ctx->device];
+    if (h_res) *h_res = 0.0;
+    return CDGPU_OK; // no rows: nothing to launch
   }
+  double *scratch = nullptr;
+  cudaError_t e = noalloc_scratch(ctx->device, &scratch);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "defect_noalloc: cudaGetSymbolAddress");
   const int blocks = (s.n_dof + kRowsPerBlock - 1) / kRowsPerBlock;
   if (s.dim == 3 && s.order == 2)
     defect_noalloc_kernel<32><<<blocks, kThreads, 0, ctx->stream>>>(s.n_dof, s.d_row_ptr, s.d_kcol, s.d_a, d_x,

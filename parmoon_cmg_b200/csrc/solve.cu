@@ -1201,6 +1201,40 @@ static int fixed_point(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &
   return CDGPU_OK;
 }
 
+// FP32 cell coefficients and tensors of a space's matrix-free operator, made from its last
+// assembly, plus the tensor-core kernel's shared-memory attribute and the error flag (all set
+// outside any capture)
+static int prepare_mf(cdgpu_ctx *ctx, Space &s)
+{
+  int rc;
+  if (!s.d_ybuf)
+  {
+    if ((rc = dev_alloc(ctx, &s.d_cf32, (size_t)s.n_cells * CD_MAXT)) ||
+        (rc = dev_alloc(ctx, &s.d_R32, (size_t)CD_MAXT * s.nbf * s.nbf)) ||
+        (rc = dev_alloc(ctx, &s.d_ybuf, (size_t)s.nbf * s.n_cells)))
+      return rc;
+  }
+  if (s.mf_version != s.assembly_version)
+  {
+    const int T = s.mf_T, Tr = n_rhs_tensors(s.dim, s.ref_disctype);
+    const long total = (long)s.n_cells * T + (long)T * s.nbf * s.nbf;
+    const int grid = (int)std::min<long>((total + 255) / 256, (long)ctx->sm_count * 8);
+    (void)cd_launch(mf_convert_kernel, grid, 256, 0, ctx->stream, s.n_cells, T, Tr, s.nbf, s.d_cellcoef, s.d_ref,
+                    s.d_cf32, s.d_R32);
+    CD_LAUNCHED(ctx);
+    s.mf_version = s.assembly_version;
+  }
+  CD_CUDA(ctx, cudaFuncSetAttribute(mf_cell27_tc_kernel<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
+  CD_CUDA(ctx, cudaFuncSetAttribute(mf_cell27_tc_kernel<13>, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
+  if (!ctx->d_err)
+  {
+    if ((rc = dev_alloc(ctx, &ctx->d_err, 1))) return rc;
+    CD_CUDA(ctx, cudaMallocHost((void **)&ctx->h_err, sizeof(int)));
+    CD_CUDA(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+  }
+  return CDGPU_OK;
+}
+
 // FP32 copies for the matrix-free operator of every level that has one; the captured FP32
 // cycle is recaptured when the set of such levels changes
 static int refresh_mf(cdgpu_ctx *ctx, Hierarchy &h)
@@ -1210,38 +1244,9 @@ static int refresh_mf(cdgpu_ctx *ctx, Hierarchy &h)
   {
     Space &s = *h.lev[l].sp;
     if (s.mf_T <= 0 || s.n_cells < kMfMinCells || !mf_shape_ok(s.nbf, s.mf_T)) continue;
-    int rc;
-    if (!s.d_ybuf)
-    {
-      if ((rc = dev_alloc(ctx, &s.d_cf32, (size_t)s.n_cells * CD_MAXT)) ||
-          (rc = dev_alloc(ctx, &s.d_R32, (size_t)CD_MAXT * s.nbf * s.nbf)) ||
-          (rc = dev_alloc(ctx, &s.d_ybuf, (size_t)s.nbf * s.n_cells)))
-        return rc;
-    }
-    if (s.mf_version != s.assembly_version)
-    {
-      const int T = s.mf_T, Tr = n_rhs_tensors(s.dim, s.ref_disctype);
-      const long total = (long)s.n_cells * T + (long)T * s.nbf * s.nbf;
-      const int grid = (int)std::min<long>((total + 255) / 256, (long)ctx->sm_count * 8);
-      (void)cd_launch(mf_convert_kernel, grid, 256, 0, ctx->stream, s.n_cells, T, Tr, s.nbf, s.d_cellcoef, s.d_ref, s.d_cf32,
-                                                        s.d_R32);
-      CD_LAUNCHED(ctx);
-      s.mf_version = s.assembly_version;
-    }
+    int rc = prepare_mf(ctx, s);
+    if (rc) return rc;
     mask |= 1u << l;
-  }
-  if (mask)
-  {
-    // shared memory of the tensor-core kernel (set outside any capture)
-    CD_CUDA(ctx, cudaFuncSetAttribute(mf_cell27_tc_kernel<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
-    CD_CUDA(ctx, cudaFuncSetAttribute(mf_cell27_tc_kernel<13>, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
-    if (!ctx->d_err)
-    {
-      int rc = dev_alloc(ctx, &ctx->d_err, 1);
-      if (rc) return rc;
-      CD_CUDA(ctx, cudaMallocHost((void **)&ctx->h_err, sizeof(int)));
-      CD_CUDA(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
-    }
   }
   if (mask != h.mf_mask && h.gexec[1])
   {
@@ -1286,4 +1291,29 @@ int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const 
   if (rc == CDGPU_OK && p.precision == 1 && h.mf_mask)
     rc = p.solver == 16 && ctx->h_err ? err_flag_status(ctx) : assemble_check(ctx);
   return rc;
+}
+
+// y = A x with one of the FP32 forms of a space's operator that the mixed multigrid cycle uses:
+// form 0 the FP32 copy of the assembled CSR matrix, 1 the matrix-free per-cell products on CUDA
+// cores, 2 the same products on the tensor cores (tcgen05, TF32 inputs).  Dirichlet rows are
+// identity rows in every form.  Forms 1 and 2 need a Q2 hexahedral space assembled by the
+// affine constant-coefficient path.
+int apply_fp32_form(cdgpu_ctx *ctx, Space &s, int form, const float *d_x, float *d_y)
+{
+  if (form == 0)
+  {
+    csr_spmv<float>(ctx, s, d_x, d_y);
+    CD_LAUNCHED(ctx);
+    return CDGPU_OK;
+  }
+  if (s.mf_T <= 0 || !mf_shape_ok(s.nbf, s.mf_T))
+    return fail(ctx, CDGPU_ERR_UNSUPPORTED,
+                "apply_fp32: the matrix-free forms need Q2 hexahedra assembled from affine cells with constant coefficients");
+  int rc = prepare_mf(ctx, s);
+  if (rc) return rc;
+  mf_apply_cells(ctx, s, d_x, form == 2);
+  CD_LAUNCHED(ctx);
+  mf_rows<MF_SPMV>(ctx, s, d_x, nullptr, nullptr, d_y, 0.f);
+  CD_LAUNCHED(ctx);
+  return assemble_check(ctx); // the tensor-core wait flag
 }

@@ -246,6 +246,25 @@ int cdgpu_tcd_step(cdgpu_ctx *ctx, int tcd_id, const cdgpu_solver_params *p, dou
   return CDGPU_OK;
 }
 
+// copies of one level's mass matrix M (as updated in place), stiffness matrix A and the system
+// matrix the last step's solve used (the level's installed entries), each nullable; like
+// TSystemTCD2D's sqmatrixM / sqmatrixA members (include/System/SystemTCD2D.h)
+int cdgpu_tcd_matrices(cdgpu_ctx *ctx, int tcd_id, int level, double *h_M, double *h_A, double *h_S)
+{
+  Tcd *t = get_tcd(ctx, tcd_id);
+  if (!t || level < 0 || level >= (int)t->h->lev.size()) return fail(ctx, CDGPU_ERR_INVALID, "tcd_matrices: bad argument");
+  if ((h_M && !t->have_mass) || (h_A && !t->have_stiff)) return fail(ctx, CDGPU_ERR_INVALID, "tcd_matrices: not assembled");
+  const Space &s = *t->h->lev[level].sp;
+  if (h_S && !s.assembled) return fail(ctx, CDGPU_ERR_INVALID, "tcd_matrices: no system matrix yet");
+  cudaSetDevice(ctx->device);
+  const size_t bytes = sizeof(double) * s.nnz;
+  if (h_M) CD_CUDA(ctx, cudaMemcpyAsync(h_M, t->M[level], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (h_A) CD_CUDA(ctx, cudaMemcpyAsync(h_A, t->A[level], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (h_S) CD_CUDA(ctx, cudaMemcpyAsync(h_S, s.d_a, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CDGPU_OK;
+}
+
 // the current finest right-hand side (f, phi) of the last assembly, to the host
 int cdgpu_tcd_rhs(cdgpu_ctx *ctx, int tcd_id, double *h_rhs)
 {

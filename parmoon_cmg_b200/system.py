@@ -135,6 +135,14 @@ class Context:
         self.check(self.lib.cdgpu_spmv(self.h, sid, _p(x), _p(y)))
         return y
 
+    def apply_fp32(self, sid, x, form):
+        """y = A x with an FP32 form of the operator: 0 CSR copy, 1 matrix-free on CUDA cores,
+        2 matrix-free on the tensor cores."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros_like(x)
+        self.check(self.lib.cdgpu_apply_fp32(self.h, sid, form, _p(x), _p(y)))
+        return y
+
     def defect(self, sid, x, f):
         x, f = _f64(x), _f64(f)
         d = np.zeros_like(x)
@@ -305,6 +313,13 @@ class TSystemTCD2D:
         r = np.zeros(self.N_DOF)
         self.ctx.check(self.ctx.lib.cdgpu_tcd_rhs(self.ctx.h, self.tcd, _p(r)))
         return r
+
+    def matrices(self, level, nnz):
+        """(M, A, S) of a level (0 = coarsest): the mass matrix as updated in place, the
+        stiffness matrix and the system matrix of the last step."""
+        out = [np.zeros(nnz) for _ in range(3)]
+        self.ctx.check(self.ctx.lib.cdgpu_tcd_matrices(self.ctx.h, self.tcd, level, *[_p(a) for a in out]))
+        return tuple(out)
 
     def AssembleMRhs(self, sol=None):
         self.ctx.check(self.ctx.lib.cdgpu_tcd_assemble_mass(self.ctx.h, self.tcd))

@@ -9,7 +9,7 @@ prolongations, solutions, iteration counts and (sine problem) the L2 / H1-semi
 errors -- as compressed .npz files.  Needs the reference build; the tests only
 read the .npz files.
 
-Usage: python tests/golden/make_golden.py
+Usage: python tests/golden/make_golden.py [case names; default all]
 """
 import os
 import subprocess
@@ -44,20 +44,37 @@ SC_LIN_MAXIT_SCALAR: {maxit}
 SC_VERBOSE: 0
 """
 
-# name, dim, order, disctype, uniform steps, levels, example, eps, b, c, f, extra keys
+B3 = (0.5773502691896258,) * 3  # (1,1,1)/sqrt(3)
+
+# name, dim, order, disctype, uniform steps, levels, example, eps, b, c, f, extra keys, mesh
+# (mesh None: the unit square / unit cube).  skew_quad is one quadrilateral that is not a
+# parallelogram and frustum one hexahedron that is not a parallelepiped, so every cell of
+# their refinements takes the reference's bilinear / trilinear map (QuadBilinear,
+# HexaTrilinear) instead of the affine one.
 CASES = [
-    ("cd3d_q1_gal_4", 3, 1, 1, 1, 2, 0, 1e-2, (0.5773502691896258,) * 3, 0.0, 1.0, ""),
-    ("cd3d_q2_gal_4", 3, 2, 1, 1, 2, 0, 1e-1, (0.2886751345948129,) * 3, 0.0, 1.0, ""),
-    ("cd3d_q1_gal_8", 3, 1, 1, 1, 3, 0, 1e-1, (1.0, 0.3, -0.2), 0.5, 1.0, ""),
-    ("cd2d_q1_sine_32", 2, 1, 1, 1, 5, 1, 0.0, (0.0, 0.0), 0.0, 0.0, "PE_NR: 10\n"),
-    ("cd2d_q1_supg_16", 2, 1, 2, 2, 3, 0, 1e-3, (1.0, 0.5), 0.0, 1.0, ""),
-    ("cd2d_q2_supg_8", 2, 2, 2, 1, 3, 0, 1e-3, (1.0, 0.5), 0.0, 1.0, ""),
-    ("cd2d_q2_gal_8", 2, 2, 1, 1, 3, 0, 1e-1, (-0.6, 0.8), 1.0, 1.0, ""),
+    ("cd3d_q1_gal_4", 3, 1, 1, 1, 2, 0, 1e-2, B3, 0.0, 1.0, "", None),
+    ("cd3d_q2_gal_4", 3, 2, 1, 1, 2, 0, 1e-1, (0.2886751345948129,) * 3, 0.0, 1.0, "", None),
+    ("cd3d_q1_gal_8", 3, 1, 1, 1, 3, 0, 1e-1, (1.0, 0.3, -0.2), 0.5, 1.0, "", None),
+    ("cd2d_q1_sine_32", 2, 1, 1, 1, 5, 1, 0.0, (0.0, 0.0), 0.0, 0.0, "PE_NR: 10\n", None),
+    ("cd2d_q1_supg_16", 2, 1, 2, 2, 3, 0, 1e-3, (1.0, 0.5), 0.0, 1.0, "", None),
+    ("cd2d_q2_supg_8", 2, 2, 2, 1, 3, 0, 1e-3, (1.0, 0.5), 0.0, 1.0, "", None),
+    ("cd2d_q2_gal_8", 2, 2, 1, 1, 3, 0, 1e-1, (-0.6, 0.8), 1.0, 1.0, "", None),
+    # the coefficients of the CD3D Q2 32^3 benchmark (eps 1e-2, b = (1,1,1)/sqrt(3), f = 1)
+    # on the 8^3 mesh with the same element; one level, because the reference's Galerkin
+    # multigrid does not converge at this Peclet number (its FGMRES stalls at rate 1 with 2 or
+    # 3 levels), while FGMRES preconditioned by its SSOR coarse-level loop alone converges
+    ("cd3d_q2_gal_8_bench", 3, 2, 1, 3, 1, 0, 1e-2, B3, 0.0, 1.0, "", None),
+    # non-affine cells
+    ("cd2d_q1_skew_supg_16", 2, 1, 2, 2, 3, 0, 1e-3, (1.0, 0.5), 0.0, 1.0, "", "skew_quad"),
+    ("cd2d_q2_skew_supg_8", 2, 2, 2, 1, 3, 0, 1e-2, (0.6, -0.8), 0.5, 1.0, "", "skew_quad"),
+    ("cd2d_q2_skew_gal_8", 2, 2, 1, 1, 3, 0, 1e-1, (-0.6, 0.8), 1.0, 1.0, "", "skew_quad"),
+    ("cd3d_q1_frustum_gal_8", 3, 1, 1, 1, 3, 0, 1e-1, (1.0, 0.3, -0.2), 0.5, 1.0, "", "frustum"),
+    ("cd3d_q2_frustum_gal_4", 3, 2, 1, 1, 2, 0, 1e-1, (0.3, 0.2, -0.4), 0.5, 1.0, "", "frustum"),
 ]
 
 
-def run_case(name, dim, order, disc, steps, levels, example, eps, b, c, f, extra, tmp):
-    geo = "unit_cube" if dim == 3 else "unit_square"
+def run_case(name, dim, order, disc, steps, levels, example, eps, b, c, f, extra, mesh, tmp):
+    geo = mesh or ("unit_cube" if dim == 3 else "unit_square")
     dat = os.path.join(tmp, name + ".dat")
     with open(dat, "w") as fh:
         fh.write(f"VERSION: 1\nLOGFILE: logfile\nOUTFILE: {os.path.join(tmp, name + '.out')}\n"
@@ -92,9 +109,11 @@ def run_case(name, dim, order, disc, steps, levels, example, eps, b, c, f, extra
 
 
 def main():
+    only = set(sys.argv[1:])
     with tempfile.TemporaryDirectory() as tmp:
         for case in CASES:
-            run_case(*case, tmp)
+            if not only or case[0] in only:
+                run_case(*case, tmp)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,219 @@
+"""Parity of the CD3D Q2 benchmark problem at its own size (32^3 cells, 274,625 DOFs).
+
+Problem: unit cube, Q2 hexahedra, eps = 1e-2, b = (1,1,1)/sqrt(3), c = 0, f = 1, Dirichlet 0,
+Galerkin on the finest level; the library's hierarchy is 2^3 ... 32^3 with SUPG coarse-grid
+operators (delta0 = 1/3) and the exact FP64 coarse solve.
+
+Checked against two independent FP64 answers:
+  * the oracle's C restatement (oracle/cdoracle.c) on the same mesh and numbering: pattern
+    bit-exact, entries and rhs of every level within 1e-12, its tightly converged solution;
+  * the compiled reference itself (oracle/_ref/cd3d_dump, TSystemCD3D with its own
+    3-level Galerkin multigrid and SSOR coarse smoother, converged to 1e-12 of the initial
+    residual): its finest matrix, right-hand side and solution, matched to this library's DOF
+    numbering through the DOF coordinates.
+
+Bars: entries/rhs <= 1e-12 relative, FP64 solution <= 1e-10, mixed-form solution <= 1e-8,
+also at the benchmark's own stopping rule (||r|| <= 1e-10 ||r0||).
+"""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from parmoon_cmg_b200 import mesh
+from parmoon_cmg_b200.system import GALERKIN, SUPG, Context, coeffs, solver_params
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EPS = 1e-2
+B3 = (0.5773502691896258,) * 3
+N_FINE, LEVELS = 32, 5
+
+TOL_ENTRIES = 1e-12
+TOL_SOL = 1e-10
+TOL_MIXED = 1e-8
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from parmoon_cmg_b200 import _build
+    _build.build()
+    c = Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def case(ctx, oracle_lib):
+    """The library's hierarchy and the oracle's assembly and tight solution of the same."""
+    spaces, parents = mesh.structured_hierarchy(3, 2, N_FINE // 2 ** (LEVELS - 1), LEVELS)
+    co = coeffs(0, eps=EPS, b=B3, f=1.0, delta0=1.0 / 3.0)
+    oco = oracle_lib.coeffs(0, eps=EPS, b=B3, f=1.0, delta0=1.0 / 3.0)
+    sids, levels = [], []
+    for l, sp in enumerate(spaces):
+        sid = ctx.upload_space(sp)
+        ctx.build_pattern(sid)
+        ctx.set_coeffs(sid, co)
+        sids.append(sid)
+        disc = GALERKIN if l == LEVELS - 1 else SUPG
+        rp, kc = oracle_lib.pattern(sp["global_numbers"], sp["begin_index"], sp["n_dof"], sp["n_active"])
+        ent, rhs = oracle_lib.assemble(3, 2, disc, sp["coords"], sp["global_numbers"], sp["begin_index"],
+                                       sp["n_dof"], sp["n_active"], rp, kc, oco)
+        lv = dict(n_dof=sp["n_dof"], n_active=sp["n_active"], row_ptr=rp, kcol=kc, entries=ent, rhs=rhs,
+                  disc=disc)
+        if l > 0:
+            lv["p_row"], lv["p_col"], lv["p_val"] = oracle_lib.prolongation(3, 2, spaces[l - 1], sp, parents[l])
+        levels.append(lv)
+    mg = ctx.hierarchy(sids, parents)
+    rhs = levels[-1]["rhs"]
+    tight = oracle_lib.solver_params(coarse_smoother=17, red_factor=0.0,
+                                     res_norm_min=1e-13 * np.linalg.norm(rhs), maxit=300)
+    x_o, its_o, _, _ = oracle_lib.solve(levels, tight, rhs, np.zeros(spaces[-1]["n_dof"]))
+    return dict(spaces=spaces, parents=parents, sids=sids, mg=mg, levels=levels, x_o=x_o, its_o=its_o)
+
+
+REF_DAT = """VERSION: 1
+LOGFILE: logfile
+OUTFILE: {out}
+BNDFILE: {mesh}/unit_cube.PRM
+GEOFILE: {mesh}/unit_cube.GEO
+MESH_TYPE: 0
+UNIFORM_STEPS: 3
+LEVELS: 3
+ANSATZ_ORDER: 2
+DISCTYPE: 1
+SOLVER_TYPE: 1
+SC_SOLVER_SCALAR: 16
+SC_PRECONDITIONER_SCALAR: 5
+SC_SMOOTHER_SCALAR: 1
+SC_SMOOTH_DAMP_FACTOR_SCALAR: 0.8
+SC_SMOOTH_DAMP_FACTOR_FINE_SCALAR: 0.8
+SC_PRE_SMOOTH_SCALAR: 2
+SC_POST_SMOOTH_SCALAR: 2
+SC_MG_CYCLE_SCALAR: 1
+SC_STEP_LENGTH_CONTROL_ALL_SCALAR: 0
+SC_STEP_LENGTH_CONTROL_FINE_SCALAR: 0
+SC_GMRES_RESTART: 30
+SC_LIN_RED_FACTOR_SCALAR: 1e-12
+SC_LIN_RES_NORM_MIN_SCALAR: 0
+SC_LIN_MAXIT_SCALAR: 1000
+SC_VERBOSE: 0
+"""
+
+
+def dof_key(X, n_nodes):
+    k = np.rint(X * (n_nodes - 1)).astype(np.int64)
+    return k[:, 0] + n_nodes * (k[:, 1] + n_nodes * k[:, 2])
+
+
+@pytest.fixture(scope="module")
+def reference(case, oracle_lib):
+    """The compiled reference's own run of the problem (3 Galerkin levels 8^3..32^3, SSOR coarse
+    smoother, stopped at ||r|| <= 1e-12 ||r0||): finest matrix, rhs and solution, with the
+    permutation from its DOF numbering to the library's (perm[i] = our DOF of its DOF i)."""
+    import refdump
+    exe = os.path.join(ROOT, "oracle", "_ref", "cd3d_dump")
+    assert os.path.exists(exe), "the compiled reference (oracle/_ref/cd3d_dump) is missing"
+    with tempfile.TemporaryDirectory() as tmp:
+        dat = os.path.join(tmp, "r.dat")
+        with open(dat, "w") as f:
+            f.write(REF_DAT.format(out=os.path.join(tmp, "r.out"), mesh=os.path.join(ROOT, "oracle", "meshes")))
+        out = os.path.join(tmp, "dump")
+        os.makedirs(out)
+        subprocess.run([exe, dat, out, repr(EPS), *map(repr, B3), "0", "1", "0", "1e-12"], cwd=tmp, check=True,
+                       capture_output=True)
+        d = refdump.load_dir(out)
+    L = refdump.level(d, int(d["levels"]) - 1)
+    sp = case["spaces"][-1]
+    nn = 2 * N_FINE + 1
+    kr = dof_key(oracle_lib.dof_coords(3, 2, L["coords"], L["global_numbers"], L["begin_index"], L["n_dof"]), nn)
+    ko = dof_key(mesh.dof_coords(sp), nn)
+    inv = np.full(nn ** 3, -1, np.int64)
+    inv[ko] = np.arange(len(ko))
+    perm = inv[kr]
+    assert L["n_dof"] == sp["n_dof"] and (perm >= 0).all() and len(np.unique(perm)) == len(perm)
+    return dict(L=L, solution=d["solution"], perm=perm, iterations=int(d["iterations"]))
+
+
+def gpu_solve(ctx, case, precision, **kw):
+    """Assemble the hierarchy (Galerkin finest level, SUPG coarse levels) and solve from zero."""
+    ctx.assemble_hierarchy(case["mg"], GALERKIN, SUPG)
+    nd = case["spaces"][-1]["n_dof"]
+    rhs = case["levels"][-1]["rhs"]
+    prm = dict(coarse_smoother=17, stop_rule=1, red_factor=1e-13, res_norm_min=0.0, maxit=300)
+    prm.update(kw)
+    x, info = ctx.solve(case["mg"], solver_params(precision=precision, **prm), rhs, np.zeros(nd))
+    assert info.status == 0, info.status
+    return x, info
+
+
+def test_bench_assembly_vs_oracle(ctx, case):
+    """Every level's pattern bit-exact and entries/rhs within 1e-12 of the oracle's."""
+    for sp, sid, lv in zip(case["spaces"], case["sids"], case["levels"]):
+        nnz = len(lv["kcol"])
+        rp, kc = ctx.get_pattern(sid, sp["n_dof"], nnz)
+        assert np.array_equal(rp, lv["row_ptr"]) and np.array_equal(kc, lv["kcol"])
+        ent, rhs = ctx.assemble(sid, lv["disc"], sp["n_dof"], nnz)
+        assert rel(ent, lv["entries"]) <= TOL_ENTRIES, (sp["n"], rel(ent, lv["entries"]))
+        assert rel(rhs, lv["rhs"]) <= TOL_ENTRIES
+
+
+def test_bench_assembly_vs_reference(ctx, case, reference):
+    """The finest matrix and right-hand side against the reference's own TSystemCD3D::Assemble at
+    32^3, entry by entry after renumbering its DOFs (P A_ref P^T)."""
+    import scipy.sparse as sps
+    L, perm = reference["L"], reference["perm"]
+    sp, lv = case["spaces"][-1], case["levels"][-1]
+    n = sp["n_dof"]
+    ent, rhs = ctx.assemble(case["sids"][-1], GALERKIN, n, len(lv["kcol"]))
+    A = sps.csr_matrix((ent, lv["kcol"], lv["row_ptr"]), shape=(n, n))
+    R = sps.csr_matrix((L["entries"], L["kcol"], L["row_ptr"]), shape=(n, n)).tocoo()
+    Rp = sps.csr_matrix((R.data, (perm[R.row], perm[R.col])), shape=(n, n))
+    assert A.nnz == Rp.nnz
+    assert abs(A - Rp).max() <= TOL_ENTRIES * abs(Rp).max()
+    # the same sparsity: no entry of one pattern is missing from the other
+    Ab, Rb = A.copy(), Rp.copy()
+    Ab.data[:] = 1.0
+    Rb.data[:] = 1.0
+    D = (Ab - Rb).tocsr()
+    D.eliminate_zeros()
+    assert D.nnz == 0
+    r_ref = np.empty(n)
+    r_ref[perm] = L["rhs"]
+    assert rel(rhs, r_ref) <= TOL_ENTRIES
+
+
+def test_bench_solution_vs_oracle_and_reference(ctx, case, reference):
+    """FP64 form within 1e-10 and mixed form within 1e-8 of both FP64 answers (solves run to
+    ||r|| <= 1e-13 ||r0||)."""
+    perm = reference["perm"]
+    x_ref = np.empty_like(reference["solution"])
+    x_ref[perm] = reference["solution"]
+    # the two independent FP64 answers agree with each other first
+    assert rel(case["x_o"], x_ref) <= TOL_SOL
+    x64, i64 = gpu_solve(ctx, case, 0)
+    assert rel(x64, case["x_o"]) <= TOL_SOL, rel(x64, case["x_o"])
+    assert rel(x64, x_ref) <= TOL_SOL, rel(x64, x_ref)
+    xm, im = gpu_solve(ctx, case, 1)
+    assert rel(xm, case["x_o"]) <= TOL_MIXED, rel(xm, case["x_o"])
+    assert rel(xm, x_ref) <= TOL_MIXED, rel(xm, x_ref)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_bench_stopping_rule_error(ctx, case, reference, precision):
+    """At the benchmark's own stopping rule (||r|| <= 1e-10 ||r0||, as timed by bench.py) both
+    forms are within 1e-8 of the reference's FP64 solution."""
+    perm = reference["perm"]
+    x_ref = np.empty_like(reference["solution"])
+    x_ref[perm] = reference["solution"]
+    x, info = gpu_solve(ctx, case, precision, red_factor=1e-10)
+    err = rel(x, x_ref)
+    print(f"precision {precision}: {info.iterations} iterations, rel. error vs reference {err:.3e}")
+    assert err <= TOL_MIXED, err

@@ -21,16 +21,19 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
-def test_defect_noalloc_matches_defect():
+# 3D Q2 takes the 32-thread row groups; 2D Q1 and 3D Q1 the 16-thread ones, on more than 2048
+# rows so that several blocks write partial sums
+@pytest.mark.parametrize("dim,order,n", [(3, 2, 6), (2, 1, 64), (3, 1, 16)])
+def test_defect_noalloc_matches_defect(dim, order, n):
     import torch
     from parmoon_cmg_b200 import _build
     _build.build()
     ctx = Context(0)
     try:
-        sp = mesh.structured_space(3, 2, 6)
+        sp = mesh.structured_space(dim, order, n)
         sid = ctx.upload_space(sp)
         nnz = ctx.build_pattern(sid)
-        ctx.set_coeffs(sid, coeffs(0, eps=1e-2, b=(0.3, 0.2, 0.1), c=0.5))
+        ctx.set_coeffs(sid, coeffs(0, eps=1e-2, b=(0.3, 0.2, 0.1)[:dim], c=0.5))
         ctx.assemble(sid, 1, sp["n_dof"], nnz, want_entries=False)
         rng = np.random.default_rng(7)
         for call in range(2):
