@@ -61,8 +61,9 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched CD2D section")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream section")
     ap.add_argument("--batched-instances", type=int, default=4096)
-    ap.add_argument("--serving-requests", type=int, default=200)
-    ap.add_argument("--serving-rate", type=float, default=40.0, help="mean arrivals per second")
+    ap.add_argument("--serving-requests", type=int, default=100, help="requests per arrival rate")
+    ap.add_argument("--serving-rates", default="5,10,20,40",
+                    help="mean arrivals per second, swept in this order (comma separated)")
     ap.add_argument("--no-tcd", action="store_true", help="skip the time-dependent CD2D section")
     ap.add_argument("--no-cd2d", action="store_true", help="skip the CD2D plain FP64 section")
     ap.add_argument("--tcd-instances", type=int, default=256)
@@ -172,8 +173,13 @@ def run_reference_arm(args, rank, world):
     procs = max(1, min(cores, 32, int(mem_gb // 2)))
     tmp = tempfile.mkdtemp()
     try:
+        # The timed part of a step is what the GPU arm times: TSystemCD3D::Assemble + Solve.
+        # Every process reports its own wall-clock times of those two calls (steady_clock
+        # around Assemble() and Solve() in the dump driver); the processes run concurrently,
+        # so a step takes the slowest process's assemble + solve.  Mesh refinement, FE spaces
+        # and matrix structures (the reference's construction phase, which the GPU arm also
+        # does once before its timed region) are reported beside it, not counted.
         def step():
-            t0 = time.perf_counter()
             ps = []
             exe = os.path.join(ROOT, "oracle", "_ref", "cd3d_dump")
             steps_ = int(round(np.log2(args.n))) - (REF_LEVELS - 1)
@@ -187,13 +193,16 @@ def run_reference_arm(args, rank, world):
                                            cwd=tmp, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
                                            text=True))
             outs = [json.loads([l for l in p.communicate()[0].splitlines() if l.startswith("{")][-1]) for p in ps]
-            return time.perf_counter() - t0, outs
+            timed = max(o["t_assemble"] + o["t_solve"] for o in outs)
+            construct = max(o["t_mesh"] + o["t_construct"] for o in outs)
+            return timed, construct, outs
         for _ in range(max(0, min(args.warmup, 1))):
             step()
-        times, its = [], []
+        times, cons, its = [], [], []
         for _ in range(args.steps):
-            dt, outs = step()
+            dt, ct, outs = step()
             times.append(dt)
+            cons.append(ct)
             its.append(outs[0]["iterations"])
         total = sum(times)
         value = procs * len(times) / total
@@ -207,10 +216,14 @@ def run_reference_arm(args, rank, world):
                                    f"one V(2,2) damped-Jacobi (0.8) cycle to ||r|| <= 1e-10 ||r0||",
                        "multigrid": f"{REF_LEVELS} levels Galerkin, SSOR coarse smoother (the reference's "
                                     f"own convergent setting; its exact coarse solve needs LAPACK)",
-                       "processes": procs, "fgmres_iterations": its[0]},
+                       "processes": procs, "fgmres_iterations": its[0],
+                       "timed_region": "TSystemCD3D::Assemble + Solve per process (steady_clock in the driver), "
+                                       "the slowest of the concurrent processes per step; the same calls the "
+                                       "GPU arm times",
+                       "construction_s_per_step": float(np.mean(cons))},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
                              "sample": f"{procs} concurrent reference processes x {args.steps} steps, "
-                                       f"each one full assemble+solve of the workload"},
+                                       f"each one assemble+solve of the workload (construction excluded)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
         print(json.dumps(out), flush=True)
@@ -440,20 +453,50 @@ def run_ours(args, rank, world, local):
         "gpu_launches": launches,
         "clocks": clocks,
     }
-    return result, ctx
+    return result, ctx, dict(x64=x64, xm=xm, space=spaces[-1])
 
 
-def _direct_check(ctx, sid, n_dof, nnz, co):
-    """FP64 solution of an instance's finest system by a direct solve on the host (scipy),
-    from the library's own FP64 assembly of the same coefficients."""
-    import scipy.sparse as sps
-    import scipy.sparse.linalg as spl
-    from parmoon_cmg_b200.system import SUPG
-    ctx.set_coeffs(sid, co)
-    ent, rhs = ctx.assemble(sid, SUPG, n_dof, nnz)
-    rp, kc = ctx.get_pattern(sid, n_dof, nnz)
-    A = sps.csr_matrix((ent, kc, rp), shape=(n_dof, n_dof))
-    return spl.spsolve(A.tocsc(), rhs)
+def reference_accuracy(n, sols, tmp):
+    """Checker of the cpu_baseline leg: the reference's own FP64 solution of the workload
+    (oracle/_ref/cd3d_dump, 3 Galerkin levels, converged to ||r|| <= 1e-12 ||r0||) against the
+    GPU arm's solutions at the timed stopping rule, matched through the DOF coordinates."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    import refdump
+    from parmoon_cmg_b200 import mesh
+    exe = os.path.join(ROOT, "oracle", "_ref", "cd3d_dump")
+    steps = int(round(np.log2(n))) - (REF_LEVELS - 1)
+    dat = os.path.join(tmp, "acc.dat")
+    with open(dat, "w") as f:
+        f.write(DAT.format(out=os.path.join(tmp, "acc.out"), mesh=os.path.join(ROOT, "oracle", "meshes"),
+                           steps=steps, levels=REF_LEVELS))
+    out = os.path.join(tmp, "acc")
+    os.makedirs(out, exist_ok=True)
+    subprocess.run([exe, dat, out, repr(EPS), *map(repr, B), "0", "1", "0", "1e-12"], cwd=tmp,
+                   capture_output=True, text=True, check=True)
+    d = refdump.load_dir(out)
+    L = refdump.level(d, int(d["levels"]) - 1)
+    sp = sols["space"]
+    nn = 2 * n + 1
+
+    def key(X):
+        k = np.rint(X * (nn - 1)).astype(np.int64)
+        return k[:, 0] + nn * (k[:, 1] + nn * k[:, 2])
+    kr = key(oracle.dof_coords(3, 2, L["coords"], L["global_numbers"], L["begin_index"], L["n_dof"]))
+    ko = key(mesh.dof_coords(sp))
+    inv = np.full(nn ** 3, -1, np.int64)
+    inv[ko] = np.arange(len(ko))
+    perm = inv[kr]
+    if (perm < 0).any():
+        raise RuntimeError("DOF coordinates of the reference and the GPU arm do not match")
+    x_ref = np.empty(L["n_dof"])
+    x_ref[perm] = d["solution"]
+    scale = np.abs(x_ref).max()
+    return {"mixed": float(np.abs(sols["xm"] - x_ref).max() / scale),
+            "fp64": float(np.abs(sols["x64"] - x_ref).max() / scale),
+            "reference_run": "oracle/_ref/cd3d_dump, 3 Galerkin levels, SSOR coarse smoother, "
+                             f"||r|| <= 1e-12 ||r0|| ({int(d['iterations'])} FGMRES iterations)",
+            "norm": "max |x - x_ref| / max |x_ref|"}
 
 
 def run_batched(ctx, args):
@@ -492,13 +535,11 @@ def run_batched(ctx, args):
     small = [i for i, w in enumerate(work) if W.dofs(2, w["order"], w["n_used"]) <= 40000]
     sample = sorted(rng.choice(small, size=min(8, len(small)), replace=False).tolist())
     errs = []
-    for i in sample:
+    for i in (sample if not args.no_cpu_baseline else []):
         w = work[i]
         sid, n_dof = cache.get(2, w["order"], w["n_used"])
         x, _ = B.fetch(slots[i], n_dof)
-        co = coeffs(0, eps=w["eps"], b=w["b"], f=1.0, poly_degree=w["order"])
-        st = B.structures[sid]
-        ref = _direct_check(ctx, st["sids"][-1], n_dof, st["nnz"][-1], co)
+        ref = fp64_solution(2, w["order"], w["n_used"], w["eps"], w["b"])
         errs.append(float(np.abs(x - ref).max() / np.abs(ref).max()))
     for sl in slots:
         B.release(sl)
@@ -510,7 +551,8 @@ def run_batched(ctx, args):
         "converged": int(sum(1 for st in status if st == 0)),
         "iterations": {"min": int(min(its)), "median": float(np.median(its)), "p99": float(np.percentile(its, 99)),
                        "max": int(max(its))},
-        "rel_err_vs_fp64_direct": {"max": max(errs) if errs else None, "sample": len(errs)},
+        "rel_err_vs_fp64_direct": {"max": max(errs) if errs else None, "sample": len(errs),
+                                   "reference": "the oracle's FP64 assembly of the instance, solved directly"},
         "config": "4096 instances, N log-uniform [16,256] (rounded to the hierarchy, recorded per instance), "
                   "Q1/Q2 50/50, eps 10^U(-6,-1), |b|=1 random angle, f=1, Dirichlet 0, SUPG; FGMRES(30) FP64 "
                   "with an FP32 V(2,2) multicolour-SSOR cycle, exact coarse solve, ||r|| <= 1e-10 ||r0||; "
@@ -520,20 +562,58 @@ def run_batched(ctx, args):
 
 def run_serving(ctx, args):
     """Serving stream: Poisson arrivals (70 % 2D / 30 % 3D, Q1/Q2, 1e3..2e6 DOFs, random
-    coefficients) admitted under a 150 GB device budget into one running batch."""
+    coefficients) admitted under a 150 GB device budget into one running batch, at several
+    arrival rates up to saturation (the same seeded requests, arrival times scaled).  At each
+    rate a sample of finished requests (the first four of at most 40,000 DOFs) is compared with
+    the FP64 solution of the same instance (checker of the cpu_baseline leg)."""
     from parmoon_cmg_b200 import workloads as W
     from parmoon_cmg_b200.serving import Server
-    reqs = W.serving_stream(args.serving_requests, args.serving_rate)
-    srv = Server(ctx, budget_bytes=150 * 10 ** 9)
-    srv.prepare(reqs)
-    srv.run(reqs)
-    st = srv.stats()
-    st.update({"metric": "serving solves/s and latency", "arrival_rate_per_s": args.serving_rate,
-               "requests": len(reqs), "budget_bytes": 150 * 10 ** 9,
-               "config": "Poisson arrivals, 70% 2D / 30% 3D, Q1/Q2 50/50, DOFs 10^U(3, log10 2e6) mapped to the "
-                         "nearest admissible mesh, eps 10^U(-6,-1), random unit b, f=1, Dirichlet 0, SUPG; "
-                         "seed 20261204"})
-    return st
+    rates = [float(r) for r in args.serving_rates.split(",") if r.strip()]
+    sweep = []
+    for rate in rates:
+        reqs = W.serving_stream(args.serving_requests, rate)
+        srv = Server(ctx, budget_bytes=150 * 10 ** 9)
+        srv.prepare(reqs)
+        sample = []
+
+        def keep(r):
+            if args.no_cpu_baseline or len(sample) >= 4 or W.dofs(r["dim"], r["order"], r["n"]) > 40000:
+                return False
+            sample.append(r)
+            return True
+        srv.run(reqs, keep_solutions=keep)
+        st = srv.stats()
+        errs = []
+        for r in sample:
+            ref = fp64_solution(r["dim"], r["order"], r["n"], r["eps"], r["b"])
+            errs.append(float(np.abs(r["solution"] - ref).max() / np.abs(ref).max()))
+        st.update({"arrival_rate_per_s": rate, "requests": len(reqs),
+                   "rel_err_vs_fp64": {"max": max(errs) if errs else None, "sample": len(errs)}})
+        sweep.append(st)
+    return {"metric": "serving solves/s and p50/p99 latency per arrival rate", "budget_bytes": 150 * 10 ** 9,
+            "sweep": sweep,
+            "config": "Poisson arrivals, 70% 2D / 30% 3D, Q1/Q2 50/50, DOFs 10^U(3, log10 2e6) mapped to the "
+                      "nearest admissible mesh, eps 10^U(-6,-1), random unit b, f=1, Dirichlet 0, SUPG; "
+                      f"{args.serving_requests} requests per rate, seed 20261204; error sample against the "
+                      "oracle's FP64 assembly solved directly"}
+
+
+def fp64_solution(dim, order, n, eps, b):
+    """Checker of the cpu_baseline leg: the FP64 solution of one instance (unit square / cube,
+    n^dim cells, SUPG with the instance's polynomial degree) from the oracle's assembly
+    (oracle/cdoracle.c, pinned to the reference's fixtures), solved by a direct sparse solve."""
+    import scipy.sparse as sps
+    import scipy.sparse.linalg as spl
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from parmoon_cmg_b200 import mesh
+    sp = mesh.structured_space(dim, order, n)
+    rp, kc = oracle.pattern(sp["global_numbers"], sp["begin_index"], sp["n_dof"], sp["n_active"])
+    co = oracle.coeffs(0, eps=eps, b=tuple(b), f=1.0, order_pd=order)
+    ent, rhs = oracle.assemble(dim, order, 2, sp["coords"], sp["global_numbers"], sp["begin_index"],
+                               sp["n_dof"], sp["n_active"], rp, kc, co)
+    A = sps.csr_matrix((ent, kc, rp), shape=(sp["n_dof"],) * 2)
+    return spl.spsolve(A.tocsc(), rhs)
 
 
 DAT2D = """VERSION: 1
@@ -680,7 +760,7 @@ def main():
         if args.impl == "reference":
             run_reference_arm(args, rank, world)
             return
-        result, ctx = run_ours(args, rank, world, local)
+        result, ctx, sols = run_ours(args, rank, world, local)
         if not args.no_cd2d:
             result["cd2d"] = run_cd2d(ctx, args)
         if not args.no_batched:
@@ -703,6 +783,10 @@ def main():
                 except Exception as e:  # the product run stays valid without the baseline
                     result["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
                                               "sample": f"unavailable: {e}"}
+                try:
+                    result["rel_err_vs_reference"] = reference_accuracy(args.n, sols, tmp)
+                except Exception as e:
+                    result["rel_err_vs_reference"] = {"unavailable": str(e)}
                 finally:
                     shutil.rmtree(tmp, ignore_errors=True)
             print(json.dumps(result), flush=True)

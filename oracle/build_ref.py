@@ -19,7 +19,8 @@ cblas headers, ALE, TNSE) are skipped and listed in ``oracle/_ref/<geo>/skipped.
 the few external symbols they would have provided are abort-stubs in
 ``oracle/ref_driver/stubs.C``.
 
-Usage:  python oracle/build_ref.py [--ref /root/reference] [--jobs 8] [--geo 2D 3D]
+Usage:  python oracle/build_ref.py [--ref <reference tree>] [--jobs 8] [--geo 2D 3D]
+        (default tree: $CDGPU_REFERENCE, else /root/reference)
 """
 import argparse
 import os
@@ -88,8 +89,11 @@ def defines(geo):
 def includes(ref):
     # EXT_LIB/tetgen holds only the tetgen *header* that include/Geometry/TetGenMeshLoader.h
     # pulls into Domain.C; no EXT_LIB binary is linked (tetgen calls resolve to abort-stubs).
+    # EXT_LIB/tecplot/include likewise only provides TECIO.h to Output2D.C / Output3D.C; the
+    # tecplot writer functions resolve to abort-stubs too
     return [f"-I{ref}/include/{d}" for d in INCLUDE_DIRS] + [f"-I{ref}/Examples",
-                                                            f"-I{ref}/EXT_LIB/tetgen"]
+                                                            f"-I{ref}/EXT_LIB/tetgen",
+                                                            f"-I{ref}/EXT_LIB/tecplot/include"]
 
 
 def compile_one(ref, geo, src, objdir):
@@ -139,9 +143,34 @@ def link_driver(ref, geo, lib, name, main_src):
     print(f"linked {exe}")
 
 
+def link_main(ref, geo, lib, name, main_src, gpu):
+    """Link the reference's own, unchanged main program (e.g. 3DPrograms/CD3D_ParMooN.C) against
+    the compiled reference; with gpu, the TSystemCD3D of parmoon_cmg_b200/shim (the
+    reference-side binding of libcdgpu) comes first on the link line, so the archive's
+    SystemCD3D object is not used and the program runs its assembly and solve on the GPU."""
+    drv = os.path.join(HERE, "ref_driver")
+    root = os.path.dirname(HERE)
+    exe = os.path.join(OUT, name)
+    srcs = [os.path.join(ref, main_src)]
+    libs = []
+    if gpu:
+        srcs.append(os.path.join(root, "parmoon_cmg_b200", "shim", "SystemCD3D_cdgpu.C"))
+        libs = [f"-L{os.path.join(root, 'parmoon_cmg_b200')}", "-lcdgpu",
+                "-Wl,-rpath,$ORIGIN/../../parmoon_cmg_b200"]
+    cmd = ["g++", "-O2", "-std=c++11", "-fpermissive", "-w"] + defines(geo) + includes(ref) + \
+          [f"-I{os.path.join(root, 'include')}"] + srcs + [os.path.join(drv, "stubs.C"),
+                                                        "-Wl,--start-group", lib, "-Wl,--end-group"] + \
+          libs + ["-lm", "-o", exe]
+    p = subprocess.run(cmd, capture_output=True, text=True)
+    if p.returncode != 0:
+        sys.stderr.write(p.stderr[-6000:])
+        raise SystemExit(f"link of {name} failed")
+    print(f"linked {exe}")
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("CDGPU_REFERENCE", "/root/reference"))
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--geo", nargs="*", default=["2D", "3D"])
     ap.add_argument("--link-only", action="store_true")
@@ -154,6 +183,11 @@ def main():
         if not a.link_only or not os.path.exists(lib):
             lib = build_geo(a.ref, geo, a.jobs)
         link_driver(a.ref, geo, lib, f"cd{geo.lower()}_dump", f"cd{geo.lower()}_dump.C")
+        if geo == "3D":
+            # the reference's CD3D main unchanged: on its own TSystemCD3D (CPU) and on libcdgpu
+            link_main(a.ref, geo, lib, "cd3d_main", "3DPrograms/CD3D_ParMooN.C", gpu=False)
+            if os.path.exists(os.path.join(os.path.dirname(HERE), "parmoon_cmg_b200", "libcdgpu.so")):
+                link_main(a.ref, geo, lib, "cd3d_main_gpu", "3DPrograms/CD3D_ParMooN.C", gpu=True)
 
 
 if __name__ == "__main__":

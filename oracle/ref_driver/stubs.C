@@ -24,6 +24,13 @@ CDGPU_STUB(dgemv_)
 CDGPU_STUB(pardiso_)
 CDGPU_STUB(pardisoinit_)
 CDGPU_STUB(triangulate)
+// tecplot writer (TOutput2D/3D::WriteTecplot); the header comes from EXT_LIB, the library does not
+CDGPU_STUB(tecini112)
+CDGPU_STUB(teczne112)
+CDGPU_STUB(tecdat112)
+CDGPU_STUB(tecnod112)
+CDGPU_STUB(tecend112)
+CDGPU_STUB(tecend)
 CDGPU_STUB(tetrahedralize)
 
 // UMFPACK-backed direct solver (src/FE/DirectSolver.C needs PARDISO/cblas headers and is

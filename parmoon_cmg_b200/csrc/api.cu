@@ -17,6 +17,17 @@ int cuda_fail(cdgpu_ctx *ctx, cudaError_t e, const char *what)
   return e == cudaErrorMemoryAllocation ? CDGPU_ERR_OOM : CDGPU_ERR_CUDA;
 }
 
+int ensure_err_flag(cdgpu_ctx *ctx)
+{
+  if (ctx->d_err) return CDGPU_OK;
+  int rc = dev_alloc(ctx, &ctx->d_err, 1);
+  if (rc) return rc;
+  CD_CUDA(ctx, cudaMallocHost((void **)&ctx->h_err, sizeof(int)));
+  *ctx->h_err = 0;
+  CD_CUDA(ctx, cudaMemset(ctx->d_err, 0, sizeof(int)));
+  return CDGPU_OK;
+}
+
 static Space *get_space(cdgpu_ctx *ctx, int id)
 {
   if (!ctx || id < 0 || id >= (int)ctx->spaces.size()) return nullptr;
@@ -32,7 +43,7 @@ static Hierarchy *get_mg(cdgpu_ctx *ctx, int id)
 static void free_space(Space *s)
 {
   if (!s) return;
-  void *ptrs[] = {s->d_coords, s->d_gn,  s->d_row_ptr, s->d_kcol,     s->d_dir_start, s->d_dir_rows, s->d_slot, s->d_inc_ptr,
+  void *ptrs[] = {s->d_coords, s->d_gn,  s->d_row_ptr, s->d_kcol,     s->d_dir_start, s->d_dir_rows, s->d_slot, s->d_inc_ptr, s->d_tiles,
                   s->d_inc,    s->d_a,   s->d_rhs,     s->d_diag,     s->d_a32,       s->d_diag32,
                   s->d_tab,    s->d_cellcoef, s->d_local, s->d_dir, s->d_ref, s->d_quadtab,
                   s->d_cf32,   s->d_R32, s->d_ybuf};
@@ -209,7 +220,7 @@ static int install_pattern(cdgpu_ctx *ctx, Space &s)
   }
   if (s.d_dir_rows) { cudaFree(s.d_dir_rows); s.d_dir_rows = nullptr; }
   s.n_dir_rows = (int)dir_rows.size();
-  if ((rc = dev_alloc(ctx, &s.d_row_ptr, s.n_dof + 1)) || (rc = dev_alloc(ctx, &s.d_kcol, s.nnz)) ||
+  if ((rc = dev_alloc(ctx, &s.d_row_ptr, s.n_dof + 1 + kCsrPad)) || (rc = dev_alloc(ctx, &s.d_kcol, s.nnz + kCsrPad)) ||
       (rc = dev_alloc(ctx, &s.d_dir_start, s.n_dof)) ||
       (rc = dev_alloc(ctx, &s.d_dir_rows, std::max<size_t>(1, dir_rows.size()))))
     return rc;
@@ -218,7 +229,10 @@ static int install_pattern(cdgpu_ctx *ctx, Space &s)
   CD_CUDA(ctx, cudaMemcpy(s.d_dir_start, dir_start.data(), sizeof(int) * s.n_dof, cudaMemcpyHostToDevice));
   if (!dir_rows.empty())
     CD_CUDA(ctx, cudaMemcpy(s.d_dir_rows, dir_rows.data(), sizeof(int) * dir_rows.size(), cudaMemcpyHostToDevice));
+  CD_CUDA(ctx, cudaMemset(s.d_row_ptr + s.n_dof + 1, 0, sizeof(int) * kCsrPad));
+  CD_CUDA(ctx, cudaMemset(s.d_kcol + s.nnz, 0, sizeof(int) * kCsrPad));
   s.shape = csr_shape(s.h_row_ptr.data(), s.n_dof);
+  if ((rc = build_csr_tiles(ctx, s))) return rc;
   // a new pattern invalidates values sized for the old one and the slot map
   s.slot_pattern = -1;
   s.pattern_checked = false;
@@ -392,6 +406,7 @@ int cdgpu_spmv(cdgpu_ctx *ctx, int space_id, const double *h_x, double *h_y)
   {
     CD_CUDA(ctx, cudaMemcpyAsync(h_y, dy, sizeof(double) * s->n_dof, cudaMemcpyDeviceToHost, ctx->stream));
     CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->d_err) rc = assemble_check(ctx); // wait flag of the bulk-copy product
   }
   cudaFree(dx);
   cudaFree(dy);
@@ -457,6 +472,7 @@ int cdgpu_defect(cdgpu_ctx *ctx, int space_id, const double *h_x, const double *
     CD_CUDA(ctx, cudaMemcpyAsync(h_d, dd, sizeof(double) * s->n_dof, cudaMemcpyDeviceToHost, ctx->stream));
     CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
+  if (!rc && ctx->d_err) rc = assemble_check(ctx); // wait flag of the bulk-copy product
   cudaFree(dx);
   cudaFree(df);
   cudaFree(dd);

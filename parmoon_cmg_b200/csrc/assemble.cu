@@ -634,6 +634,7 @@ int err_flag_status(cdgpu_ctx *ctx)
     CD_CUDA(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
     if (e == 1) return fail(ctx, CDGPU_ERR_PATTERN, "assemble: a cell coupling is missing from the CSR pattern");
     if (e == 3) return fail(ctx, CDGPU_ERR_CUDA, "multigrid: a tensor-core product did not complete in time");
+    if (e == 4) return fail(ctx, CDGPU_ERR_CUDA, "CSR product: a bulk copy of a matrix tile did not complete in time");
     return fail(ctx, CDGPU_ERR_UNSUPPORTED, "assemble: CSR row longer than the kernel's row buffer");
   }
   return CDGPU_OK;
@@ -765,7 +766,7 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, 
   }
   if (!s.d_a)
   {
-    if ((rc = dev_alloc(ctx, &s.d_a, s.nnz)) || (rc = dev_alloc(ctx, &s.d_a32, s.nnz)) ||
+    if ((rc = dev_alloc(ctx, &s.d_a, s.nnz + kCsrPad)) || (rc = dev_alloc(ctx, &s.d_a32, s.nnz + kCsrPad)) ||
         (rc = dev_alloc(ctx, &s.d_rhs, s.n_dof)) || (rc = dev_alloc(ctx, &s.d_diag, s.n_dof)) ||
         (rc = dev_alloc(ctx, &s.d_diag32, s.n_dof)))
       return rc;

@@ -256,3 +256,209 @@ inline void launch_csr(cdgpu_ctx *ctx, const CsrShape &sh, const CsrArgs<T> &pa,
     default: (void)cd_launch(csr_kernel<T, 32, 8, MODE>, grid, 256, 0, ctx->stream, p); break;
   }
 }
+
+// ---------------------------------------------------------------------------
+// FP64 CSR product / defect / Jacobi sweep with the matrix streamed into shared memory by the
+// bulk-copy engine (TMA, cp.async.bulk) for matrices too large for L2 (the finest level).
+//
+// The rows are cut once per pattern into tiles of at most kTmaRows rows and kTmaCap nonzeros
+// (CsrTiles, built on the host).  A persistent CTA takes tiles b, b + G, b + 2G, ...; one
+// producer thread copies each tile's row pointers, column indices and values into one of
+// kTmaStages shared-memory stages (three bulk copies completing on the stage's "full"
+// mbarrier), running up to kTmaStages - 1 tiles ahead; kTmaWarps consumer warps take 8 rows
+// each (4 threads per row), gather x, reduce, run the epilogue of csr_kernel, and release the
+// stage on its "empty" mbarrier.  The DRAM stream is the bulk copies alone, so it no longer
+// waits on the gathers' dependent loads.  A bulk copy must start on a 16-byte boundary and
+// move a multiple of 16 bytes: each copy starts at the tile's first element rounded down to a
+// multiple of 4 elements and ends rounded up (the arrays are allocated 8 elements longer).
+// Every mbarrier wait is bounded; on a timeout the kernel sets err = 4, stops, waits (bounded)
+// for the copies it issued and returns.
+// ---------------------------------------------------------------------------
+constexpr int kTmaRows = 64, kTmaCap = 2048, kTmaStages = 4, kTmaWarps = 8;
+constexpr int kTmaValsBytes = (kTmaCap + 8) * 8, kTmaColsBytes = (kTmaCap + 8) * 4;
+constexpr int kTmaRpBytes = ((kTmaRows + 1 + 8) * 4 + 127) / 128 * 128;
+constexpr int kTmaStageBytes = kTmaValsBytes + kTmaColsBytes + kTmaRpBytes;
+constexpr int kTmaSmem = kTmaStages * kTmaStageBytes + 256;
+constexpr long kTmaSpin = 1L << 22; // polls of one wait before it is declared timed out
+
+__device__ __forceinline__ uint32_t tma_smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool tma_try_wait(uint64_t *bar, uint32_t parity)
+{
+  uint32_t done;
+  asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+               "selp.b32 %0, 1, 0, P1;\n\t}"
+               : "=r"(done)
+               : "r"(tma_smem_u32(bar)), "r"(parity)
+               : "memory");
+  return done != 0;
+}
+
+// bounded wait; gives up early once another thread of the CTA has aborted
+__device__ __forceinline__ bool tma_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag)
+{
+  for (long it = 0; it < kTmaSpin; it++)
+  {
+    if (tma_try_wait(bar, parity)) return true;
+    if ((it & 255) == 255 && *abort_flag) return false;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   tma_smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(tma_smem_u32(bar))
+               : "memory");
+}
+
+struct TmaMeta
+{
+  int rb, re, rb0, nb0; // rows [rb, re); row-pointer and nonzero copies start at rb0, nb0
+};
+
+template <int MODE>
+__global__ void __launch_bounds__((kTmaWarps + 1) * 32) csr_tma_kernel(CsrArgs<double> p, const int2 *__restrict__ tiles,
+                                                                         int n_tiles, int *__restrict__ err)
+{
+  extern __shared__ __align__(128) unsigned char tma_sm[];
+  __shared__ __align__(8) uint64_t full[kTmaStages], empty[kTmaStages];
+  __shared__ TmaMeta meta[kTmaStages];
+  __shared__ int abort_s;
+  __shared__ double red[kTmaWarps];
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int G = gridDim.x;
+  const int my_tiles = blockIdx.x < n_tiles ? (n_tiles - 1 - blockIdx.x) / G + 1 : 0;
+  if (threadIdx.x == 0)
+  {
+    for (int s = 0; s < kTmaStages; s++)
+    {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tma_smem_u32(&full[s])), "r"(1));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tma_smem_u32(&empty[s])), "r"(kTmaWarps));
+    }
+    abort_s = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto stage_vals = [&](int s) { return (double *)(tma_sm + (size_t)s * kTmaStageBytes); };
+  auto stage_cols = [&](int s) { return (int *)(tma_sm + (size_t)s * kTmaStageBytes + kTmaValsBytes); };
+  auto stage_rp = [&](int s) { return (int *)(tma_sm + (size_t)s * kTmaStageBytes + kTmaValsBytes + kTmaColsBytes); };
+  double acc = 0;
+  if (warp == kTmaWarps)
+  {
+    // producer: one thread issues the copies of this CTA's tiles
+    if (lane == 0)
+    {
+      // the matrix is written by no kernel of a solve; with p.pre the first stages are issued
+      // before the wait for the predecessor (whose output x is only gathered by the consumers)
+      if (!p.pre) CD_PDL_WAIT();
+      int issued = 0;
+      for (int k = 0; k < my_tiles; k++)
+      {
+        const int s = k % kTmaStages, f = k / kTmaStages;
+        if (f > 0 && !tma_wait(&empty[s], (f - 1) & 1, &abort_s))
+        {
+          atomicExch(err, 4);
+          abort_s = 1;
+          break;
+        }
+        if (*(volatile int *)&abort_s) break;
+        const int t = blockIdx.x + k * G;
+        const int2 a = tiles[t], b = tiles[t + 1];
+        TmaMeta m;
+        m.rb = a.x;
+        m.re = b.x;
+        m.rb0 = a.x & ~3;
+        m.nb0 = a.y & ~3;
+        const int rp_n = ((b.x + 1 + 3) & ~3) - m.rb0; // row pointers rb0 .. re, rounded up
+        const int nz_n = ((b.y + 3) & ~3) - m.nb0;     // nonzeros nb0 .. ne, rounded up
+        meta[s] = m;
+        const uint32_t bytes = (uint32_t)(rp_n * 4 + nz_n * 12);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tma_smem_u32(&full[s])), "r"(bytes)
+                     : "memory");
+        tma_bulk_g2s(stage_rp(s), p.rp + m.rb0, rp_n * 4, &full[s]);
+        tma_bulk_g2s(stage_cols(s), p.kc + m.nb0, nz_n * 4, &full[s]);
+        tma_bulk_g2s(stage_vals(s), p.a + m.nb0, nz_n * 8, &full[s]);
+        issued = k + 1;
+        if (k == kTmaStages - 1 && p.pre) CD_PDL_WAIT();
+      }
+      if (p.pre && issued < kTmaStages) CD_PDL_WAIT();
+      CD_PDL_TRIGGER();
+      // no copy may still be in flight when the CTA exits: wait (bounded) for the last fill of
+      // every stage (returns at once for fills the consumers have already seen)
+      for (int s = 0; s < kTmaStages && s < issued; s++)
+      {
+        const int k_last = s + ((issued - 1 - s) / kTmaStages) * kTmaStages;
+        for (long it = 0; it < kTmaSpin && !tma_try_wait(&full[s], (k_last / kTmaStages) & 1); it++)
+          ;
+      }
+    }
+  }
+  else
+  {
+    CD_PDL_WAIT(); // x (and, in the Jacobi sweep, f) are read only after the predecessor completed
+    const int g = lane / 4, l4 = lane % 4;
+    for (int k = 0; k < my_tiles; k++)
+    {
+      const int s = k % kTmaStages, f = k / kTmaStages;
+      // every lane waits (each needs the acquire of the stage's data); the outcome is made
+      // warp-uniform, so a timeout never leaves part of the warp before the shuffles below
+      const bool arrived = tma_wait(&full[s], f & 1, &abort_s);
+      if (!__all_sync(0xffffffffu, arrived))
+      {
+        if (lane == 0)
+        {
+          atomicExch(err, 4);
+          abort_s = 1;
+        }
+        break;
+      }
+      const TmaMeta m = meta[s];
+      const double *va = stage_vals(s);
+      const int *co = stage_cols(s), *rs = stage_rp(s);
+      const int r = m.rb + warp * 8 + g;
+      double sum = 0;
+      if (r < m.re)
+      {
+        const int jb = rs[r - m.rb0] - m.nb0, je = rs[r + 1 - m.rb0] - m.nb0;
+        for (int j0 = jb + l4; j0 < je; j0 += 32)
+        {
+          int c[8];
+          double v[8];
+#pragma unroll
+          for (int u = 0; u < 8; u++)
+          {
+            const int j = j0 + 4 * u;
+            c[u] = j < je ? co[j] : -1;
+            v[u] = j < je ? va[j] : 0.0;
+          }
+          double xv[8];
+#pragma unroll
+          for (int u = 0; u < 8; u++) xv[u] = c[u] >= 0 ? __ldg(p.x + c[u]) : 0.0;
+#pragma unroll
+          for (int u = 0; u < 8; u++) sum += v[u] * xv[u];
+        }
+      }
+      sum = csr_group_sum<4>(sum);
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tma_smem_u32(&empty[s])) : "memory");
+      if (r < m.re && l4 == 0) csr_epilogue<double, MODE>(p, r, sum, acc);
+    }
+  }
+  if (MODE == CM_DEFECT && p.partial)
+  {
+    if (warp < kTmaWarps)
+    {
+      acc = csr_group_sum<32>(acc);
+      if (lane == 0) red[warp] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+      double tot = 0;
+      for (int w = 0; w < kTmaWarps; w++) tot += red[w];
+      p.partial[blockIdx.x] = tot;
+    }
+  }
+}

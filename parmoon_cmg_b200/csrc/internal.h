@@ -61,6 +61,11 @@ struct Space
   int *d_dir_rows = nullptr;  // the active rows that have Dirichlet columns
   int n_dir_rows = 0;
   CsrShape shape;
+  // tiles of the bulk-copy (TMA) FP64 product (csr.cuh, csr_tma_kernel): tile t covers rows
+  // [d_tiles[t].x, d_tiles[t+1].x) and nonzeros from d_tiles[t].y; n_tiles = 0 when the matrix
+  // keeps the plain CSR kernels (small, or a row longer than a tile)
+  int2 *d_tiles = nullptr;
+  int n_tiles = 0;
   // DOF -> (cell, local index) incidence, ascending cell per DOF
   int *d_inc_ptr = nullptr, *d_inc = nullptr;
   // slot map of the row gather: for incidence t of an active row and local column j, the
@@ -179,6 +184,12 @@ struct cdgpu_ctx
   int *h_err = nullptr;
 };
 
+// the device error flag (ctx->d_err) and its pinned host mirror, allocated on first use
+int ensure_err_flag(cdgpu_ctx *ctx);
+// CSR arrays are allocated this many elements longer than the pattern, so that the bulk
+// copies of the TMA product may round their end up to a 16-byte boundary
+constexpr int kCsrPad = 8;
+
 // error helpers: set ctx->err and return a status
 int fail(cdgpu_ctx *ctx, int status, const std::string &msg);
 int cuda_fail(cdgpu_ctx *ctx, cudaError_t e, const char *what);
@@ -265,5 +276,7 @@ int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m);
 int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *d_rhs,
               double *d_sol, cdgpu_solve_info *info);
 int apply_fp32_form(cdgpu_ctx *ctx, Space &s, int form, const float *d_x, float *d_y);
+// tiles of the TMA product for a freshly installed pattern (solve.cu)
+int build_csr_tiles(cdgpu_ctx *ctx, Space &s);
 // looks up the allocation-free defect's scratch array on a device (noalloc.cu)
 void noalloc_prepare(int device);

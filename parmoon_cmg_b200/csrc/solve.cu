@@ -473,6 +473,24 @@ template <typename T> static CsrArgs<T> csr_args(const Space &s, const T *x)
   p.x = x;
   return p;
 }
+// FP64 operations on a matrix with TMA tiles go through csr_tma_kernel: persistent CTAs, at
+// most two per SM (their shared-memory stages), never more than there are tiles
+static int tma_grid(const cdgpu_ctx *ctx, const Space &s) { return std::max(1, std::min(s.n_tiles, ctx->sm_count * 2)); }
+template <typename T, int MODE> static bool launch_tma(cdgpu_ctx *ctx, const Space &s, const CsrArgs<T> &pa, int grid)
+{
+  if constexpr (std::is_same<T, double>::value)
+  {
+    if (s.n_tiles > 0 && ctx->d_err)
+    {
+      CsrArgs<double> p = pa;
+      p.pre = ctx->pdl_pre ? 1 : 0;
+      (void)cd_launch(csr_tma_kernel<MODE>, grid, (kTmaWarps + 1) * 32, kTmaSmem, ctx->stream, p,
+                      (const int2 *)s.d_tiles, s.n_tiles, ctx->d_err);
+      return true;
+    }
+  }
+  return false;
+}
 template <typename T> static void csr_jacobi(cdgpu_ctx *ctx, const Space &s, const T *x, const T *f, T *xo, T omega)
 {
   CsrArgs<T> p = csr_args<T>(s, x);
@@ -480,8 +498,10 @@ template <typename T> static void csr_jacobi(cdgpu_ctx *ctx, const Space &s, con
   p.diag = dg<T>(s);
   p.y = xo;
   p.omega = omega;
+  if (launch_tma<T, CM_JACOBI>(ctx, s, p, tma_grid(ctx, s))) return;
   launch_csr<T, CM_JACOBI>(ctx, s.shape, p, csr_grid(ctx, s.shape, s.n_dof));
 }
+// grid: the launch's number of blocks (and of partial sums), from defect_grid
 template <typename T>
 static void csr_defect(cdgpu_ctx *ctx, const Space &s, const T *x, const T *f, T *d, double *partial, int grid)
 {
@@ -489,12 +509,19 @@ static void csr_defect(cdgpu_ctx *ctx, const Space &s, const T *x, const T *f, T
   p.f = f;
   p.y = d;
   p.partial = partial;
+  if (launch_tma<T, CM_DEFECT>(ctx, s, p, grid)) return;
   launch_csr<T, CM_DEFECT>(ctx, s.shape, p, grid);
+}
+template <typename T> static int defect_grid(const cdgpu_ctx *ctx, const Space &s)
+{
+  if (std::is_same<T, double>::value && s.n_tiles > 0 && ctx->d_err) return tma_grid(ctx, s);
+  return csr_grid(ctx, s.shape, s.n_dof);
 }
 template <typename T> static void csr_spmv(cdgpu_ctx *ctx, const Space &s, const T *x, T *y)
 {
   CsrArgs<T> p = csr_args<T>(s, x);
   p.y = y;
+  if (launch_tma<T, CM_SPMV>(ctx, s, p, tma_grid(ctx, s))) return;
   launch_csr<T, CM_SPMV>(ctx, s.shape, p, csr_grid(ctx, s.shape, s.n_dof));
 }
 // coarse rhs = R d (zero on non-active coarse rows), coarse solution reset
@@ -636,7 +663,7 @@ template <typename T> static int cycle(cdgpu_ctx *ctx, Hierarchy &h, CycleState 
       done = true;
     }
   }
-  if (!done) csr_defect<T>(ctx, s, v.sol, v.rhs, v.def, nullptr, csr_grid(ctx, s.shape, s.n_dof));
+  if (!done) csr_defect<T>(ctx, s, v.sol, v.rhs, v.def, nullptr, defect_grid<T>(ctx, s));
   CD_LAUNCHED(ctx);
   csr_restrict<T>(ctx, L, sc, v.def, vc.rhs, vc.sol);
   CD_LAUNCHED(ctx);
@@ -742,6 +769,39 @@ static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, 
                                ctx->stream));
   CD_CUDA(ctx, cudaGraphLaunch(h.gexec[k], ctx->stream));
   ctx->launches += h.graph_nodes[k];
+  return CDGPU_OK;
+}
+
+// Tiles of the TMA product: consecutive rows, at most kTmaRows rows and kTmaCap nonzeros per
+// tile, for matrices whose stream does not fit in L2 (smaller ones are latency-bound and keep
+// the plain kernels).  A row longer than kTmaCap leaves the matrix on the plain kernels.
+constexpr long kTmaMinNnz = 4L << 20;
+
+int build_csr_tiles(cdgpu_ctx *ctx, Space &s)
+{
+  if (s.d_tiles) { cudaFree(s.d_tiles); s.d_tiles = nullptr; }
+  s.n_tiles = 0;
+  if (s.nnz < kTmaMinNnz) return CDGPU_OK;
+  std::vector<int2> tiles;
+  const int *rp = s.h_row_ptr.data();
+  int r = 0;
+  while (r < s.n_dof)
+  {
+    if (rp[r + 1] - rp[r] > kTmaCap) return CDGPU_OK;
+    int e = r;
+    while (e < s.n_dof && e - r < kTmaRows && rp[e + 1] - rp[r] <= kTmaCap) e++;
+    tiles.push_back(make_int2(r, rp[r]));
+    r = e;
+  }
+  tiles.push_back(make_int2(s.n_dof, rp[s.n_dof]));
+  int rc;
+  if ((rc = ensure_err_flag(ctx))) return rc;
+  if ((rc = dev_alloc(ctx, &s.d_tiles, tiles.size()))) return rc;
+  CD_CUDA(ctx, cudaMemcpy(s.d_tiles, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
+  CD_CUDA(ctx, cudaFuncSetAttribute(csr_tma_kernel<CM_SPMV>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmem));
+  CD_CUDA(ctx, cudaFuncSetAttribute(csr_tma_kernel<CM_DEFECT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmem));
+  CD_CUDA(ctx, cudaFuncSetAttribute(csr_tma_kernel<CM_JACOBI>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmem));
+  s.n_tiles = (int)tiles.size() - 1;
   return CDGPU_OK;
 }
 
@@ -939,7 +999,7 @@ static int finest_defect_norm(cdgpu_ctx *ctx, Hierarchy &h, const double *x, con
                               double *norm_out_dev)
 {
   const Space &s = *h.lev.back().sp;
-  const int grid = csr_grid(ctx, s.shape, s.n_dof); // <= 8 blocks per SM, within d_partial
+  const int grid = defect_grid<double>(ctx, s); // <= 8 blocks per SM, within d_partial
   csr_defect<double>(ctx, s, x, f, d, h.d_partial, grid);
   CD_LAUNCHED(ctx);
   (void)cd_launch(sum_blocks_kernel, 1, 256, 0, ctx->stream, grid, h.d_partial, norm_out_dev);
@@ -957,7 +1017,7 @@ int spmv64(cdgpu_ctx *ctx, const Space &s, const double *x, double *y)
 int defect64(cdgpu_ctx *ctx, const Space &s, const double *x, const double *f, double *d, double *res)
 {
   int rc;
-  const int grid = csr_grid(ctx, s.shape, s.n_dof);
+  const int grid = defect_grid<double>(ctx, s);
   double *partial = nullptr, *out = nullptr;
   if ((rc = dev_alloc(ctx, &partial, grid)) || (rc = dev_alloc(ctx, &out, 1))) return rc;
   csr_defect<double>(ctx, s, x, f, d, partial, grid);
@@ -1287,9 +1347,10 @@ int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const 
       return fail(ctx, CDGPU_ERR_INVALID, "exact coarse solve: singular coarse matrix");
     }
   }
-  // tensor-core wait flag: FGMRES copied it back with its last synchronisation
-  if (rc == CDGPU_OK && p.precision == 1 && h.mf_mask)
-    rc = p.solver == 16 && ctx->h_err ? err_flag_status(ctx) : assemble_check(ctx);
+  // wait flags of the tensor-core and bulk-copy kernels: FGMRES copied the flag back with its
+  // last synchronisation
+  if (rc == CDGPU_OK && ctx->d_err && ctx->h_err)
+    rc = p.solver == 16 ? err_flag_status(ctx) : assemble_check(ctx);
   return rc;
 }
 

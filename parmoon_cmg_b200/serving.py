@@ -55,7 +55,9 @@ class Server:
 
     def run(self, requests, keep_solutions=False):
         """Replay the requests at their arrival times (seconds from the start); returns the
-        finished requests with 'latency', 'iterations', 'status'."""
+        finished requests with 'latency', 'iterations', 'status'.  keep_solutions: True, or a
+        predicate of the request, selects the requests whose solution is fetched into
+        r['solution']."""
         pending = sorted(requests, key=lambda r: r["t"])
         t0 = time.perf_counter()
         i = 0
@@ -74,11 +76,12 @@ class Server:
             tnow = time.perf_counter() - t0
             for slot in finished:
                 r = self.running.pop(slot)
-                x, info = self.batch.fetch(slot, r["n_dof_used"] if keep_solutions else 0)
+                keep = keep_solutions(r) if callable(keep_solutions) else keep_solutions
+                x, info = self.batch.fetch(slot, r["n_dof_used"] if keep else 0)
                 r["latency"] = tnow - r["t"]
                 r["iterations"] = info.iterations
                 r["status"] = info.status
-                if keep_solutions:
+                if keep:
                     r["solution"] = x
                 self.batch.release(slot)
                 self.done.append(r)

@@ -90,7 +90,12 @@ def test_golden_assembly(ctx, name):
         assert rel(rhs, L["rhs"]) <= TOL_ENTRIES
 
 
-@pytest.mark.parametrize("name", golden_names())
+# the solve needs a multigrid hierarchy: a single-level fixture would make its whole problem
+# the coarsest level, whose exact solve is a dense inverse in one thread block and whose
+# smoother loop is sequential; its entries and rhs are checked above, and the benchmark
+# coefficients it carries are solved at 32^3 against the oracle and the compiled reference
+# (test_gpu_headline.py)
+@pytest.mark.parametrize("name", [n for n in golden_names() if int(golden(n)["levels"]) > 1])
 def test_golden_solve(ctx, name):
     d = golden(name)
     dim, order, disc, lv, sids = setup_golden(ctx, d)
@@ -105,10 +110,7 @@ def test_golden_solve(ctx, name):
     rhs = fin["rhs"]  # the reference's right-hand side (checked bit-close above)
     sol0 = np.zeros(fin["n_dof"])
     sol0[fin["n_active"]:] = rhs[fin["n_active"]:]
-    # the exact coarse solve inverts the coarsest level densely in one thread block, which suits
-    # multigrid hierarchies; a single-level fixture (the whole problem is the coarsest level) is
-    # solved with the coarse SSOR loop as the preconditioner
-    for cs in ((17, 3, 1) if int(d["levels"]) > 1 else (3,)):
+    for cs in (17, 3, 1):
         prm = solver_params(red_factor=0.0, res_norm_min=1e-14 * np.linalg.norm(rhs), maxit=2000,
                             coarse_smoother=cs)
         sol, info = ctx.solve(mg, prm, rhs, sol0)
@@ -403,3 +405,26 @@ def test_solver_variants_vs_oracle(ctx, oracle_lib, solver, cycle):
     _, its1, _, _ = oracle_lib.solve(levels, oracle_lib.solver_params(red_factor=1e-10, **common), rhs, sol0)
     _, i1 = ctx.solve(mg, solver_params(red_factor=1e-10, **common), rhs, sol0)
     assert abs(i1.iterations - its1) <= (1 if solver == 11 else 2), (i1.iterations, its1)
+
+
+@pytest.mark.parametrize("n", [27, 32])
+def test_large_spmv_and_defect_vs_oracle(ctx, oracle_lib, n):
+    """Matrices too large for L2 (27^3 and 32^3 Q2: 9.6M and 15.8M nonzeros) take the product
+    whose matrix tiles are streamed into shared memory by bulk copies; product and defect
+    against the oracle's CSR product, and the defect norm."""
+    co = coeffs(0, eps=1e-2, b=(0.57735026918962573,) * 3, c=0.3, f=1.0)
+    sp = mesh.structured_space(3, 2, n)
+    sid = ctx.upload_space(sp)
+    nnz = ctx.build_pattern(sid)
+    ctx.set_coeffs(sid, co)
+    ent, rhs = ctx.assemble(sid, 1, sp["n_dof"], nnz)
+    rp, kc = ctx.get_pattern(sid, sp["n_dof"], nnz)
+    rng = np.random.default_rng(n)
+    for _ in range(2):
+        x = rng.standard_normal(sp["n_dof"])
+        y_o = oracle_lib.spmv(rp, kc, ent, x)
+        y = ctx.spmv(sid, x)
+        assert rel(y, y_o) <= 1e-13
+        dd, res = ctx.defect(sid, x, rhs)
+        assert rel(dd, rhs - y_o) <= 1e-12
+        assert abs(res - np.linalg.norm(rhs - y_o)) <= 1e-12 * np.linalg.norm(rhs - y_o)
