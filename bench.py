@@ -543,8 +543,10 @@ def run_batched(ctx, args):
         errs.append(float(np.abs(x - ref).max() / np.abs(ref).max()))
     for sl in slots:
         B.release(sl)
+    cpu = None if args.no_cpu_baseline else batched_cpu_baseline(work)
     return {
         "metric": "batched CD2D solves/s", "value": len(work) / t_total, "unit": "solves/s",
+        "cpu_baseline": cpu,
         "instances": len(work), "wall_s": t_total, "submit_s": t_submit,
         "dofs_total": int(sum(W.dofs(2, w["order"], w["n_used"]) for w in work)),
         "device_bytes": int(need), "structures": len(cache.ids),
@@ -596,6 +598,79 @@ def run_serving(ctx, args):
                       "nearest admissible mesh, eps 10^U(-6,-1), random unit b, f=1, Dirichlet 0, SUPG; "
                       f"{args.serving_requests} requests per rate, seed 20261204; error sample against the "
                       "oracle's FP64 assembly solved directly"}
+
+
+BATCH_DAT = """VERSION: 1
+LOGFILE: logfile
+OUTFILE: {out}
+BNDFILE: {mesh}/unit_square.PRM
+GEOFILE: {mesh}/unit_square.GEO
+MESH_TYPE: 0
+UNIFORM_STEPS: {steps}
+LEVELS: {levels}
+ANSATZ_ORDER: {order}
+DISCTYPE: 2
+SOLVER_TYPE: 1
+SC_SOLVER_SCALAR: 16
+SC_PRECONDITIONER_SCALAR: 5
+SC_SMOOTHER_SCALAR: 3
+SC_COARSE_SMOOTHER_SCALAR: 3
+SC_SMOOTH_DAMP_FACTOR_SCALAR: 1.0
+SC_SMOOTH_DAMP_FACTOR_FINE_SCALAR: 1.0
+SC_PRE_SMOOTH_SCALAR: 2
+SC_POST_SMOOTH_SCALAR: 2
+SC_MG_CYCLE_SCALAR: 1
+SC_STEP_LENGTH_CONTROL_ALL_SCALAR: 0
+SC_STEP_LENGTH_CONTROL_FINE_SCALAR: 0
+SC_GMRES_RESTART: 30
+SC_LIN_RED_FACTOR_SCALAR: 1e-10
+SC_LIN_RES_NORM_MIN_SCALAR: 0
+SC_LIN_MAXIT_SCALAR: 300
+SC_VERBOSE: 0
+"""
+
+
+def batched_cpu_baseline(work, sample_size=16):
+    """cpu_baseline of the batched workload: the reference's own 2D multigrid FGMRES
+    (oracle/_ref/cd2d_dump: TSystemCD2D assembly + TMultiGrid2D / TFgmresIte, lexicographic SSOR
+    V(2,2), SSOR coarse smoother) on a seeded sample of the instances whose mesh the reference's
+    unit-square refinement produces (N a power of two), one process per host core; solves/s =
+    sample / wall time of the concurrent runs."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "cd2d_dump")
+    if not os.path.exists(exe):
+        return {"value": None, "sample": "unavailable: oracle/_ref/cd2d_dump not built"}
+    rng = np.random.default_rng(20261206)
+    pick = [i for i, w in enumerate(work) if w["n0"] in (2, 4)]
+    sample = sorted(rng.choice(pick, size=min(sample_size, len(pick)), replace=False).tolist())
+    cores = cpu_count()
+    tmp = tempfile.mkdtemp()
+    try:
+        cmds = []
+        for k, i in enumerate(sample):
+            w = work[i]
+            dat = os.path.join(tmp, f"b{k}.dat")
+            with open(dat, "w") as f:
+                f.write(BATCH_DAT.format(out=os.path.join(tmp, f"b{k}.out"), mesh=os.path.join(ROOT, "oracle", "meshes"),
+                                         steps=int(round(np.log2(w["n0"]))), levels=w["levels"], order=w["order"]))
+            cmds.append([exe, dat, "-", "0", repr(w["eps"]), repr(w["b"][0]), repr(w["b"][1]), "0", "1"])
+        t0 = time.perf_counter()
+        running, outs = [], []
+        pending = list(cmds)
+        while pending or running:
+            while pending and len(running) < cores:
+                running.append(subprocess.Popen(pending.pop(0), cwd=tmp, stdout=subprocess.PIPE,
+                                                stderr=subprocess.DEVNULL, text=True))
+            p = running.pop(0)
+            outs.append(json.loads([l for l in p.communicate()[0].splitlines() if l.startswith("{")][-1]))
+        wall = time.perf_counter() - t0
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    its = [o["iterations"] for o in outs]
+    return {"value": len(sample) / wall, "unit": "solves/s", "cores": min(cores, len(sample)), "kind": "reference",
+            "sample": f"{len(sample)} seeded instances with N a power of two (N = {sorted(set(work[i]['n_used'] for i in sample))}), "
+                      f"one reference process per core, wall {wall:.1f} s including mesh and structure set-up",
+            "iterations": {"median": float(np.median(its)), "max": int(max(its)),
+                           "at_maxit_300": int(sum(1 for x in its if x >= 300))}}
 
 
 def fp64_solution(dim, order, n, eps, b):

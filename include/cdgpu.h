@@ -127,6 +127,11 @@ int cdgpu_upload_space(cdgpu_ctx *ctx, int dim, int order, int n_cells, const do
 int cdgpu_build_pattern(cdgpu_ctx *ctx, int space_id, int *nnz);
 int cdgpu_upload_pattern(cdgpu_ctx *ctx, int space_id, const int *h_row_ptr, const int *h_kcol,
                          int nnz);
+/* The same pattern as cdgpu_build_pattern, built on the device (one warp per row sorts the
+ * DOFs of the row's cells; row lengths, a scan, then the columns), for callers that set up
+ * many meshes (a request loop's new mesh sizes).  Bit-identical to the host build, which it
+ * falls back to for rows with more than 512 candidate columns. */
+int cdgpu_build_pattern_device(cdgpu_ctx *ctx, int space_id, int *nnz);
 int cdgpu_get_pattern(cdgpu_ctx *ctx, int space_id, int *h_row_ptr, int *h_kcol);
 
 /* --- coefficients ----------------------------------------------------------
@@ -148,6 +153,14 @@ int cdgpu_quadrature_points(cdgpu_ctx *ctx, int space_id, double *h_xyz, int *n_
  * whose coefficients are of kind CDGPU_COEFF_SINE have this exact solution; others return
  * CDGPU_ERR_UNSUPPORTED. */
 int cdgpu_errors(cdgpu_ctx *ctx, int space_id, const double *h_sol, double *l2, double *h1semi);
+/* The same errors against any exact solution, for the MEASURE_ERRORS branch of the mains
+ * (TFEFunction3D::GetErrors with L2H1Errors, src/FE/FEFunction3D.C:57; 2D FEFunction2D.C:73):
+ * the host tabulates the example's Exact() at the points of cdgpu_quadrature_points,
+ * h_exact = n_cells x n_quad x (1 + dim) doubles (u, du/dx, du/dy[, du/dz]); the device
+ * evaluates u_h and grad u_h there and sums w |det J| (u_h - u)^2 and |grad(u_h - u)|^2.
+ * h_sol: the full solution (n_dof values).  2D and 3D, Q1 and Q2. */
+int cdgpu_errors_table(cdgpu_ctx *ctx, int space_id, const double *h_sol, const double *h_exact, double *l2,
+                       double *h1semi);
 
 /* --- assembly ---------------------------------------------------------------
  * Replaces TSystemCD3D::Assemble / TAssembleMat3D::Reset + Assemble3D

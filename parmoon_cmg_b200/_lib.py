@@ -57,6 +57,7 @@ SIGNATURES = {
     "cdgpu_upload_space": (_I, [_P, _I, _I, _I, _P, _P, _P, _I, _I, _I, C.POINTER(_I)]),
     "cdgpu_build_pattern": (_I, [_P, _I, C.POINTER(_I)]),
     "cdgpu_upload_pattern": (_I, [_P, _I, _P, _P, _I]),
+    "cdgpu_build_pattern_device": (_I, [_P, _I, C.POINTER(_I)]),
     "cdgpu_get_pattern": (_I, [_P, _I, _P, _P]),
     "cdgpu_set_coeffs": (_I, [_P, _I, C.POINTER(Coeffs), _P]),
     "cdgpu_quadrature_points": (_I, [_P, _I, _P, C.POINTER(_I)]),
@@ -65,6 +66,7 @@ SIGNATURES = {
     "cdgpu_spmv": (_I, [_P, _I, _P, _P]),
     "cdgpu_defect": (_I, [_P, _I, _P, _P, _P, C.POINTER(C.c_double)]),
     "cdgpu_errors": (_I, [_P, _I, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "cdgpu_errors_table": (_I, [_P, _I, _P, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "cdgpu_spmv_device": (_I, [_P, _I, _P, _P]),
     "cdgpu_apply_fp32": (_I, [_P, _I, _I, _P, _P]),
     "cdgpu_defect_noalloc": (_I, [_P, _I, _P, _P, _P, C.POINTER(C.c_double)]),

@@ -206,7 +206,9 @@ int cdgpu_upload_space(cdgpu_ctx *ctx, int dim, int order, int n_cells, const do
   return CDGPU_OK;
 }
 
-static int install_pattern(cdgpu_ctx *ctx, Space &s)
+// d_kcol_built: the columns already on the device (built there, nnz + kCsrPad entries; the
+// space takes ownership), else they are uploaded from s.h_kcol
+static int install_pattern(cdgpu_ctx *ctx, Space &s, int *d_kcol_built = nullptr)
 {
   int rc;
   s.nnz = s.h_row_ptr[s.n_dof];
@@ -220,12 +222,19 @@ static int install_pattern(cdgpu_ctx *ctx, Space &s)
   }
   if (s.d_dir_rows) { cudaFree(s.d_dir_rows); s.d_dir_rows = nullptr; }
   s.n_dir_rows = (int)dir_rows.size();
-  if ((rc = dev_alloc(ctx, &s.d_row_ptr, s.n_dof + 1 + kCsrPad)) || (rc = dev_alloc(ctx, &s.d_kcol, s.nnz + kCsrPad)) ||
+  if (d_kcol_built)
+  {
+    if (s.d_kcol) cudaFree(s.d_kcol);
+    s.d_kcol = d_kcol_built;
+  }
+  if ((rc = dev_alloc(ctx, &s.d_row_ptr, s.n_dof + 1 + kCsrPad)) ||
+      (!d_kcol_built && (rc = dev_alloc(ctx, &s.d_kcol, s.nnz + kCsrPad))) ||
       (rc = dev_alloc(ctx, &s.d_dir_start, s.n_dof)) ||
       (rc = dev_alloc(ctx, &s.d_dir_rows, std::max<size_t>(1, dir_rows.size()))))
     return rc;
   CD_CUDA(ctx, cudaMemcpy(s.d_row_ptr, s.h_row_ptr.data(), sizeof(int) * (s.n_dof + 1), cudaMemcpyHostToDevice));
-  CD_CUDA(ctx, cudaMemcpy(s.d_kcol, s.h_kcol.data(), sizeof(int) * s.nnz, cudaMemcpyHostToDevice));
+  if (!d_kcol_built)
+    CD_CUDA(ctx, cudaMemcpy(s.d_kcol, s.h_kcol.data(), sizeof(int) * s.nnz, cudaMemcpyHostToDevice));
   CD_CUDA(ctx, cudaMemcpy(s.d_dir_start, dir_start.data(), sizeof(int) * s.n_dof, cudaMemcpyHostToDevice));
   if (!dir_rows.empty())
     CD_CUDA(ctx, cudaMemcpy(s.d_dir_rows, dir_rows.data(), sizeof(int) * dir_rows.size(), cudaMemcpyHostToDevice));
@@ -251,6 +260,21 @@ int cdgpu_build_pattern(cdgpu_ctx *ctx, int space_id, int *nnz)
   build_pattern(*s, s->h_row_ptr, s->h_kcol);
   int rc = install_pattern(ctx, *s);
   if (rc) return rc;
+  if (nnz) *nnz = (int)s->nnz;
+  return CDGPU_OK;
+}
+
+int cdgpu_build_pattern_device(cdgpu_ctx *ctx, int space_id, int *nnz)
+{
+  Space *s = get_space(ctx, space_id);
+  if (!s) return fail(ctx, CDGPU_ERR_INVALID, "build_pattern_device: bad space id");
+  cudaSetDevice(ctx->device);
+  int *d_kcol = nullptr;
+  bool fallback = false;
+  int rc = build_pattern_device(ctx, *s, &d_kcol, &fallback);
+  if (rc) return rc;
+  if (fallback) build_pattern(*s, s->h_row_ptr, s->h_kcol); // a row beyond the kernel's buffer
+  if ((rc = install_pattern(ctx, *s, d_kcol))) return rc;
   if (nnz) *nnz = (int)s->nnz;
   return CDGPU_OK;
 }
@@ -452,6 +476,34 @@ int cdgpu_errors(cdgpu_ctx *ctx, int space_id, const double *h_sol, double *l2, 
   rc = e == cudaSuccess ? space_errors_sine(ctx, *s, du, l2, h1semi) : cuda_fail(ctx, e, "errors: copy");
   cudaStreamSynchronize(ctx->stream);
   cudaFree(du);
+  return rc;
+}
+
+int cdgpu_errors_table(cdgpu_ctx *ctx, int space_id, const double *h_sol, const double *h_exact, double *l2,
+                       double *h1semi)
+{
+  Space *s = get_space(ctx, space_id);
+  if (!s || !h_sol || !h_exact || !l2 || !h1semi) return fail(ctx, CDGPU_ERR_INVALID, "errors_table: bad argument");
+  cudaSetDevice(ctx->device);
+  if (!s->re_ready)
+  {
+    make_ref_element(s->dim, s->order, s->re);
+    s->re_ready = true;
+  }
+  const size_t ne = (size_t)s->n_cells * s->re.nq * (1 + s->dim);
+  double *du = nullptr, *dex = nullptr;
+  int rc;
+  if ((rc = dev_alloc(ctx, &du, s->n_dof)) || (rc = dev_alloc(ctx, &dex, ne)))
+  {
+    if (du) cudaFree(du);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpyAsync(du, h_sol, sizeof(double) * s->n_dof, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dex, h_exact, sizeof(double) * ne, cudaMemcpyHostToDevice, ctx->stream);
+  rc = e == cudaSuccess ? space_errors_table(ctx, *s, du, dex, l2, h1semi) : cuda_fail(ctx, e, "errors_table: copy");
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(du);
+  cudaFree(dex);
   return rc;
 }
 

@@ -722,6 +722,105 @@ __global__ void __launch_bounds__(256) errors_sine_kernel(int n_cells, int nbf, 
   }
 }
 
+// The same errors against any exact solution the host tabulates at the assembly's quadrature
+// points (TFEFunction2D/3D::GetErrors with L2H1Errors, src/FE/FEFunction2D.C:73,
+// src/FE/FEFunction3D.C:57): ex[(c*nq + q)*(1+dim) + k] = u, du/dx, du/dy[, du/dz] at point q
+// of cell c (the points of cdgpu_quadrature_points); 2D and 3D, any supported element.
+__global__ void __launch_bounds__(256) errors_table_kernel(int dim, int n_cells, int nbf, int nq, int nv,
+                                                           int affine_all, const double *__restrict__ coords,
+                                                           const int *__restrict__ gn, const double *__restrict__ qx,
+                                                           const double *__restrict__ qw,
+                                                           const double *__restrict__ phi,
+                                                           const double *__restrict__ dphi,
+                                                           const double *__restrict__ u,
+                                                           const double *__restrict__ ex,
+                                                           double *__restrict__ partial)
+{
+  CD_PDL_ENTRY();
+  __shared__ double red[2][8];
+  double e0 = 0.0, e1 = 0.0;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cells; c += gridDim.x * blockDim.x)
+  {
+    double V[24];
+    for (int k = 0; k < nv * dim; k++) V[k] = coords[(size_t)c * nv * dim + k];
+    for (int q = 0; q < nq; q++)
+    {
+      double x[3], J[9], Ji[9];
+      d_ref_map(dim, nv, affine_all != 0, V, qx + dim * q, x, J);
+      const double det = d_invert(dim, J, Ji);
+      double uh = 0.0, g[3] = {0.0, 0.0, 0.0};
+      for (int b = 0; b < nbf; b++)
+      {
+        const double *gr = dphi + (size_t)(q * nbf + b) * dim;
+        const double ub = u[gn[(size_t)c * nbf + b]];
+        uh += ub * phi[q * nbf + b];
+        for (int r = 0; r < dim; r++)
+        {
+          double s = 0.0;
+          for (int e = 0; e < dim; e++) s += Ji[e * dim + r] * gr[e];
+          g[r] += ub * s;
+        }
+      }
+      const double *xq = ex + ((size_t)c * nq + q) * (1 + dim);
+      const double w = qw[q] * fabs(det);
+      e0 += w * (uh - xq[0]) * (uh - xq[0]);
+      double s1 = 0.0;
+      for (int r = 0; r < dim; r++) s1 += (g[r] - xq[1 + r]) * (g[r] - xq[1 + r]);
+      e1 += w * s1;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1)
+  {
+    e0 += __shfl_xor_sync(0xffffffffu, e0, o);
+    e1 += __shfl_xor_sync(0xffffffffu, e1, o);
+  }
+  if (threadIdx.x % 32 == 0)
+  {
+    red[0][threadIdx.x / 32] = e0;
+    red[1][threadIdx.x / 32] = e1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < 8; w++) { a += red[0][w]; b += red[1][w]; }
+    partial[2 * blockIdx.x] = a;
+    partial[2 * blockIdx.x + 1] = b;
+  }
+}
+
+int space_errors_table(cdgpu_ctx *ctx, Space &s, const double *d_u, const double *d_ex, double *l2, double *h1semi)
+{
+  int rc;
+  if (!s.re_ready)
+  {
+    make_ref_element(s.dim, s.order, s.re);
+    s.re_ready = true;
+  }
+  if ((rc = ensure_quadtab(ctx, s))) return rc;
+  const RefElement &re = s.re;
+  const double *qx = s.d_quadtab, *qw = qx + re.qx.size(), *phi = qw + re.qw.size(), *dphi = phi + re.phi.size();
+  const int grid = std::max(1, std::min((s.n_cells + 255) / 256, ctx->sm_count * 4));
+  double *d_partial = nullptr;
+  if ((rc = dev_alloc(ctx, &d_partial, (size_t)2 * grid))) return rc;
+  (void)cd_launch(errors_table_kernel, grid, 256, 0, ctx->stream, s.dim, s.n_cells, s.nbf, re.nq, s.nv,
+                  s.all_affine ? 1 : 0, (const double *)s.d_coords, (const int *)s.d_gn, qx, qw, phi, dphi, d_u,
+                  d_ex, d_partial);
+  cudaError_t e = cudaGetLastError();
+  std::vector<double> part((size_t)2 * grid);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(part.data(), d_partial, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d_partial);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "errors_table");
+  CD_LAUNCHED(ctx);
+  double a = 0.0, b = 0.0;
+  for (int i = 0; i < grid; i++) { a += part[2 * i]; b += part[2 * i + 1]; }
+  *l2 = std::sqrt(a);
+  *h1semi = std::sqrt(b);
+  return CDGPU_OK;
+}
+
 int space_errors_sine(cdgpu_ctx *ctx, Space &s, const double *d_u, double *l2, double *h1semi)
 {
   if (s.dim != 2 || !s.co_set || s.co.kind != CDGPU_COEFF_SINE)

@@ -265,6 +265,8 @@ bool dense_inverse(int n, std::vector<double> &a); // in place, row-major; false
 int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, bool check = true);
 // L2 and H1-semi errors against the SineLaplace solution (2D, coefficient kind SINE)
 int space_errors_sine(cdgpu_ctx *ctx, Space &s, const double *d_u, double *l2, double *h1semi);
+// the same against an exact solution tabulated at the quadrature points (u and its gradient)
+int space_errors_table(cdgpu_ctx *ctx, Space &s, const double *d_u, const double *d_ex, double *l2, double *h1semi);
 int assemble_check(cdgpu_ctx *ctx);
 int err_flag_status(cdgpu_ctx *ctx);
 int add_neumann(cdgpu_ctx *ctx, Space &s, int n_edges, const int *cell, const int *edge,
@@ -276,6 +278,8 @@ int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m);
 int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *d_rhs,
               double *d_sol, cdgpu_solve_info *info);
 int apply_fp32_form(cdgpu_ctx *ctx, Space &s, int form, const float *d_x, float *d_y);
+// the CSR pattern built on the device (pattern.cu)
+int build_pattern_device(cdgpu_ctx *ctx, Space &s, int **d_kcol_out, bool *fallback);
 // tiles of the TMA product for a freshly installed pattern (solve.cu)
 int build_csr_tiles(cdgpu_ctx *ctx, Space &s);
 // looks up the allocation-free defect's scratch array on a device (noalloc.cu)

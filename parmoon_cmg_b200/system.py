@@ -87,6 +87,12 @@ class Context:
         self.check(self.lib.cdgpu_build_pattern(self.h, sid, C.byref(nnz)))
         return nnz.value
 
+    def build_pattern_device(self, sid):
+        """The CSR pattern built on the device (bit-identical to build_pattern)."""
+        nnz = C.c_int()
+        self.check(self.lib.cdgpu_build_pattern_device(self.h, sid, C.byref(nnz)))
+        return nnz.value
+
     def upload_pattern(self, sid, row_ptr, kcol):
         row_ptr, kcol = _i32(row_ptr), _i32(kcol)
         self.check(self.lib.cdgpu_upload_pattern(self.h, sid, _p(row_ptr), _p(kcol), len(kcol)))
@@ -119,6 +125,14 @@ class Context:
         """(L2, H1-semi) errors of ``sol`` against the SineLaplace solution, on the device."""
         l2, h1 = C.c_double(), C.c_double()
         self.check(self.lib.cdgpu_errors(self.h, sid, _p(_f64(sol)), C.byref(l2), C.byref(h1)))
+        return l2.value, h1.value
+
+    def errors_table(self, sid, sol, exact):
+        """(L2, H1-semi) errors of ``sol`` against an exact solution tabulated at the
+        quadrature points: exact[cell, q] = (u, du/dx, du/dy[, du/dz]), on the device."""
+        l2, h1 = C.c_double(), C.c_double()
+        self.check(self.lib.cdgpu_errors_table(self.h, sid, _p(_f64(sol)), _p(_f64(exact)), C.byref(l2),
+                                               C.byref(h1)))
         return l2.value, h1.value
 
     def add_neumann(self, sid, cells, edges, g, n_dof=None):
@@ -376,7 +390,8 @@ class Batch:
     def add_structure(self, spaces, parents):
         """Upload a hierarchy (spaces coarsest first); returns its structure id."""
         sids = [self.ctx.upload_space(s) for s in spaces]
-        nnz = [self.ctx.build_pattern(sid) for sid in sids]
+        # the patterns of a new mesh are built on the device (bit-identical to the host build)
+        nnz = [self.ctx.build_pattern_device(sid) for sid in sids]
         mg = self.ctx.hierarchy(sids, parents)
         self.structures.append(dict(mg=mg, n_dof=int(spaces[-1]["n_dof"]), sids=sids, nnz=nnz))
         return len(self.structures) - 1

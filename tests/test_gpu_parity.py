@@ -428,3 +428,62 @@ def test_large_spmv_and_defect_vs_oracle(ctx, oracle_lib, n):
         dd, res = ctx.defect(sid, x, rhs)
         assert rel(dd, rhs - y_o) <= 1e-12
         assert abs(res - np.linalg.norm(rhs - y_o)) <= 1e-12 * np.linalg.norm(rhs - y_o)
+
+
+def test_errors_table_equals_sine_errors(ctx):
+    """The tabulated-exact-solution error evaluation agrees with the SineLaplace one (the
+    reference's recorded known answer) on the same solution."""
+    d = golden("cd2d_q1_sine_32")
+    dim, order, disc, lv, sids = setup_golden(ctx, d)
+    fin = lv[-1]
+    x = d["solution"]
+    l2s, h1s = ctx.errors(sids[-1], x)
+    nc = len(fin["begin_index"]) - 1
+    q = ctx.quadrature_points(sids[-1], nc, 2)
+    s, c = np.sin(np.pi * q), np.cos(np.pi * q)
+    ex = np.stack([s[..., 0] * s[..., 1], np.pi * c[..., 0] * s[..., 1], np.pi * s[..., 0] * c[..., 1]], -1)
+    l2, h1 = ctx.errors_table(sids[-1], x, ex)
+    assert abs(l2 - l2s) <= 1e-12 * l2s and abs(h1 - h1s) <= 1e-12 * h1s
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_device_pattern_equals_reference(ctx, name):
+    """The CSR pattern built on the device (cdgpu_build_pattern_device) is the reference's
+    TSquareStructure + Sort, bit for bit, on every level of every fixture (the non-affine meshes
+    and the reference's own DOF numbering included)."""
+    d = golden(name)
+    dim, order = int(d["dim"]), int(d["order"])
+    for l in range(int(d["levels"])):
+        L = refdump.level(d, l)
+        sid = ctx.upload_space(dict(dim=dim, order=order, coords=L["coords"], global_numbers=L["global_numbers"],
+                                    begin_index=L["begin_index"], n_dof=L["n_dof"], n_active=L["n_active"]))
+        nnz = ctx.build_pattern_device(sid)
+        assert nnz == len(L["kcol"])
+        rp, kc = ctx.get_pattern(sid, L["n_dof"], nnz)
+        assert np.array_equal(rp, L["row_ptr"]) and np.array_equal(kc, L["kcol"])
+
+
+@pytest.mark.parametrize("dim,order,n", [(3, 2, 32), (3, 1, 48), (2, 2, 256), (2, 1, 300)])
+def test_device_pattern_equals_host_build(ctx, dim, order, n):
+    """Large structured meshes: device build == host build, and the device build's matrix
+    assembles and multiplies like the host build's."""
+    import time
+    sp = mesh.structured_space(dim, order, n)
+    a = ctx.upload_space(sp)
+    b = ctx.upload_space(sp)
+    t0 = time.perf_counter()
+    nnz_h = ctx.build_pattern(a)
+    t1 = time.perf_counter()
+    nnz_d = ctx.build_pattern_device(b)
+    t2 = time.perf_counter()
+    print(f"{dim}D Q{order} n={n}: host build {1e3 * (t1 - t0):.1f} ms, device build {1e3 * (t2 - t1):.1f} ms")
+    assert nnz_h == nnz_d
+    ra, ka = ctx.get_pattern(a, sp["n_dof"], nnz_h)
+    rb, kb = ctx.get_pattern(b, sp["n_dof"], nnz_d)
+    assert np.array_equal(ra, rb) and np.array_equal(ka, kb)
+    co = coeffs(0, eps=1e-2, b=(0.3, 0.2, 0.1)[:dim], f=1.0)
+    ctx.set_coeffs(a, co)
+    ctx.set_coeffs(b, co)
+    ea, _ = ctx.assemble(a, 1, sp["n_dof"], nnz_h)
+    eb, _ = ctx.assemble(b, 1, sp["n_dof"], nnz_d)
+    assert np.array_equal(ea, eb)

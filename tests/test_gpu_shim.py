@@ -137,3 +137,58 @@ def laplace_oracle_solution(oracle):
     prm = oracle.solver_params(red_factor=0.0, res_norm_min=1e-14 * np.linalg.norm(rhs), maxit=300)
     x, _, _, _ = oracle.solve(levels, prm, rhs, sol0)
     return x
+
+
+def test_errors_table_reproduces_reference_output(cpu_errors):
+    """GetErrors on the device for any exact solution (cdgpu_errors_table): the Laplace example
+    solved through the C ABI on the reference's own mesh and DOF numbering gives the L2 and
+    H1-semi errors that the reference's CD3D main prints, digit for digit."""
+    import refdump
+    from parmoon_cmg_b200 import _build, _lib
+    from parmoon_cmg_b200.system import Context, coeffs, solver_params
+    _build.build()
+    with tempfile.TemporaryDirectory() as tmp:
+        dat = os.path.join(tmp, "d.dat")
+        with open(dat, "w") as f:
+            f.write(DAT.format(out=os.path.join(tmp, "d.out"), mesh=os.path.join(ROOT, "oracle", "meshes")))
+        out = os.path.join(tmp, "dump")
+        os.makedirs(out)
+        subprocess.run([os.path.join(REF, "cd3d_dump"), dat, out, "1", "0", "0", "0", "0", "0", "0"], cwd=tmp,
+                       check=True, capture_output=True)
+        d = refdump.load_dir(out)
+    lv = [refdump.level(d, l) for l in range(int(d["levels"]))]
+    ctx = Context(0)
+    try:
+        sids = []
+        for S in lv:
+            sid = ctx.upload_space(dict(dim=3, order=2, coords=S["coords"], global_numbers=S["global_numbers"],
+                                        begin_index=S["begin_index"], n_dof=S["n_dof"], n_active=S["n_active"]))
+            ctx.build_pattern(sid)
+            nc = len(S["begin_index"]) - 1
+            q = ctx.quadrature_points(sid, nc, 3)
+            tab = np.zeros(q.shape[:2] + (6,))
+            tab[..., 0] = 1.0
+            tab[..., 5] = 3 * np.pi ** 2 * np.prod(np.sin(np.pi * q), axis=-1)
+            ctx.set_coeffs(sid, coeffs(_lib.COEFF_TABLE), tab)
+            sids.append(sid)
+        mg = ctx.hierarchy(sids, [None] + [S["parent"] for S in lv[1:]])
+        import oracle
+        rhs = None
+        for S, sid in zip(lv, sids):
+            xyz = oracle.dof_coords(3, 2, S["coords"], S["global_numbers"], S["begin_index"], S["n_dof"])
+            g = np.prod(np.sin(np.pi * xyz[S["n_active"]:]), axis=-1)
+            _, rhs = ctx.assemble(sid, 1, S["n_dof"], 1, dirichlet=g, want_entries=False)
+        fin = lv[-1]
+        sol0 = np.zeros(fin["n_dof"])
+        sol0[fin["n_active"]:] = rhs[fin["n_active"]:]
+        x, info = ctx.solve(mg, solver_params(coarse_smoother=3, red_factor=1e-13, maxit=30), rhs, sol0)
+        assert info.status == 0
+        nc = len(fin["begin_index"]) - 1
+        q = ctx.quadrature_points(sids[-1], nc, 3)
+        s, c = np.sin(np.pi * q), np.cos(np.pi * q)
+        ex = np.stack([s[..., 0] * s[..., 1] * s[..., 2], np.pi * c[..., 0] * s[..., 1] * s[..., 2],
+                       np.pi * s[..., 0] * c[..., 1] * s[..., 2], np.pi * s[..., 0] * s[..., 1] * c[..., 2]], -1)
+        l2, h1 = ctx.errors_table(sids[-1], x, ex)
+    finally:
+        ctx.close()
+    assert (f"{l2:g}", f"{h1:g}") == cpu_errors, ((l2, h1), cpu_errors)
