@@ -385,6 +385,7 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     spmv_ms = e0.elapsed_time(e1) / reps
     spmv_bytes = 12 * nnz + 4 * (n + 1) + 16 * n
+    tuning = ctx.product_tuning(sids[-1])
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
         hbm = json.load(open(peaks_path))["hbm_gbs"]
@@ -395,7 +396,7 @@ def run_ours(args, rank, world, local):
     # DRAM bytes (read + write) of one launch of this kernel on this workload, from the ncu
     # capture summarised in profiles/
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "csr_kernel_spmv_f64_cd3d_q2_32.md")
+    prof = os.path.join(ROOT, "profiles", "csr_tma_kernel_spmv_f64_cd3d_q2_32.md")
     if args.n == 32 and os.path.exists(prof):
         for line in open(prof):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -446,7 +447,9 @@ def run_ours(args, rank, world, local):
         "assembly": {"ms_all_levels": ms_asm, "mcells_per_s": n_cells_total / (ms_asm * 1e-3) / 1e6},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic,
-                     "kernel": "csr_kernel<double,8,16,SPMV,4> (finest level, the FGMRES matvec)",
+                     "kernel": "csr_tma_kernel<SPMV, cap, stages> (finest level, the FGMRES matvec; matrix "
+                               "tiles streamed into shared memory by bulk copies)",
+                     "autotuner": tuning,
                      "peak_source": peak_src, "spmv_ms": spmv_ms, "algorithmic_bytes": spmv_bytes},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 16 * n,
                 "d2h_bytes_per_step": 16 * n},

@@ -188,6 +188,12 @@ int cdgpu_spmv(cdgpu_ctx *ctx, int space_id, const double *h_x, double *h_y);
 int cdgpu_defect(cdgpu_ctx *ctx, int space_id, const double *h_x, const double *h_f, double *h_d,
                  double *res);
 int cdgpu_spmv_device(cdgpu_ctx *ctx, int space_id, const double *d_x, double *d_y);
+/* The FP64 product, defect and Jacobi sweep of a matrix larger than L2 stream its tiles into
+ * shared memory with bulk copies; the tile shape (nonzeros per tile, pipeline stages, CTAs
+ * per SM) is chosen by timing every variant on the matrix at the first solve that uses it.
+ * This copies a one-line report of that choice (or "not tuned yet") into buf.  No reference
+ * counterpart (MatVect / Defect, src/FE/Blas2.C:11-99, are the operations). */
+int cdgpu_product_tuning(cdgpu_ctx *ctx, int space_id, char *buf, int len);
 /* y = A x with an FP32 form of the assembled operator, the forms the mixed multigrid cycle
  * applies (TMGLevel3D's MatVect/Defect on the FP32 levels, src/FE/MGLevel3D.C:194-252):
  * form 0 the FP32 copy of the CSR entries; 1 the matrix-free per-cell products

@@ -479,6 +479,16 @@ int cdgpu_errors(cdgpu_ctx *ctx, int space_id, const double *h_sol, double *l2, 
   return rc;
 }
 
+int cdgpu_product_tuning(cdgpu_ctx *ctx, int space_id, char *buf, int len)
+{
+  Space *s = get_space(ctx, space_id);
+  if (!s || !buf || len <= 0) return fail(ctx, CDGPU_ERR_INVALID, "product_tuning: bad argument");
+  std::string r;
+  csr_tuning_report(ctx, *s, r);
+  snprintf(buf, len, "%s", r.c_str());
+  return CDGPU_OK;
+}
+
 int cdgpu_errors_table(cdgpu_ctx *ctx, int space_id, const double *h_sol, const double *h_exact, double *l2,
                        double *h1semi)
 {

@@ -274,11 +274,14 @@ inline void launch_csr(cdgpu_ctx *ctx, const CsrShape &sh, const CsrArgs<T> &pa,
 // Every mbarrier wait is bounded; on a timeout the kernel sets err = 4, stops, waits (bounded)
 // for the copies it issued and returns.
 // ---------------------------------------------------------------------------
-constexpr int kTmaRows = 64, kTmaCap = 2048, kTmaStages = 4, kTmaWarps = 8;
-constexpr int kTmaValsBytes = (kTmaCap + 8) * 8, kTmaColsBytes = (kTmaCap + 8) * 4;
+// CAP (nonzeros per tile) and STAGES are template parameters: the variants a tile-shape
+// autotuner chooses from per matrix (solve.cu, tune_tma); kTmaRows = 8 consumer warps x 8 rows
+constexpr int kTmaRows = 64, kTmaWarps = 8;
 constexpr int kTmaRpBytes = ((kTmaRows + 1 + 8) * 4 + 127) / 128 * 128;
-constexpr int kTmaStageBytes = kTmaValsBytes + kTmaColsBytes + kTmaRpBytes;
-constexpr int kTmaSmem = kTmaStages * kTmaStageBytes + 256;
+__host__ __device__ constexpr int tma_vals_bytes(int cap) { return (cap + 8) * 8; }
+__host__ __device__ constexpr int tma_cols_bytes(int cap) { return (cap + 8) * 4; }
+__host__ __device__ constexpr int tma_stage_bytes(int cap) { return tma_vals_bytes(cap) + tma_cols_bytes(cap) + kTmaRpBytes; }
+__host__ __device__ constexpr int tma_smem_bytes(int cap, int stages) { return stages * tma_stage_bytes(cap) + 256; }
 constexpr long kTmaSpin = 1L << 22; // polls of one wait before it is declared timed out
 
 __device__ __forceinline__ uint32_t tma_smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -318,10 +321,16 @@ struct TmaMeta
   int rb, re, rb0, nb0; // rows [rb, re); row-pointer and nonzero copies start at rb0, nb0
 };
 
-template <int MODE>
+template <int MODE, int CAP, int STAGES>
 __global__ void __launch_bounds__((kTmaWarps + 1) * 32) csr_tma_kernel(CsrArgs<double> p, const int2 *__restrict__ tiles,
                                                                          int n_tiles, int *__restrict__ err)
 {
+  constexpr int kTmaStages = STAGES, kTmaCap = CAP;
+  constexpr int kTmaValsBytes = tma_vals_bytes(CAP), kTmaColsBytes = tma_cols_bytes(CAP);
+  constexpr int kTmaStageBytes = tma_stage_bytes(CAP);
+  static_assert(kTmaValsBytes % 16 == 0 && kTmaColsBytes % 16 == 0 && kTmaStageBytes % 16 == 0,
+                "bulk-copy destinations must stay 16-byte aligned");
+  (void)kTmaCap;
   extern __shared__ __align__(128) unsigned char tma_sm[];
   __shared__ __align__(8) uint64_t full[kTmaStages], empty[kTmaStages];
   __shared__ TmaMeta meta[kTmaStages];

@@ -66,6 +66,11 @@ struct Space
   // keeps the plain CSR kernels (small, or a row longer than a tile)
   int2 *d_tiles = nullptr;
   int n_tiles = 0;
+  // the variant of the TMA product chosen by the autotuner on the first assembly of this
+  // pattern (index into the variant table of solve.cu; -1 = not tuned yet) and its report
+  int tma_var = -1;
+  int tma_ctas = 0; // resident CTAs per SM of the chosen variant
+  std::string tma_report;
   // DOF -> (cell, local index) incidence, ascending cell per DOF
   int *d_inc_ptr = nullptr, *d_inc = nullptr;
   // slot map of the row gather: for incidence t of an active row and local column j, the
@@ -282,5 +287,7 @@ int apply_fp32_form(cdgpu_ctx *ctx, Space &s, int form, const float *d_x, float 
 int build_pattern_device(cdgpu_ctx *ctx, Space &s, int **d_kcol_out, bool *fallback);
 // tiles of the TMA product for a freshly installed pattern (solve.cu)
 int build_csr_tiles(cdgpu_ctx *ctx, Space &s);
+// the TMA product's variant choice for a space, as text
+int csr_tuning_report(cdgpu_ctx *ctx, Space &s, std::string &out);
 // looks up the allocation-free defect's scratch array on a device (noalloc.cu)
 void noalloc_prepare(int device);

@@ -473,9 +473,52 @@ template <typename T> static CsrArgs<T> csr_args(const Space &s, const T *x)
   p.x = x;
   return p;
 }
-// FP64 operations on a matrix with TMA tiles go through csr_tma_kernel: persistent CTAs, at
-// most two per SM (their shared-memory stages), never more than there are tiles
-static int tma_grid(const cdgpu_ctx *ctx, const Space &s) { return std::max(1, std::min(s.n_tiles, ctx->sm_count * 2)); }
+// FP64 operations on a matrix with TMA tiles go through csr_tma_kernel in the variant (tile
+// capacity, stages) the autotuner chose for the matrix (variant 0 until it has run):
+// persistent CTAs, as many per SM as the variant's shared memory allows, never more than
+// there are tiles
+struct TmaVariant
+{
+  int cap, stages;
+};
+static const TmaVariant kTmaVariants[] = {{2048, 4}, {2048, 2}, {3072, 3}, {3072, 2}, {4096, 2}};
+constexpr int kNumTmaVariants = sizeof(kTmaVariants) / sizeof(kTmaVariants[0]);
+
+template <int MODE> static void (*tma_kernel(int v))(CsrArgs<double>, const int2 *, int, int *)
+{
+  switch (v)
+  {
+    case 1: return csr_tma_kernel<MODE, 2048, 2>;
+    case 2: return csr_tma_kernel<MODE, 3072, 3>;
+    case 3: return csr_tma_kernel<MODE, 3072, 2>;
+    case 4: return csr_tma_kernel<MODE, 4096, 2>;
+    default: return csr_tma_kernel<MODE, 2048, 4>;
+  }
+}
+static int tma_smem(int v) { return tma_smem_bytes(kTmaVariants[v].cap, kTmaVariants[v].stages); }
+static int tma_var(const Space &s) { return s.tma_var < 0 ? 0 : s.tma_var; }
+
+// resident CTAs per SM of a variant (its shared-memory attribute set on the way)
+static int tma_ctas_per_sm(int v)
+{
+  const int sm = tma_smem(v);
+  int nb = 0;
+  for (auto k : {tma_kernel<CM_SPMV>(v), tma_kernel<CM_DEFECT>(v), tma_kernel<CM_JACOBI>(v)})
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, tma_kernel<CM_SPMV>(v), (kTmaWarps + 1) * 32, sm) != cudaSuccess)
+  {
+    cudaGetLastError();
+    return 0;
+  }
+  return nb;
+}
+
+static int tma_grid(const cdgpu_ctx *ctx, const Space &s)
+{
+  const int per_sm = s.tma_var < 0 ? 2 : std::max(1, s.tma_ctas);
+  return std::max(1, std::min(s.n_tiles, ctx->sm_count * per_sm));
+}
+
 template <typename T, int MODE> static bool launch_tma(cdgpu_ctx *ctx, const Space &s, const CsrArgs<T> &pa, int grid)
 {
   if constexpr (std::is_same<T, double>::value)
@@ -484,7 +527,8 @@ template <typename T, int MODE> static bool launch_tma(cdgpu_ctx *ctx, const Spa
     {
       CsrArgs<double> p = pa;
       p.pre = ctx->pdl_pre ? 1 : 0;
-      (void)cd_launch(csr_tma_kernel<MODE>, grid, (kTmaWarps + 1) * 32, kTmaSmem, ctx->stream, p,
+      const int v = tma_var(s);
+      (void)cd_launch(tma_kernel<MODE>(v), grid, (kTmaWarps + 1) * 32, tma_smem(v), ctx->stream, p,
                       (const int2 *)s.d_tiles, s.n_tiles, ctx->d_err);
       return true;
     }
@@ -772,36 +816,133 @@ static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, 
   return CDGPU_OK;
 }
 
-// Tiles of the TMA product: consecutive rows, at most kTmaRows rows and kTmaCap nonzeros per
+// Tiles of the TMA product: consecutive rows, at most kTmaRows rows and `cap` nonzeros per
 // tile, for matrices whose stream does not fit in L2 (smaller ones are latency-bound and keep
-// the plain kernels).  A row longer than kTmaCap leaves the matrix on the plain kernels.
+// the plain kernels).  A row longer than the smallest capacity leaves the matrix on the plain
+// kernels.
 constexpr long kTmaMinNnz = 4L << 20;
+
+static bool make_tiles(const Space &s, int cap, std::vector<int2> &tiles)
+{
+  tiles.clear();
+  const int *rp = s.h_row_ptr.data();
+  int r = 0;
+  while (r < s.n_dof)
+  {
+    if (rp[r + 1] - rp[r] > cap) return false;
+    int e = r;
+    while (e < s.n_dof && e - r < kTmaRows && rp[e + 1] - rp[r] <= cap) e++;
+    tiles.push_back(make_int2(r, rp[r]));
+    r = e;
+  }
+  tiles.push_back(make_int2(s.n_dof, rp[s.n_dof]));
+  return true;
+}
 
 int build_csr_tiles(cdgpu_ctx *ctx, Space &s)
 {
   if (s.d_tiles) { cudaFree(s.d_tiles); s.d_tiles = nullptr; }
   s.n_tiles = 0;
+  s.tma_var = -1;
+  s.tma_report.clear();
   if (s.nnz < kTmaMinNnz) return CDGPU_OK;
   std::vector<int2> tiles;
-  const int *rp = s.h_row_ptr.data();
-  int r = 0;
-  while (r < s.n_dof)
-  {
-    if (rp[r + 1] - rp[r] > kTmaCap) return CDGPU_OK;
-    int e = r;
-    while (e < s.n_dof && e - r < kTmaRows && rp[e + 1] - rp[r] <= kTmaCap) e++;
-    tiles.push_back(make_int2(r, rp[r]));
-    r = e;
-  }
-  tiles.push_back(make_int2(s.n_dof, rp[s.n_dof]));
+  if (!make_tiles(s, kTmaVariants[0].cap, tiles)) return CDGPU_OK;
   int rc;
   if ((rc = ensure_err_flag(ctx))) return rc;
   if ((rc = dev_alloc(ctx, &s.d_tiles, tiles.size()))) return rc;
   CD_CUDA(ctx, cudaMemcpy(s.d_tiles, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
-  CD_CUDA(ctx, cudaFuncSetAttribute(csr_tma_kernel<CM_SPMV>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmem));
-  CD_CUDA(ctx, cudaFuncSetAttribute(csr_tma_kernel<CM_DEFECT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmem));
-  CD_CUDA(ctx, cudaFuncSetAttribute(csr_tma_kernel<CM_JACOBI>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmem));
+  if (tma_ctas_per_sm(0) <= 0) return cuda_fail(ctx, cudaErrorInvalidConfiguration, "TMA product: no resident CTA");
   s.n_tiles = (int)tiles.size() - 1;
+  return CDGPU_OK;
+}
+
+// Tile-shape autotuner of the TMA product, run once per pattern on the first solve with
+// assembled values (outside any stream capture): every variant (tile capacity, stages,
+// resident CTAs per SM from its shared memory) times five products y = A x on this matrix
+// after one warm-up launch; the fastest is kept with its tiles.  The report lists the
+// variants and their mean times.
+static int tune_tma(cdgpu_ctx *ctx, Space &s)
+{
+  if (s.n_tiles <= 0 || s.tma_var >= 0) return CDGPU_OK;
+  int rc;
+  double *x = nullptr, *y = nullptr;
+  if ((rc = dev_alloc(ctx, &x, s.n_dof)) || (rc = dev_alloc(ctx, &y, s.n_dof)))
+  {
+    if (x) cudaFree(x);
+    return rc;
+  }
+  CD_CUDA(ctx, cudaMemsetAsync(x, 0, sizeof(double) * s.n_dof, ctx->stream));
+  cudaEvent_t e0, e1;
+  CD_CUDA(ctx, cudaEventCreate(&e0));
+  CD_CUDA(ctx, cudaEventCreate(&e1));
+  int best = -1, best_ctas = 0, best_n = 0;
+  float best_ms = 1e30f;
+  int2 *best_tiles = nullptr;
+  std::string report;
+  for (int v = 0; v < kNumTmaVariants; v++)
+  {
+    std::vector<int2> tiles;
+    const int ctas = tma_ctas_per_sm(v);
+    if (ctas <= 0 || !make_tiles(s, kTmaVariants[v].cap, tiles)) continue;
+    int2 *dt = nullptr;
+    if ((rc = dev_alloc(ctx, &dt, tiles.size()))) break;
+    CD_CUDA(ctx, cudaMemcpy(dt, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
+    const int nt = (int)tiles.size() - 1;
+    const int grid = std::max(1, std::min(nt, ctx->sm_count * ctas));
+    CsrArgs<double> p = csr_args<double>(s, x);
+    p.y = y;
+    auto k = tma_kernel<CM_SPMV>(v);
+    (void)cd_launch(k, grid, (kTmaWarps + 1) * 32, tma_smem(v), ctx->stream, p, (const int2 *)dt, nt, ctx->d_err);
+    CD_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
+    for (int i = 0; i < 5; i++)
+      (void)cd_launch(k, grid, (kTmaWarps + 1) * 32, tma_smem(v), ctx->stream, p, (const int2 *)dt, nt, ctx->d_err);
+    CD_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
+    CD_CUDA(ctx, cudaEventSynchronize(e1));
+    CD_LAUNCHED(ctx);
+    float ms = 0;
+    CD_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
+    ms /= 5;
+    char line[128];
+    snprintf(line, sizeof(line), "%scap %d stages %d ctas/SM %d: %.1f us", report.empty() ? "" : "; ",
+             kTmaVariants[v].cap, kTmaVariants[v].stages, ctas, 1e3 * ms);
+    report += line;
+    if (ms < best_ms)
+    {
+      if (best_tiles) cudaFree(best_tiles);
+      best_tiles = dt;
+      best_ms = ms;
+      best = v;
+      best_ctas = ctas;
+      best_n = nt;
+    }
+    else
+      cudaFree(dt);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(x);
+  cudaFree(y);
+  if (rc) { if (best_tiles) cudaFree(best_tiles); return rc; }
+  if ((rc = assemble_check(ctx))) { if (best_tiles) cudaFree(best_tiles); return rc; } // wait flag of the timed launches
+  if (best < 0) return CDGPU_OK; // keep the default variant
+  cudaFree(s.d_tiles);
+  s.d_tiles = best_tiles;
+  s.n_tiles = best_n;
+  s.tma_var = best;
+  s.tma_ctas = best_ctas;
+  char sel[96];
+  snprintf(sel, sizeof(sel), "chosen: cap %d stages %d ctas/SM %d; ", kTmaVariants[best].cap, kTmaVariants[best].stages,
+           best_ctas);
+  s.tma_report = sel + report;
+  return CDGPU_OK;
+}
+
+int csr_tuning_report(cdgpu_ctx *ctx, Space &s, std::string &out)
+{
+  (void)ctx;
+  out = s.n_tiles > 0 ? (s.tma_var >= 0 ? s.tma_report : std::string("default variant (not tuned yet)"))
+                      : std::string("plain CSR kernels (no TMA tiles for this matrix)");
   return CDGPU_OK;
 }
 
@@ -1330,6 +1471,7 @@ int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const 
   if (p.coarse_smoother != 17 && h.lev[0].sp->n_dof > 6000)
     return fail(ctx, CDGPU_ERR_UNSUPPORTED, "solve: coarse smoother loop needs a coarsest level below 6000 DOFs");
   int rc;
+  if ((rc = tune_tma(ctx, *h.lev.back().sp))) return rc; // once per pattern, before any capture
   if (p.coarse_smoother == 17 && (rc = refresh_coarse_inverse(ctx, h))) return rc;
   if (p.precision == 1 && (rc = refresh_mf(ctx, h))) return rc;
   cdgpu_solve_info local{};

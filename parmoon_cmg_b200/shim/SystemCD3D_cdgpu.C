@@ -41,6 +41,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <string>
 #include <vector>
 
 #include "../../include/cdgpu.h"
@@ -323,12 +324,27 @@ void TSystemCD3D::Solve(double *sol, double *rhs)
     exit(4711);
   }
   if (info.status == CDGPU_ERR_NOT_CONVERGED) OutPut("libcdgpu: solver not converged" << endl);
-  // optional copy of the solution for an external check (no counterpart in the reference)
+  // optional copy of the solution and of the DOF positions (TFESpace3D::GetDOFPosition) for an
+  // external check (no counterpart in the reference)
   if (const char *path = getenv("CDGPU_DUMP_SOLUTION"))
   {
     if (FILE *f = fopen(path, "wb"))
     {
       fwrite(sol, sizeof(double), N_DOF, f);
+      fclose(f);
+    }
+    std::vector<double> x(N_DOF), y(N_DOF), z(N_DOF), xyz(3 * (size_t)N_DOF);
+    FeSpaces[N_Levels - 1]->GetDOFPosition(x.data(), y.data(), z.data());
+    for (int i = 0; i < N_DOF; i++)
+    {
+      xyz[3 * (size_t)i] = x[i];
+      xyz[3 * (size_t)i + 1] = y[i];
+      xyz[3 * (size_t)i + 2] = z[i];
+    }
+    std::string p2 = std::string(path) + ".xyz";
+    if (FILE *f = fopen(p2.c_str(), "wb"))
+    {
+      fwrite(xyz.data(), sizeof(double), xyz.size(), f);
       fclose(f);
     }
   }

@@ -149,6 +149,12 @@ class Context:
         self.check(self.lib.cdgpu_spmv(self.h, sid, _p(x), _p(y)))
         return y
 
+    def product_tuning(self, sid):
+        """The tile-shape choice of the FP64 product of a space's matrix, as text."""
+        buf = C.create_string_buffer(1024)
+        self.check(self.lib.cdgpu_product_tuning(self.h, sid, buf, 1024))
+        return buf.value.decode()
+
     def apply_fp32(self, sid, x, form):
         """y = A x with an FP32 form of the operator: 0 CSR copy, 1 matrix-free on CUDA cores,
         2 matrix-free on the tensor cores."""

@@ -199,6 +199,11 @@ def test_bench_solution_vs_oracle_and_reference(ctx, case, reference):
     # the two independent FP64 answers agree with each other first
     assert rel(case["x_o"], x_ref) <= TOL_SOL
     x64, i64 = gpu_solve(ctx, case, 0)
+    # the finest matrix (15.8M nonzeros) takes the bulk-copy product, whose tile shape the
+    # autotuner chose on this first solve
+    tuning = ctx.product_tuning(case["sids"][-1])
+    print(tuning)
+    assert tuning.startswith("chosen:"), tuning
     assert rel(x64, case["x_o"]) <= TOL_SOL, rel(x64, case["x_o"])
     assert rel(x64, x_ref) <= TOL_SOL, rel(x64, x_ref)
     xm, im = gpu_solve(ctx, case, 1)
