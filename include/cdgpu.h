@@ -162,6 +162,16 @@ int cdgpu_errors(cdgpu_ctx *ctx, int space_id, const double *h_sol, double *l2, 
 int cdgpu_errors_table(cdgpu_ctx *ctx, int space_id, const double *h_sol, const double *h_exact, double *l2,
                        double *h1semi);
 
+/* --- output ------------------------------------------------------------------
+ * Replaces TOutput3D::WriteVtk / TOutput2D::WriteVtk (src/FE/Output3D.C:1747) for one scalar
+ * function: legacy ASCII VTK with the mesh vertices, the cells and the function's vertex
+ * values (name: the SCALARS name, NULL = "u").  sol: n_dof values on the device
+ * (sol_on_device = 1, e.g. a batch or device solve's result) or on the host.  The vertices are
+ * numbered in ascending order of their DOFs (the reference numbers them by vertex address, so
+ * the files list the same points and values in another order). */
+int cdgpu_write_vtk(cdgpu_ctx *ctx, int space_id, const double *sol, int sol_on_device, const char *path,
+                    const char *name);
+
 /* --- assembly ---------------------------------------------------------------
  * Replaces TSystemCD3D::Assemble / TAssembleMat3D::Reset + Assemble3D
  * (src/System/SystemCD3D.C:314-339, src/System/AssembleMat3D.C:230-505) and

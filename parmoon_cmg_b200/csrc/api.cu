@@ -66,7 +66,7 @@ static void free_mg(Hierarchy *h)
   for (auto &g : h->gexec)
     if (g) cudaGraphExecDestroy(g);
   void *ptrs[] = {h->d_cinv, h->d_cpiv, h->d_V, h->d_Z, h->d_w, h->d_ctl, h->d_partial, h->d_x, h->d_b,
-                  h->d_io};
+                  h->d_io, h->d_coop_bar};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -487,6 +487,71 @@ int cdgpu_product_tuning(cdgpu_ctx *ctx, int space_id, char *buf, int len)
   csr_tuning_report(ctx, *s, r);
   snprintf(buf, len, "%s", r.c_str());
   return CDGPU_OK;
+}
+
+// Legacy-VTK output of a solution, in the form TOutput3D::WriteVtk / TOutput2D::WriteVtk write
+// it (src/FE/Output3D.C:1747-2010): ASCII UNSTRUCTURED_GRID, the mesh vertices as POINTS, one
+// hexahedron (type 12) or quadrilateral (type 9) per cell, the function's values at the vertices
+// as POINT_DATA, 6 significant digits in scientific notation.  The vertices are the vertex DOFs
+// of the Q1/Q2 space (a conforming function's value there is its DOF value), numbered in
+// ascending DOF order; the reference numbers them by sorting vertex addresses.  sol may be on
+// the device (sol_on_device != 0: it is copied back first) or on the host.
+int cdgpu_write_vtk(cdgpu_ctx *ctx, int space_id, const double *sol, int sol_on_device, const char *path,
+                    const char *name)
+{
+  Space *s = get_space(ctx, space_id);
+  if (!s || !sol || !path) return fail(ctx, CDGPU_ERR_INVALID, "write_vtk: bad argument");
+  std::vector<double> u(s->n_dof);
+  if (sol_on_device)
+  {
+    cudaSetDevice(ctx->device);
+    CD_CUDA(ctx, cudaMemcpyAsync(u.data(), sol, sizeof(double) * s->n_dof, cudaMemcpyDeviceToHost, ctx->stream));
+    CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  else
+    std::copy(sol, sol + s->n_dof, u.begin());
+  // local index of every cell vertex among the cell's DOFs (tensor order, x fastest)
+  const int p1 = s->order + 1;
+  int vdof[8];
+  for (int v = 0; v < s->nv; v++)
+  {
+    const int ix = (v == 1 || v == 2 || v == 5 || v == 6) ? s->order : 0;
+    const int iy = (v == 2 || v == 3 || v == 6 || v == 7) ? s->order : 0;
+    const int iz = v >= 4 ? s->order : 0;
+    vdof[v] = ix + p1 * iy + (s->dim == 3 ? p1 * p1 * iz : 0);
+  }
+  std::vector<int> point(s->n_dof, -1);
+  std::vector<double> xyz((size_t)s->n_dof * 3, 0.0);
+  for (int c = 0; c < s->n_cells; c++)
+    for (int v = 0; v < s->nv; v++)
+    {
+      const int d = s->h_gn[(size_t)c * s->nbf + vdof[v]];
+      point[d] = 0;
+      for (int a = 0; a < s->dim; a++) xyz[(size_t)d * 3 + a] = s->h_coords[((size_t)c * s->nv + v) * s->dim + a];
+    }
+  int np = 0;
+  for (int d = 0; d < s->n_dof; d++)
+    if (point[d] >= 0) point[d] = np++;
+  FILE *f = fopen(path, "w");
+  if (!f) return fail(ctx, CDGPU_ERR_INVALID, std::string("write_vtk: cannot open ") + path);
+  fprintf(f, "# vtk DataFile Version 4.2\nfile created by libcdgpu\nASCII\nDATASET UNSTRUCTURED_GRID\n\n");
+  fprintf(f, "POINTS %d double\n", np);
+  for (int d = 0; d < s->n_dof; d++)
+    if (point[d] >= 0) fprintf(f, "%.6e %.6e %.6e\n", xyz[(size_t)d * 3], xyz[(size_t)d * 3 + 1], xyz[(size_t)d * 3 + 2]);
+  fprintf(f, "\nCELLS %d %d\n", s->n_cells, s->n_cells * (s->nv + 1));
+  for (int c = 0; c < s->n_cells; c++)
+  {
+    fprintf(f, "%d ", s->nv);
+    for (int v = 0; v < s->nv; v++) fprintf(f, "%d ", point[s->h_gn[(size_t)c * s->nbf + vdof[v]]]);
+    fprintf(f, "\n");
+  }
+  fprintf(f, "\nCELL_TYPES %d\n", s->n_cells);
+  for (int c = 0; c < s->n_cells; c++) fprintf(f, "%d ", s->dim == 3 ? 12 : 9);
+  fprintf(f, "\n\nPOINT_DATA %d\nSCALARS %s double\nLOOKUP_TABLE default\n", np, name && name[0] ? name : "u");
+  for (int d = 0; d < s->n_dof; d++)
+    if (point[d] >= 0) fprintf(f, "%.6e\n", u[d]);
+  const bool ok = fclose(f) == 0;
+  return ok ? CDGPU_OK : fail(ctx, CDGPU_ERR_INVALID, "write_vtk: write failed");
 }
 
 int cdgpu_errors_table(cdgpu_ctx *ctx, int space_id, const double *h_sol, const double *h_exact, double *l2,

@@ -158,6 +158,11 @@ struct Hierarchy
   cudaEvent_t ev_slot[2] = {nullptr, nullptr}; // recorded behind each slot's copy
   int *h_cflag = nullptr;     // pinned copy of the coarse inversion's zero-pivot flag
   bool cflag_pending = false; // copy enqueued, not yet checked
+  // the FP32 V-cycle below the finest level as one cooperative kernel (coop.cuh): its
+  // barrier words and whether the last capture used it (false after a failed attempt)
+  unsigned *d_coop_bar = nullptr;
+  bool coop_failed = false;
+  bool coop_used = false;
 };
 
 // ---------------------------------------------------------------------------
@@ -185,6 +190,8 @@ struct cdgpu_ctx
   // set while the multigrid cycle is recorded into its graph: its kernels load the data that
   // no kernel of the cycle writes before waiting for their predecessor
   bool pdl_pre = false;
+  // set while the FP32 cycle is recorded: grid of the cooperative coarse-cycle kernel (0: none)
+  int coop_grid_hint = 0;
   int *d_err = nullptr; // assembly error flag (device) and its pinned host mirror
   int *h_err = nullptr;
 };

@@ -29,6 +29,7 @@
 #include "internal.h"
 #include "csr.cuh"
 #include "mf.cuh"
+#include "coop.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -639,6 +640,7 @@ template <typename T> static int jacobi_first(cdgpu_ctx *ctx, Level &L, T omega,
 struct CycleState
 {
   const cdgpu_solver_params *p;
+  int coop_grid = 0; // > 0: the levels below the finest run as one cooperative kernel of this many CTAs
   int rec[64];
   int pre_done[64];    // pre-smoothing sweeps already done (fused into the cycle's start)
   bool sol_zero[64];   // active part and Dirichlet part zero
@@ -687,6 +689,87 @@ template <typename T> static int coarse_solve(cdgpu_ctx *ctx, Hierarchy &h, Cycl
   return CDGPU_OK;
 }
 
+// The FP32 V-cycle of levels 0 .. L-2 as one cooperative kernel (coop.cuh), when the cycle is
+// a V-cycle with the exact coarse solve, no level below the finest uses the matrix-free
+// operator, and every CTA of the grid can be resident.  Returns the grid size, 0 if not.
+static int coop_grid_size(cdgpu_ctx *ctx, const Hierarchy &h, const cdgpu_solver_params &p)
+{
+  const int L = (int)h.lev.size();
+  if (h.coop_failed || L < 3 || L - 1 > kCoopMaxLevels || p.cycle != 1 || p.coarse_smoother != 17 || p.pre < 0 || p.post < 0)
+    return 0;
+  if (const char *v = getenv("CDGPU_COOP_CYCLE"))
+    if (v[0] == '0') return 0;
+  for (int l = 0; l < L - 1; l++)
+    if (use_mf(*h.lev[l].sp)) return 0;
+  const Space &c = *h.lev[0].sp;
+  const size_t smem = sizeof(double) * (c.n_dof + c.n_active);
+  if (smem > 48 * 1024) return 0;
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mg_coop_cycle_kernel, kCoopThreads, smem) != cudaSuccess)
+  {
+    cudaGetLastError();
+    return 0;
+  }
+  return nb > 0 ? ctx->sm_count * std::min(nb, 2) : 0;
+}
+
+static int launch_coop_cycle(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, int grid)
+{
+  const int top = (int)h.lev.size() - 2;
+  CoopArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.top = top;
+  a.pre = p.pre;
+  a.post = p.post;
+  a.omega = (float)p.omega;
+  a.damp = (float)p.gmg_damp;
+  for (int i = 0; i <= top; i++)
+  {
+    const Level &L = h.lev[i];
+    const Space &s = *L.sp;
+    CoopLevel &c = a.lev[i];
+    c.n = s.n_dof;
+    c.n_active = s.n_active;
+    c.gs = s.shape.gs;
+    c.rp = s.d_row_ptr;
+    c.kc = s.d_kcol;
+    c.a = s.d_a32;
+    c.diag = s.d_diag32;
+    c.sol = L.v32.sol;
+    c.alt = L.v32.alt;
+    c.rhs = L.v32.rhs;
+    c.def = L.v32.def;
+    if (i > 0)
+    {
+      c.r_row = L.d_r_row; c.r_col = L.d_r_col; c.r_val = L.d_r_val32; c.r_gs = L.r_shape.gs;
+      c.p_row = L.d_p_row; c.p_col = L.d_p_col; c.p_val = L.d_p_val32; c.p_gs = L.p_shape.gs;
+    }
+  }
+  const Space &c0 = *h.lev[0].sp;
+  a.a0 = c0.d_a;
+  a.dir_start0 = c0.d_dir_start;
+  a.cinv = h.d_cinv;
+  a.bar = h.d_coop_bar;
+  a.err = ctx->d_err;
+  CD_CUDA(ctx, cudaMemsetAsync(h.d_coop_bar, 0, 4 * sizeof(unsigned), ctx->stream));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = kCoopThreads;
+  cfg.dynamicSmemBytes = sizeof(double) * (c0.n_dof + c0.n_active);
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CD_CUDA(ctx, cudaLaunchKernelEx(&cfg, mg_coop_cycle_kernel, a));
+  ctx->launches++;
+  // the host's view of the top level's buffers after its pre + post sweeps inside the kernel
+  Level &T = h.lev[top];
+  if ((p.pre + p.post) % 2) std::swap(T.v32.sol, T.v32.alt);
+  return CDGPU_OK;
+}
+
 template <typename T> static int cycle(cdgpu_ctx *ctx, Hierarchy &h, CycleState &cs, int i)
 {
   if (i == 0) return coarse_solve<T>(ctx, h, cs);
@@ -712,8 +795,18 @@ template <typename T> static int cycle(cdgpu_ctx *ctx, Hierarchy &h, CycleState 
   csr_restrict<T>(ctx, L, sc, v.def, vc.rhs, vc.sol);
   CD_LAUNCHED(ctx);
   cs.sol_zero[i - 1] = cs.active_zero[i - 1] = true;
-  for (int j = 0; j < cs.rec[i]; j++)
-    if ((rc = cycle<T>(ctx, h, cs, i - 1))) return rc;
+  bool coop = false;
+  if constexpr (std::is_same<T, float>::value)
+  {
+    if (cs.coop_grid > 0 && i == (int)h.lev.size() - 1)
+    {
+      if ((rc = launch_coop_cycle(ctx, h, *cs.p, cs.coop_grid))) return rc;
+      coop = true;
+    }
+  }
+  if (!coop)
+    for (int j = 0; j < cs.rec[i]; j++)
+      if ((rc = cycle<T>(ctx, h, cs, i - 1))) return rc;
   if (cs.p->cycle < 1) cs.rec[i] = 1;
   csr_prolong<T>(ctx, L, s, vc.sol, v.sol, (T)cs.p->gmg_damp);
   CD_LAUNCHED(ctx);
@@ -733,6 +826,7 @@ template <typename T> static int mg_record(cdgpu_ctx *ctx, Hierarchy &h, const c
   int n = F.sp->n_dof;
   CycleState cs;
   cs.p = &p;
+  if constexpr (std::is_same<T, float>::value) cs.coop_grid = ctx->coop_grid_hint;
   // SetRecursion(levels = L-1), MultiGrid3D.C:691-703
   cs.rec[1] = 1;
   for (int k = 2; k <= L - 1; k++) cs.rec[k] = p.cycle > 0 ? p.cycle : 2;
@@ -790,20 +884,40 @@ static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, 
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_exact_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm1));
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_smooth_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm2));
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_smooth_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm2));
-    cudaGraph_t g = nullptr;
-    const long long before = ctx->launches;
-    CD_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    ctx->pdl_pre = true; // kernels of the cycle load matrix data before waiting (CD_PDL_WAIT)
-    rc = k == 1 ? mg_record<float>(ctx, h, p) : mg_record<double>(ctx, h, p);
-    ctx->pdl_pre = false;
-    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
-    h.graph_nodes[k] = ctx->launches - before; // kernels per replay; capturing runs none
-    ctx->launches = before;
-    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture of the multigrid cycle");
-    e = cudaGraphInstantiate(&h.gexec[k], g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) { h.gexec[k] = nullptr; return cuda_fail(ctx, e, "graph instantiate"); }
+    // the FP32 cycle below the finest level as one cooperative kernel where possible; if the
+    // capture or instantiation with it fails, the cycle is captured again kernel by kernel
+    for (int attempt = 0; attempt < 2; attempt++)
+    {
+      ctx->coop_grid_hint = k == 1 ? coop_grid_size(ctx, h, p) : 0;
+      if (ctx->coop_grid_hint > 0 && !h.d_coop_bar && (rc = dev_alloc(ctx, &h.d_coop_bar, 4))) return rc;
+      cudaGraph_t g = nullptr;
+      const long long before = ctx->launches;
+      CD_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      ctx->pdl_pre = true; // kernels of the cycle load matrix data before waiting (CD_PDL_WAIT)
+      rc = k == 1 ? mg_record<float>(ctx, h, p) : mg_record<double>(ctx, h, p);
+      ctx->pdl_pre = false;
+      cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+      h.graph_nodes[k] = ctx->launches - before; // kernels per replay; capturing runs none
+      ctx->launches = before;
+      if (rc == CDGPU_OK && e == cudaSuccess)
+      {
+        e = cudaGraphInstantiate(&h.gexec[k], g, 0);
+        if (e != cudaSuccess) h.gexec[k] = nullptr;
+      }
+      if (g) cudaGraphDestroy(g);
+      const bool ok = rc == CDGPU_OK && e == cudaSuccess;
+      if (!ok && ctx->coop_grid_hint > 0)
+      {
+        cudaGetLastError();
+        h.coop_failed = true; // retry without the cooperative kernel
+        continue;
+      }
+      h.coop_used = ok && ctx->coop_grid_hint > 0;
+      ctx->coop_grid_hint = 0;
+      if (rc) return rc;
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "capture of the multigrid cycle");
+      break;
+    }
     h.gparams[k] = p;
   }
   int slot = (h.io_slot++) & 63;

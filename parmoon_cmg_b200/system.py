@@ -135,6 +135,11 @@ class Context:
                                                C.byref(h1)))
         return l2.value, h1.value
 
+    def write_vtk(self, sid, sol, path, name="u", on_device=False):
+        """Legacy VTK file of a solution (host array, or a device pointer with on_device)."""
+        ptr = C.c_void_p(sol) if on_device else _p(_f64(sol))
+        self.check(self.lib.cdgpu_write_vtk(self.h, sid, ptr, 1 if on_device else 0, path.encode(), name.encode()))
+
     def add_neumann(self, sid, cells, edges, g, n_dof=None):
         """Add Neumann data; returns the updated right-hand side when n_dof is given."""
         cells, edges, g = _i32(cells), _i32(edges), _f64(g)

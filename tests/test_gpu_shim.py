@@ -147,10 +147,12 @@ def laplace_oracle_solution(oracle):
     return x, oracle.dof_coords(3, 2, fin["coords"], fin["global_numbers"], fin["begin_index"], fin["n_dof"])
 
 
-def test_errors_table_reproduces_reference_output(cpu_errors):
-    """GetErrors on the device for any exact solution (cdgpu_errors_table): the Laplace example
-    solved through the C ABI on the reference's own mesh and DOF numbering gives the L2 and
-    H1-semi errors that the reference's CD3D main prints, digit for digit."""
+@pytest.fixture(scope="module")
+def laplace_gpu():
+    """The Laplace example solved through the C ABI on the reference's own mesh and DOF
+    numbering (cd3d_dump with the same .dat), coefficients tabulated at the library's
+    quadrature points, the exact solution as Dirichlet data."""
+    import oracle
     import refdump
     from parmoon_cmg_b200 import _build, _lib
     from parmoon_cmg_b200.system import Context, coeffs, solver_params
@@ -166,37 +168,90 @@ def test_errors_table_reproduces_reference_output(cpu_errors):
         d = refdump.load_dir(out)
     lv = [refdump.level(d, l) for l in range(int(d["levels"]))]
     ctx = Context(0)
-    try:
-        sids = []
-        for S in lv:
-            sid = ctx.upload_space(dict(dim=3, order=2, coords=S["coords"], global_numbers=S["global_numbers"],
-                                        begin_index=S["begin_index"], n_dof=S["n_dof"], n_active=S["n_active"]))
-            ctx.build_pattern(sid)
-            nc = len(S["begin_index"]) - 1
-            q = ctx.quadrature_points(sid, nc, 3)
-            tab = np.zeros(q.shape[:2] + (6,))
-            tab[..., 0] = 1.0
-            tab[..., 5] = 3 * np.pi ** 2 * np.prod(np.sin(np.pi * q), axis=-1)
-            ctx.set_coeffs(sid, coeffs(_lib.COEFF_TABLE), tab)
-            sids.append(sid)
-        mg = ctx.hierarchy(sids, [None] + [S["parent"] for S in lv[1:]])
-        import oracle
-        rhs = None
-        for S, sid in zip(lv, sids):
-            xyz = oracle.dof_coords(3, 2, S["coords"], S["global_numbers"], S["begin_index"], S["n_dof"])
-            g = np.prod(np.sin(np.pi * xyz[S["n_active"]:]), axis=-1)
-            _, rhs = ctx.assemble(sid, 1, S["n_dof"], 1, dirichlet=g, want_entries=False)
-        fin = lv[-1]
-        sol0 = np.zeros(fin["n_dof"])
-        sol0[fin["n_active"]:] = rhs[fin["n_active"]:]
-        x, info = ctx.solve(mg, solver_params(coarse_smoother=3, red_factor=1e-13, maxit=30), rhs, sol0)
-        assert info.status == 0
-        nc = len(fin["begin_index"]) - 1
-        q = ctx.quadrature_points(sids[-1], nc, 3)
-        s, c = np.sin(np.pi * q), np.cos(np.pi * q)
-        ex = np.stack([s[..., 0] * s[..., 1] * s[..., 2], np.pi * c[..., 0] * s[..., 1] * s[..., 2],
-                       np.pi * s[..., 0] * c[..., 1] * s[..., 2], np.pi * s[..., 0] * s[..., 1] * c[..., 2]], -1)
-        l2, h1 = ctx.errors_table(sids[-1], x, ex)
-    finally:
-        ctx.close()
+    sids = []
+    for S in lv:
+        sid = ctx.upload_space(dict(dim=3, order=2, coords=S["coords"], global_numbers=S["global_numbers"],
+                                    begin_index=S["begin_index"], n_dof=S["n_dof"], n_active=S["n_active"]))
+        ctx.build_pattern(sid)
+        nc = len(S["begin_index"]) - 1
+        q = ctx.quadrature_points(sid, nc, 3)
+        tab = np.zeros(q.shape[:2] + (6,))
+        tab[..., 0] = 1.0
+        tab[..., 5] = 3 * np.pi ** 2 * np.prod(np.sin(np.pi * q), axis=-1)
+        ctx.set_coeffs(sid, coeffs(_lib.COEFF_TABLE), tab)
+        sids.append(sid)
+    mg = ctx.hierarchy(sids, [None] + [S["parent"] for S in lv[1:]])
+    rhs = None
+    for S, sid in zip(lv, sids):
+        xyz = oracle.dof_coords(3, 2, S["coords"], S["global_numbers"], S["begin_index"], S["n_dof"])
+        g = np.prod(np.sin(np.pi * xyz[S["n_active"]:]), axis=-1)
+        _, rhs = ctx.assemble(sid, 1, S["n_dof"], 1, dirichlet=g, want_entries=False)
+    fin = lv[-1]
+    sol0 = np.zeros(fin["n_dof"])
+    sol0[fin["n_active"]:] = rhs[fin["n_active"]:]
+    x, info = ctx.solve(mg, solver_params(coarse_smoother=3, red_factor=1e-13, maxit=30), rhs, sol0)
+    assert info.status == 0
+    yield dict(ctx=ctx, sids=sids, lv=lv, x=x)
+    ctx.close()
+
+
+def test_errors_table_reproduces_reference_output(cpu_errors, laplace_gpu):
+    """GetErrors on the device for any exact solution (cdgpu_errors_table): the L2 and H1-semi
+    errors that the reference's CD3D main prints, digit for digit."""
+    ctx, sids, fin, x = laplace_gpu["ctx"], laplace_gpu["sids"], laplace_gpu["lv"][-1], laplace_gpu["x"]
+    nc = len(fin["begin_index"]) - 1
+    q = ctx.quadrature_points(sids[-1], nc, 3)
+    s, c = np.sin(np.pi * q), np.cos(np.pi * q)
+    ex = np.stack([s[..., 0] * s[..., 1] * s[..., 2], np.pi * c[..., 0] * s[..., 1] * s[..., 2],
+                   np.pi * s[..., 0] * c[..., 1] * s[..., 2], np.pi * s[..., 0] * s[..., 1] * c[..., 2]], -1)
+    l2, h1 = ctx.errors_table(sids[-1], x, ex)
     assert (f"{l2:g}", f"{h1:g}") == cpu_errors, ((l2, h1), cpu_errors)
+
+
+def read_vtk(path):
+    """POINTS, CELLS (connectivity rows) and the first POINT_DATA scalar field of a legacy VTK file."""
+    tok = open(path).read().split()
+    i = tok.index("POINTS")
+    n = int(tok[i + 1])
+    pts = np.array(tok[i + 3:i + 3 + 3 * n], float).reshape(n, 3)
+    i = tok.index("CELLS")
+    nc = int(tok[i + 1])
+    cells, j = [], i + 3
+    for _ in range(nc):
+        k = int(tok[j])
+        cells.append([int(t) for t in tok[j + 1:j + 1 + k]])
+        j += k + 1
+    i = tok.index("POINT_DATA")
+    j = tok.index("LOOKUP_TABLE", i) + 2
+    vals = np.array(tok[j:j + n], float)
+    return pts, cells, vals
+
+
+def test_vtk_from_device_buffer_matches_reference_output(laplace_gpu):
+    """cdgpu_write_vtk from a solution held on the device writes the points, hexahedra and
+    vertex values that the reference's own TOutput3D::WriteVtk writes for the same problem
+    (its CD3D main with WRITE_VTK), up to the order of the points and the printed digits."""
+    import torch
+    ctx, sid, x = laplace_gpu["ctx"], laplace_gpu["sids"][-1], laplace_gpu["x"]
+    with tempfile.TemporaryDirectory() as tmp:
+        dat = os.path.join(tmp, "v.dat")
+        with open(dat, "w") as f:
+            f.write(DAT.format(out=os.path.join(tmp, "v.out"), mesh=os.path.join(ROOT, "oracle", "meshes"))
+                    .replace("WRITE_VTK: 0", "WRITE_VTK: 1\nVTKBASENAME: ref"))
+        subprocess.run([os.path.join(REF, "cd3d_main"), dat], cwd=tmp, check=True, capture_output=True, timeout=600)
+        vtks = sorted(f for f in os.listdir(os.path.join(tmp, "VTK")) if f.endswith(".vtk"))
+        assert vtks, "the reference wrote no VTK file"
+        p_ref, c_ref, v_ref = read_vtk(os.path.join(tmp, "VTK", vtks[-1]))
+        d_x = torch.tensor(x, device="cuda:0")
+        torch.cuda.synchronize()
+        ours = os.path.join(tmp, "ours.vtk")
+        ctx.write_vtk(sid, d_x.data_ptr(), ours, on_device=True)
+        p, cells, v = read_vtk(ours)
+    assert len(p) == len(p_ref) and len(cells) == len(c_ref)
+    key = lambda P: np.rint(P * 8).astype(np.int64) @ np.array([1, 9, 81])
+    o, o_ref = np.argsort(key(p)), np.argsort(key(p_ref))
+    assert np.array_equal(key(p)[o], key(p_ref)[o_ref])
+    assert np.abs(v[o] - v_ref[o_ref]).max() <= 1e-5 * np.abs(v_ref).max()
+    # the same cells, as sets of vertex positions
+    cell_key = lambda P, C: sorted(tuple(sorted(key(P[c]).tolist())) for c in C)
+    assert cell_key(p, cells) == cell_key(p_ref, c_ref)
