@@ -184,12 +184,18 @@ int cdgpu_write_vtk(cdgpu_ctx *ctx, int space_id, const double *sol, int sol_on_
  * h_dirichlet: values of DOFs [n_active, n_dof) (BoundValue at the nodes), NULL = 0. */
 int cdgpu_assemble(cdgpu_ctx *ctx, int space_id, int disctype, const double *h_dirichlet,
                    double *h_entries, double *h_rhs);
-/* Neumann boundary data: adds sum_q hE w_q g_q phi_k(x_q) to active rows, like the
- * NEUMANN branch of Assemble2D (src/FE/Assemble2D.C:797-827).  Per edge: its cell,
- * local edge m (vertices m, m+1), and g at the (order+1) Gauss points of the edge in
- * ascending order from vertex m.  h_rhs (nullable) receives the updated right-hand side. */
+/* Neumann boundary data: adds sum_q |J_q| w_q g_q phi_k(x_q) to active rows, like the
+ * NEUMANN branch of Assemble2D (src/FE/Assemble2D.C:797-827) and the NEUMANN / ROBIN branch of
+ * TAssembleMat3D::Assemble3D (src/System/AssembleMat3D.C:1068-1170).  2D: per edge its cell,
+ * local edge m (vertices m, m+1) and g at the (order+1) Gauss points from vertex m; 3D: per face
+ * its cell, local face m (THexahedron's face-vertex table) and g at the (order+1)^2 Gauss points
+ * of the face, in the order cdgpu_boundary_points lists them.  h_rhs (nullable) receives the
+ * updated right-hand side. */
 int cdgpu_add_neumann(cdgpu_ctx *ctx, int space_id, int n_edges, const int *h_cell,
                       const int *h_local_edge, const double *h_g, double *h_rhs);
+/* physical coordinates (n x points x dim) of the Gauss points of boundary edges (2D) or faces
+ * (3D) at which cdgpu_add_neumann expects g (the points where the reference calls BoundValue) */
+int cdgpu_boundary_points(cdgpu_ctx *ctx, int space_id, int n, const int *h_cell, const int *h_local, double *h_xyz);
 
 /* --- matrix-vector products -------------------------------------------------
  * Replace MatVect / MatVect_Scalar and ScalarDefect / Defect_Scalar

@@ -63,6 +63,7 @@ SIGNATURES = {
     "cdgpu_quadrature_points": (_I, [_P, _I, _P, C.POINTER(_I)]),
     "cdgpu_assemble": (_I, [_P, _I, _I, _P, _P, _P]),
     "cdgpu_add_neumann": (_I, [_P, _I, _I, _P, _P, _P, _P]),
+    "cdgpu_boundary_points": (_I, [_P, _I, _I, _P, _P, _P]),
     "cdgpu_spmv": (_I, [_P, _I, _P, _P]),
     "cdgpu_defect": (_I, [_P, _I, _P, _P, _P, C.POINTER(C.c_double)]),
     "cdgpu_errors": (_I, [_P, _I, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),

@@ -66,7 +66,7 @@ static void free_mg(Hierarchy *h)
   for (auto &g : h->gexec)
     if (g) cudaGraphExecDestroy(g);
   void *ptrs[] = {h->d_cinv, h->d_cpiv, h->d_V, h->d_Z, h->d_w, h->d_ctl, h->d_partial, h->d_x, h->d_b,
-                  h->d_io, h->d_coop_bar};
+                  h->d_io, h->d_gs_count};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -387,6 +387,17 @@ int cdgpu_add_neumann(cdgpu_ctx *ctx, int space_id, int n_edges, const int *h_ce
     CD_CUDA(ctx, cudaMemcpyAsync(h_rhs, s->d_rhs, sizeof(double) * s->n_dof, cudaMemcpyDeviceToHost, ctx->stream));
     CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
+  return CDGPU_OK;
+}
+
+int cdgpu_boundary_points(cdgpu_ctx *ctx, int space_id, int n, const int *h_cell, const int *h_local, double *h_xyz)
+{
+  Space *s = get_space(ctx, space_id);
+  if (!s || n < 0 || (n > 0 && (!h_cell || !h_local || !h_xyz))) return fail(ctx, CDGPU_ERR_INVALID, "boundary_points: bad argument");
+  for (int e = 0; e < n; e++)
+    if (h_cell[e] < 0 || h_cell[e] >= s->n_cells || h_local[e] < 0 || h_local[e] > (s->dim == 2 ? 3 : 5))
+      return fail(ctx, CDGPU_ERR_INVALID, "boundary_points: bad cell or edge/face index");
+  boundary_points(*s, n, h_cell, h_local, h_xyz);
   return CDGPU_OK;
 }
 

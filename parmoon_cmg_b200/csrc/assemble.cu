@@ -1001,26 +1001,149 @@ __global__ void neumann_kernel(int order, int nbf, int n_edges, const double *co
   }
 }
 
+// ---------------------------------------------------------------------------
+// Neumann data on hexahedron faces (the NEUMANN / ROBIN branch of TAssembleMat3D::Assemble3D,
+// src/System/AssembleMat3D.C:1068-1170): face m of a cell has the vertices kHexFace[m]
+// (THexahedron's face-vertex table) and the bilinear map of the face square [-1,1]^2 through
+// them; per Gauss point (t_i, s_j) of an (order+1)^2 rule the area element |n| is the norm of
+// the cross product of the map's two derivatives, and the basis functions are evaluated at the
+// same bilinear combination of the reference cube's face corners.  One CTA, faces in order.
+// ---------------------------------------------------------------------------
+__constant__ int kHexFace[6][4] = {{0, 1, 2, 3}, {0, 4, 5, 1}, {1, 5, 6, 2}, {2, 6, 7, 3}, {0, 3, 7, 4}, {4, 7, 6, 5}};
+
+__host__ __device__ inline void gauss_1d(int nl, double *z, double *w)
+{
+  if (nl == 2) { z[0] = -1.0 / sqrt(3.0); z[1] = -z[0]; w[0] = w[1] = 1.0; }
+  else { z[0] = -sqrt(0.6); z[1] = 0; z[2] = sqrt(0.6); w[0] = w[2] = 5.0 / 9.0; w[1] = 8.0 / 9.0; }
+}
+
+__device__ inline double lagrange_1d(int order, int k, double x)
+{
+  if (order == 1) return k ? 0.5 * (1 + x) : 0.5 * (1 - x);
+  return k == 0 ? 0.5 * x * (x - 1) : k == 1 ? 1 - x * x : 0.5 * x * (x + 1);
+}
+
+__global__ void neumann3d_kernel(int order, int nbf, int n_faces, const double *coords, const int *gn, int n_active,
+                                 const int *cell, const int *face, const double *g, double *rhs)
+{
+  const int nl = order + 1, nq = nl * nl, p1 = order + 1;
+  double z[3], w[3];
+  gauss_1d(nl, z, w);
+  for (int e = 0; e < n_faces; e++)
+  {
+    const int c = cell[e], m = face[e];
+    const double *V = coords + (size_t)c * 24;
+    double X[4][3], R[4][3];
+    for (int k = 0; k < 4; k++)
+    {
+      const int v = kHexFace[m][k];
+      for (int a = 0; a < 3; a++) X[k][a] = V[v * 3 + a];
+      R[k][0] = (v == 1 || v == 2 || v == 5 || v == 6) ? 1.0 : -1.0;
+      R[k][1] = (v == 2 || v == 3 || v == 6 || v == 7) ? 1.0 : -1.0;
+      R[k][2] = v >= 4 ? 1.0 : -1.0;
+    }
+    double c1[3], c2[3], c3[3];
+    for (int a = 0; a < 3; a++)
+    {
+      c1[a] = (-X[0][a] + X[1][a] + X[2][a] - X[3][a]) * 0.25;
+      c2[a] = (-X[0][a] - X[1][a] + X[2][a] + X[3][a]) * 0.25;
+      c3[a] = (X[0][a] - X[1][a] + X[2][a] - X[3][a]) * 0.25;
+    }
+    const int k = threadIdx.x;
+    if (k < nbf)
+    {
+      const int kx = k % p1, ky = (k / p1) % p1, kz = k / (p1 * p1);
+      double add = 0;
+      for (int q = 0; q < nq; q++)
+      {
+        const double t = z[q % nl], s = z[q / nl];
+        const double t0 = 0.5 * (t + 1), t1 = 0.5 * (s + 1);
+        const double L[4] = {(1 - t0) * (1 - t1), t0 * (1 - t1), t0 * t1, (1 - t0) * t1};
+        double xi[3] = {0, 0, 0};
+        for (int j = 0; j < 4; j++)
+          for (int a = 0; a < 3; a++) xi[a] += L[j] * R[j][a];
+        double d1[3], d2[3];
+        for (int a = 0; a < 3; a++)
+        {
+          d1[a] = c1[a] + s * c3[a];
+          d2[a] = c2[a] + t * c3[a];
+        }
+        const double nx = d1[1] * d2[2] - d1[2] * d2[1], ny = d1[2] * d2[0] - d1[0] * d2[2],
+                     nz = d1[0] * d2[1] - d1[1] * d2[0];
+        const double phi = lagrange_1d(order, kx, xi[0]) * lagrange_1d(order, ky, xi[1]) * lagrange_1d(order, kz, xi[2]);
+        add += g[(size_t)e * nq + q] * w[q % nl] * w[q / nl] * sqrt(nx * nx + ny * ny + nz * nz) * phi;
+      }
+      const int d = gn[(size_t)c * nbf + k];
+      if (d < n_active) rhs[d] += add;
+    }
+    __syncthreads();
+  }
+}
+
+// physical coordinates of the Gauss points of boundary edges (2D) or faces (3D), in the order
+// add_neumann expects the data: 2D (order+1) points from vertex m towards m+1; 3D (order+1)^2
+// points q = i + (order+1) j at (t_i, s_j) of the face's bilinear map
+void boundary_points(const Space &s, int n, const int *cell, const int *local, double *xyz)
+{
+  const int nl = s.order + 1;
+  double z[3], w[3];
+  gauss_1d(nl, z, w);
+  static const int hf[6][4] = {{0, 1, 2, 3}, {0, 4, 5, 1}, {1, 5, 6, 2}, {2, 6, 7, 3}, {0, 3, 7, 4}, {4, 7, 6, 5}};
+  for (int e = 0; e < n; e++)
+  {
+    const double *V = &s.h_coords[(size_t)cell[e] * s.nv * s.dim];
+    const int m = local[e];
+    if (s.dim == 2)
+    {
+      const int m1 = (m + 1) % 4;
+      for (int l = 0; l < nl; l++)
+      {
+        const double t = 0.5 * (z[l] + 1);
+        for (int a = 0; a < 2; a++) xyz[((size_t)e * nl + l) * 2 + a] = V[2 * m + a] + (V[2 * m1 + a] - V[2 * m + a]) * t;
+      }
+    }
+    else
+      for (int q = 0; q < nl * nl; q++)
+      {
+        const double t0 = 0.5 * (z[q % nl] + 1), t1 = 0.5 * (z[q / nl] + 1);
+        const double L[4] = {(1 - t0) * (1 - t1), t0 * (1 - t1), t0 * t1, (1 - t0) * t1};
+        for (int a = 0; a < 3; a++)
+        {
+          double x = 0;
+          for (int j = 0; j < 4; j++) x += L[j] * V[hf[m][j] * 3 + a];
+          xyz[((size_t)e * nl * nl + q) * 3 + a] = x;
+        }
+      }
+  }
+}
+
 int add_neumann(cdgpu_ctx *ctx, Space &s, int n_edges, const int *cell, const int *edge,
                 const double *g)
 {
-  if (s.dim != 2) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "Neumann data: 2D only");
   if (!s.assembled) return fail(ctx, CDGPU_ERR_INVALID, "Neumann data: assemble first");
   if (n_edges <= 0) return CDGPU_OK;
-  int nl = s.order + 1, rc;
+  int nl = s.dim == 2 ? s.order + 1 : (s.order + 1) * (s.order + 1), rc;
+  const int max_local = s.dim == 2 ? 3 : 5;
   int *d_cell = nullptr, *d_edge = nullptr;
   double *d_g = nullptr;
   if ((rc = dev_alloc(ctx, &d_cell, n_edges)) || (rc = dev_alloc(ctx, &d_edge, n_edges)) ||
       (rc = dev_alloc(ctx, &d_g, (size_t)n_edges * nl)))
     return rc;
   for (int e = 0; e < n_edges; e++)
-    if (cell[e] < 0 || cell[e] >= s.n_cells || edge[e] < 0 || edge[e] > 3)
-      return fail(ctx, CDGPU_ERR_INVALID, "Neumann data: bad cell or edge index");
+    if (cell[e] < 0 || cell[e] >= s.n_cells || edge[e] < 0 || edge[e] > max_local)
+    {
+      cudaFree(d_cell); cudaFree(d_edge); cudaFree(d_g);
+      return fail(ctx, CDGPU_ERR_INVALID, "Neumann data: bad cell or edge/face index");
+    }
   CD_CUDA(ctx, cudaMemcpyAsync(d_cell, cell, sizeof(int) * n_edges, cudaMemcpyHostToDevice, ctx->stream));
   CD_CUDA(ctx, cudaMemcpyAsync(d_edge, edge, sizeof(int) * n_edges, cudaMemcpyHostToDevice, ctx->stream));
   CD_CUDA(ctx, cudaMemcpyAsync(d_g, g, sizeof(double) * n_edges * nl, cudaMemcpyHostToDevice, ctx->stream));
-  neumann_kernel<<<1, 32, 0, ctx->stream>>>(s.order, s.nbf, n_edges, s.d_coords, s.d_gn, s.n_active,
-                                            d_cell, d_edge, d_g, s.d_rhs);
+  if (s.dim == 2)
+    neumann_kernel<<<1, 32, 0, ctx->stream>>>(s.order, s.nbf, n_edges, s.d_coords, s.d_gn, s.n_active,
+                                              d_cell, d_edge, d_g, s.d_rhs);
+  else
+    neumann3d_kernel<<<1, 32, 0, ctx->stream>>>(s.order, s.nbf, n_edges, s.d_coords, s.d_gn, s.n_active,
+                                                d_cell, d_edge, d_g, s.d_rhs);
   CD_LAUNCHED(ctx);
   CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   cudaFree(d_cell); cudaFree(d_edge); cudaFree(d_g);

@@ -158,11 +158,7 @@ struct Hierarchy
   cudaEvent_t ev_slot[2] = {nullptr, nullptr}; // recorded behind each slot's copy
   int *h_cflag = nullptr;     // pinned copy of the coarse inversion's zero-pivot flag
   bool cflag_pending = false; // copy enqueued, not yet checked
-  // the FP32 V-cycle below the finest level as one cooperative kernel (coop.cuh): its
-  // barrier words and whether the last capture used it (false after a failed attempt)
-  unsigned *d_coop_bar = nullptr;
-  bool coop_failed = false;
-  bool coop_used = false;
+  unsigned *d_gs_count = nullptr; // arrival counter of the Gram-Schmidt passes' last-block reduction
 };
 
 // ---------------------------------------------------------------------------
@@ -190,8 +186,6 @@ struct cdgpu_ctx
   // set while the multigrid cycle is recorded into its graph: its kernels load the data that
   // no kernel of the cycle writes before waiting for their predecessor
   bool pdl_pre = false;
-  // set while the FP32 cycle is recorded: grid of the cooperative coarse-cycle kernel (0: none)
-  int coop_grid_hint = 0;
   int *d_err = nullptr; // assembly error flag (device) and its pinned host mirror
   int *h_err = nullptr;
 };
@@ -283,6 +277,7 @@ int assemble_check(cdgpu_ctx *ctx);
 int err_flag_status(cdgpu_ctx *ctx);
 int add_neumann(cdgpu_ctx *ctx, Space &s, int n_edges, const int *cell, const int *edge,
                 const double *g);
+void boundary_points(const Space &s, int n, const int *cell, const int *local, double *xyz);
 int spmv64(cdgpu_ctx *ctx, const Space &s, const double *x, double *y);
 int defect64(cdgpu_ctx *ctx, const Space &s, const double *x, const double *f, double *d,
              double *res);

@@ -29,7 +29,6 @@
 #include "internal.h"
 #include "csr.cuh"
 #include "mf.cuh"
-#include "coop.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -261,14 +260,18 @@ __global__ void coarse_smooth_kernel(int n, int n_active, const int *__restrict_
 //   GS_AXPY_DOTS  w -= sum_j coef_j Y_j, then partial dots of the new w with every Y_j
 //   GS_AXPY_NORM  w -= sum_j coef_j Y_j, then partial ||w||^2
 // Every thread keeps the K basis values of its row in registers; per-block partials go to
-// partial[block * 33 + slot] and are summed in block order by reduce_partials_kernel.
+// partial[block * 33 + slot] and are summed in block order by the pass's last block.
 enum { GS_DOTS = 0, GS_AXPY_DOTS = 1, GS_AXPY_NORM = 2 };
 
+// The last block to finish (an arrival counter, reset by that block) sums the per-block
+// partials of every slot in block order into out[slot] (lanes over blocks, then a fixed
+// warp tree), so no separate reduction kernel is launched.
 template <int K, int MODE>
 __global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, const double *__restrict__ Y,
                                                          double *__restrict__ w,
                                                          const double *__restrict__ coef,
-                                                         double *__restrict__ partial)
+                                                         double *__restrict__ partial,
+                                                         double *__restrict__ out, unsigned *__restrict__ counter)
 {
   CD_PDL_ENTRY();
   constexpr int NS = MODE == GS_AXPY_NORM ? 1 : K;
@@ -313,16 +316,31 @@ __global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, const double *__
     double t = 0;
     for (int g = 0; g < kBlock / 32; g++) t += red[g][threadIdx.x];
     partial[(size_t)blockIdx.x * 33 + threadIdx.x] = t;
+    __threadfence();
   }
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int j = warp; j < NS; j += kBlock / 32)
+  {
+    double t = 0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) t += *(volatile double *)(partial + (size_t)b * 33 + j);
+    t = group_sum<32>(t);
+    if (lane == 0) out[j] = t;
+  }
+  if (threadIdx.x == 0) *counter = 0u;
 }
 
 template <int MODE>
 static void launch_gs(int k, int grid, cudaStream_t st, int n, const double *Y, double *w, const double *coef,
-                      double *partial)
+                      double *partial, double *out, unsigned *counter)
 {
   switch (k)
   {
-#define CD_GS_CASE(K) case K: (void)cd_launch(gs_pass_kernel<K, MODE>, grid, kBlock, 0, st, n, Y, w, coef, partial); break;
+#define CD_GS_CASE(K) case K: (void)cd_launch(gs_pass_kernel<K, MODE>, grid, kBlock, 0, st, n, Y, w, coef, partial, out, counter); break;
     CD_GS_CASE(1) CD_GS_CASE(2) CD_GS_CASE(3) CD_GS_CASE(4) CD_GS_CASE(5) CD_GS_CASE(6) CD_GS_CASE(7)
     CD_GS_CASE(8) CD_GS_CASE(9) CD_GS_CASE(10) CD_GS_CASE(11) CD_GS_CASE(12) CD_GS_CASE(13) CD_GS_CASE(14)
     CD_GS_CASE(15) CD_GS_CASE(16) CD_GS_CASE(17) CD_GS_CASE(18) CD_GS_CASE(19) CD_GS_CASE(20) CD_GS_CASE(21)
@@ -330,26 +348,6 @@ static void launch_gs(int k, int grid, cudaStream_t st, int n, const double *Y, 
     CD_GS_CASE(29) CD_GS_CASE(30) CD_GS_CASE(31) CD_GS_CASE(32)
 #undef CD_GS_CASE
     default: break;
-  }
-}
-
-// out[j] = sum_b partial[b][j] for j < nslots, one block per slot, fixed summation order
-__global__ void reduce_partials_kernel(int nblocks, int nslots, const double *__restrict__ partial,
-                                       double *__restrict__ out)
-{
-  CD_PDL_ENTRY();
-  __shared__ double red[32];
-  const int j = blockIdx.x;
-  double t = 0;
-  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) t += partial[(size_t)b * 33 + j];
-  t = group_sum<32>(t);
-  if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = t;
-  __syncthreads();
-  if (threadIdx.x == 0)
-  {
-    double s = 0;
-    for (int w = 0; w < (int)blockDim.x / 32; w++) s += red[w];
-    out[j] = s;
   }
 }
 
@@ -640,7 +638,6 @@ template <typename T> static int jacobi_first(cdgpu_ctx *ctx, Level &L, T omega,
 struct CycleState
 {
   const cdgpu_solver_params *p;
-  int coop_grid = 0; // > 0: the levels below the finest run as one cooperative kernel of this many CTAs
   int rec[64];
   int pre_done[64];    // pre-smoothing sweeps already done (fused into the cycle's start)
   bool sol_zero[64];   // active part and Dirichlet part zero
@@ -689,87 +686,6 @@ template <typename T> static int coarse_solve(cdgpu_ctx *ctx, Hierarchy &h, Cycl
   return CDGPU_OK;
 }
 
-// The FP32 V-cycle of levels 0 .. L-2 as one cooperative kernel (coop.cuh), when the cycle is
-// a V-cycle with the exact coarse solve, no level below the finest uses the matrix-free
-// operator, and every CTA of the grid can be resident.  Returns the grid size, 0 if not.
-static int coop_grid_size(cdgpu_ctx *ctx, const Hierarchy &h, const cdgpu_solver_params &p)
-{
-  const int L = (int)h.lev.size();
-  if (h.coop_failed || L < 3 || L - 1 > kCoopMaxLevels || p.cycle != 1 || p.coarse_smoother != 17 || p.pre < 0 || p.post < 0)
-    return 0;
-  if (const char *v = getenv("CDGPU_COOP_CYCLE"))
-    if (v[0] == '0') return 0;
-  for (int l = 0; l < L - 1; l++)
-    if (use_mf(*h.lev[l].sp)) return 0;
-  const Space &c = *h.lev[0].sp;
-  const size_t smem = sizeof(double) * (c.n_dof + c.n_active);
-  if (smem > 48 * 1024) return 0;
-  int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mg_coop_cycle_kernel, kCoopThreads, smem) != cudaSuccess)
-  {
-    cudaGetLastError();
-    return 0;
-  }
-  return nb > 0 ? ctx->sm_count * std::min(nb, 2) : 0;
-}
-
-static int launch_coop_cycle(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, int grid)
-{
-  const int top = (int)h.lev.size() - 2;
-  CoopArgs a;
-  std::memset(&a, 0, sizeof(a));
-  a.top = top;
-  a.pre = p.pre;
-  a.post = p.post;
-  a.omega = (float)p.omega;
-  a.damp = (float)p.gmg_damp;
-  for (int i = 0; i <= top; i++)
-  {
-    const Level &L = h.lev[i];
-    const Space &s = *L.sp;
-    CoopLevel &c = a.lev[i];
-    c.n = s.n_dof;
-    c.n_active = s.n_active;
-    c.gs = s.shape.gs;
-    c.rp = s.d_row_ptr;
-    c.kc = s.d_kcol;
-    c.a = s.d_a32;
-    c.diag = s.d_diag32;
-    c.sol = L.v32.sol;
-    c.alt = L.v32.alt;
-    c.rhs = L.v32.rhs;
-    c.def = L.v32.def;
-    if (i > 0)
-    {
-      c.r_row = L.d_r_row; c.r_col = L.d_r_col; c.r_val = L.d_r_val32; c.r_gs = L.r_shape.gs;
-      c.p_row = L.d_p_row; c.p_col = L.d_p_col; c.p_val = L.d_p_val32; c.p_gs = L.p_shape.gs;
-    }
-  }
-  const Space &c0 = *h.lev[0].sp;
-  a.a0 = c0.d_a;
-  a.dir_start0 = c0.d_dir_start;
-  a.cinv = h.d_cinv;
-  a.bar = h.d_coop_bar;
-  a.err = ctx->d_err;
-  CD_CUDA(ctx, cudaMemsetAsync(h.d_coop_bar, 0, 4 * sizeof(unsigned), ctx->stream));
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = kCoopThreads;
-  cfg.dynamicSmemBytes = sizeof(double) * (c0.n_dof + c0.n_active);
-  cfg.stream = ctx->stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  CD_CUDA(ctx, cudaLaunchKernelEx(&cfg, mg_coop_cycle_kernel, a));
-  ctx->launches++;
-  // the host's view of the top level's buffers after its pre + post sweeps inside the kernel
-  Level &T = h.lev[top];
-  if ((p.pre + p.post) % 2) std::swap(T.v32.sol, T.v32.alt);
-  return CDGPU_OK;
-}
-
 template <typename T> static int cycle(cdgpu_ctx *ctx, Hierarchy &h, CycleState &cs, int i)
 {
   if (i == 0) return coarse_solve<T>(ctx, h, cs);
@@ -795,18 +711,8 @@ template <typename T> static int cycle(cdgpu_ctx *ctx, Hierarchy &h, CycleState 
   csr_restrict<T>(ctx, L, sc, v.def, vc.rhs, vc.sol);
   CD_LAUNCHED(ctx);
   cs.sol_zero[i - 1] = cs.active_zero[i - 1] = true;
-  bool coop = false;
-  if constexpr (std::is_same<T, float>::value)
-  {
-    if (cs.coop_grid > 0 && i == (int)h.lev.size() - 1)
-    {
-      if ((rc = launch_coop_cycle(ctx, h, *cs.p, cs.coop_grid))) return rc;
-      coop = true;
-    }
-  }
-  if (!coop)
-    for (int j = 0; j < cs.rec[i]; j++)
-      if ((rc = cycle<T>(ctx, h, cs, i - 1))) return rc;
+  for (int j = 0; j < cs.rec[i]; j++)
+    if ((rc = cycle<T>(ctx, h, cs, i - 1))) return rc;
   if (cs.p->cycle < 1) cs.rec[i] = 1;
   csr_prolong<T>(ctx, L, s, vc.sol, v.sol, (T)cs.p->gmg_damp);
   CD_LAUNCHED(ctx);
@@ -826,7 +732,6 @@ template <typename T> static int mg_record(cdgpu_ctx *ctx, Hierarchy &h, const c
   int n = F.sp->n_dof;
   CycleState cs;
   cs.p = &p;
-  if constexpr (std::is_same<T, float>::value) cs.coop_grid = ctx->coop_grid_hint;
   // SetRecursion(levels = L-1), MultiGrid3D.C:691-703
   cs.rec[1] = 1;
   for (int k = 2; k <= L - 1; k++) cs.rec[k] = p.cycle > 0 ? p.cycle : 2;
@@ -884,40 +789,20 @@ static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, 
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_exact_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm1));
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_smooth_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm2));
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_smooth_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm2));
-    // the FP32 cycle below the finest level as one cooperative kernel where possible; if the
-    // capture or instantiation with it fails, the cycle is captured again kernel by kernel
-    for (int attempt = 0; attempt < 2; attempt++)
-    {
-      ctx->coop_grid_hint = k == 1 ? coop_grid_size(ctx, h, p) : 0;
-      if (ctx->coop_grid_hint > 0 && !h.d_coop_bar && (rc = dev_alloc(ctx, &h.d_coop_bar, 4))) return rc;
-      cudaGraph_t g = nullptr;
-      const long long before = ctx->launches;
-      CD_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-      ctx->pdl_pre = true; // kernels of the cycle load matrix data before waiting (CD_PDL_WAIT)
-      rc = k == 1 ? mg_record<float>(ctx, h, p) : mg_record<double>(ctx, h, p);
-      ctx->pdl_pre = false;
-      cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
-      h.graph_nodes[k] = ctx->launches - before; // kernels per replay; capturing runs none
-      ctx->launches = before;
-      if (rc == CDGPU_OK && e == cudaSuccess)
-      {
-        e = cudaGraphInstantiate(&h.gexec[k], g, 0);
-        if (e != cudaSuccess) h.gexec[k] = nullptr;
-      }
-      if (g) cudaGraphDestroy(g);
-      const bool ok = rc == CDGPU_OK && e == cudaSuccess;
-      if (!ok && ctx->coop_grid_hint > 0)
-      {
-        cudaGetLastError();
-        h.coop_failed = true; // retry without the cooperative kernel
-        continue;
-      }
-      h.coop_used = ok && ctx->coop_grid_hint > 0;
-      ctx->coop_grid_hint = 0;
-      if (rc) return rc;
-      if (e != cudaSuccess) return cuda_fail(ctx, e, "capture of the multigrid cycle");
-      break;
-    }
+    cudaGraph_t g = nullptr;
+    const long long before = ctx->launches;
+    CD_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    ctx->pdl_pre = true; // kernels of the cycle load matrix data before waiting (CD_PDL_WAIT)
+    rc = k == 1 ? mg_record<float>(ctx, h, p) : mg_record<double>(ctx, h, p);
+    ctx->pdl_pre = false;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    h.graph_nodes[k] = ctx->launches - before; // kernels per replay; capturing runs none
+    ctx->launches = before;
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture of the multigrid cycle");
+    e = cudaGraphInstantiate(&h.gexec[k], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { h.gexec[k] = nullptr; return cuda_fail(ctx, e, "graph instantiate"); }
     h.gparams[k] = p;
   }
   int slot = (h.io_slot++) & 63;
@@ -1104,6 +989,8 @@ int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m)
     for (auto &e : h.ev_slot) CD_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     CD_CUDA(ctx, cudaMallocHost((void **)&h.h_io, 128 * sizeof(double *)));
     if ((rc = dev_alloc(ctx, &h.d_io, 2))) return rc;
+    if ((rc = dev_alloc(ctx, &h.d_gs_count, 1))) return rc;
+    CD_CUDA(ctx, cudaMemset(h.d_gs_count, 0, sizeof(unsigned)));
   }
   return CDGPU_OK;
 }
@@ -1378,19 +1265,14 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
       if ((rc2 = spmv64(ctx, s, Z(i), h.d_w))) return rc2;
       int k = i + 1, pb = h.partial_blocks;
       // pass 1: h1 = V^T w
-      launch_gs<GS_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, nullptr, h.d_partial);
-      CD_LAUNCHED(ctx);
-      (void)cd_launch(reduce_partials_kernel, k, 256, 0, ctx->stream, pb, k, h.d_partial, h.d_ctl);
+      launch_gs<GS_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, nullptr, h.d_partial, h.d_ctl, h.d_gs_count);
       CD_LAUNCHED(ctx);
       // pass 2: w -= V h1, h2 = V^T w
-      launch_gs<GS_AXPY_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, h.d_ctl, h.d_partial);
-      CD_LAUNCHED(ctx);
-      (void)cd_launch(reduce_partials_kernel, k, 256, 0, ctx->stream, pb, k, h.d_partial, h.d_ctl + 33);
+      launch_gs<GS_AXPY_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, h.d_ctl, h.d_partial, h.d_ctl + 33, h.d_gs_count);
       CD_LAUNCHED(ctx);
       // w -= V h2, ||w||^2
-      launch_gs<GS_AXPY_NORM>(k, pb, ctx->stream, n, h.d_V, h.d_w, h.d_ctl + 33, h.d_partial);
-      CD_LAUNCHED(ctx);
-      (void)cd_launch(reduce_partials_kernel, 1, 256, 0, ctx->stream, pb, 1, h.d_partial, h.d_ctl + 66);
+      launch_gs<GS_AXPY_NORM>(k, pb, ctx->stream, n, h.d_V, h.d_w, h.d_ctl + 33, h.d_partial, h.d_ctl + 66,
+                              h.d_gs_count);
       CD_LAUNCHED(ctx);
       CD_CUDA(ctx, cudaMemcpyAsync(h.h_slot + (i & 1) * 80, h.d_ctl, sizeof(double) * 67, cudaMemcpyDeviceToHost,
                                    ctx->stream));

@@ -16,7 +16,9 @@
 //   Assemble     per level: Dirichlet values by the reference's nodal functionals on every
 //                Dirichlet face (the loop of TAssembleMat3D::Assemble3D,
 //                src/System/AssembleMat3D.C:969-1066), cdgpu_assemble into RhsArray[i]
-//                (entries stay on the device), Dirichlet part of rhs copied into SolArray[i]
+//                (entries stay on the device), the Neumann / Robin faces' boundary integral
+//                of the example's BoundValue (AssembleMat3D.C:1068-1170) by
+//                cdgpu_add_neumann, Dirichlet part of rhs copied into SolArray[i]
 //                (src/System/SystemCD3D.C:314-339)
 //   Solve        cdgpu_solve with the ParamDB keys of TSystemCD3D::Solve's GMG branch
 //                (FGMRES 16 / fixed point 11, multigrid preconditioner 5)
@@ -126,6 +128,44 @@ void dirichlet_values(TFESpace3D *space, BoundCondFunct3D *bc, BoundValueFunct3D
       const int *jd = desc->GetJointDOF(m);
       for (int l = 0; l < desc->GetN_JointDOF(); l++)
         if (dof[jd[l]] >= na) dir[dof[jd[l]] - na] = fv[l];
+    }
+  }
+}
+// boundary faces whose centre has a NEUMANN or ROBIN condition (their rhs part, as
+// TAssembleMat3D::Assemble3D adds it; the Robin matrix part belongs to the main program)
+void neumann_faces(TFESpace3D *space, BoundCondFunct3D *bc, std::vector<int> &cells, std::vector<int> &faces,
+                   std::vector<int> &ids)
+{
+  TCollection *coll = space->GetCollection();
+  cells.clear();
+  faces.clear();
+  ids.clear();
+  for (int c = 0; c < coll->GetN_Cells(); c++)
+  {
+    TBaseCell *cell = coll->GetCell(c);
+    const int *fv_idx, *flen;
+    int maxlen;
+    cell->GetShapeDesc()->GetFaceVertex(fv_idx, flen, maxlen);
+    for (int m = 0; m < cell->GetN_Faces(); m++)
+    {
+      TJoint *joint = cell->GetJoint(m);
+      if (joint->GetType() != BoundaryFace && joint->GetType() != IsoBoundFace) continue;
+      double xf = 0, yf = 0, zf = 0;
+      for (int l = 0; l < flen[m]; l++)
+      {
+        double x, y, z;
+        cell->GetVertex(fv_idx[m * maxlen + l])->GetCoords(x, y, z);
+        xf += x / flen[m];
+        yf += y / flen[m];
+        zf += z / flen[m];
+      }
+      const int id = ((TBoundFace *)joint)->GetBoundComp()->GetID();
+      BoundCond cond;
+      bc(id, xf, yf, zf, cond);
+      if (cond != NEUMANN && cond != ROBIN) continue;
+      cells.push_back(c);
+      faces.push_back(m);
+      ids.push_back(id);
     }
   }
 }
@@ -280,6 +320,25 @@ void TSystemCD3D::Assemble()
     dirichlet_values(sp, BoundaryConditions[0], BoundaryValues[0], dir);
     check(st.ctx, cdgpu_assemble(st.ctx, st.sids[i], Disctype, dir.empty() ? nullptr : dir.data(), nullptr, RhsArray[i]),
           "assemble");
+    // Neumann data: the example's BoundValue at the library's Gauss points of every such face
+    std::vector<int> cells, faces, ids;
+    neumann_faces(sp, BoundaryConditions[0], cells, faces, ids);
+    if (!cells.empty())
+    {
+      const int order = sp->GetBeginIndex()[1] - sp->GetBeginIndex()[0] == 27 ? 2 : 1, nq = (order + 1) * (order + 1);
+      std::vector<double> xyz(cells.size() * nq * 3), g(cells.size() * nq);
+      check(st.ctx, cdgpu_boundary_points(st.ctx, st.sids[i], (int)cells.size(), cells.data(), faces.data(), xyz.data()),
+            "boundary_points");
+      for (size_t e = 0; e < cells.size(); e++)
+        for (int q = 0; q < nq; q++)
+        {
+          const double *x = &xyz[(e * nq + q) * 3];
+          BoundaryValues[0](ids[e], x[0], x[1], x[2], g[e * nq + q]);
+        }
+      check(st.ctx, cdgpu_add_neumann(st.ctx, st.sids[i], (int)cells.size(), cells.data(), faces.data(), g.data(),
+                                      RhsArray[i]),
+            "add_neumann");
+    }
     std::memcpy(SolArray[i] + na, RhsArray[i] + na, (size_t)(n - na) * sizeof(double));
   }
 }

@@ -4,12 +4,17 @@ oracle/build_ref.py links the reference's main program twice from its unchanged 
   cd3d_main      with the reference's own TSystemCD3D (src/System/SystemCD3D.C, CPU),
   cd3d_main_gpu  with parmoon_cmg_b200/shim/SystemCD3D_cdgpu.C, the TSystemCD3D that runs
                  assembly and the multigrid FGMRES solve in libcdgpu on the GPU.
-Both read the same .dat (unit cube, Q2, 3 multigrid levels 2^3..8^3, Examples/CD_3D/Laplace.h:
--Laplace u = 3 pi^2 sin(pi x) sin(pi y) sin(pi z), its exact solution as Dirichlet data,
-MEASURE_ERRORS on).  The GPU program must print the CPU program's L2 and H1-semi errors digit
-for digit, in the FP64 and in the mixed form, and its solution must match the oracle's tight
-FP64 solution of the same discrete problem (the reference's own mesh, dumped by
-oracle/_ref/cd3d_dump, matched by DOF position) within 1e-10 (FP64) and 1e-8 (mixed).
+Both read the same .dat: unit cube, Q2, 3 multigrid levels 2^3..8^3, the main's own example
+Examples/CD_3D/Laplace.h (eps = 1/RE_NR, no source term, Dirichlet data BoundValue on the
+faces whose boundary component is not 0 and Neumann data 1 on component 0), VTK output and
+MEASURE_ERRORS on.  The main writes the solution to VTK (TOutput3D::WriteVtk), then replaces
+it by the interpolant of Exact() and prints that interpolant's L2 / H1-semi errors.
+
+Checked: the GPU program's VTK has the CPU program's points, cells and values (6 printed
+digits), in the FP64 and in the mixed form (the two forms' solutions within 1e-8 of each
+other); the printed errors match digit for digit; cdgpu_errors_table gives those printed
+errors for the same interpolant; cdgpu_write_vtk from a device buffer writes the CPU
+program's VTK content.
 """
 import os
 import re
@@ -53,7 +58,8 @@ SC_LIN_RES_NORM_MIN_SCALAR: 0
 SC_LIN_MAXIT_SCALAR: 30
 SC_VERBOSE: 0
 MEASURE_ERRORS: 1
-WRITE_VTK: 0
+WRITE_VTK: 1
+VTKBASENAME: cd3d
 """
 
 
@@ -69,143 +75,6 @@ def run_main(exe, tmp, env_extra=None):
     h1 = re.findall(r"^H1-semi: (\S+)", p.stdout, re.M)
     assert l2 and h1, p.stdout[-2000:]
     return l2[-1], h1[-1], p.stdout
-
-
-@pytest.fixture(scope="module")
-def cpu_errors():
-    exe = os.path.join(REF, "cd3d_main")
-    assert os.path.exists(exe), "oracle/_ref/cd3d_main is missing (oracle/build_ref.py)"
-    with tempfile.TemporaryDirectory() as tmp:
-        l2, h1, _ = run_main(exe, tmp)
-    return l2, h1
-
-
-@pytest.mark.parametrize("precision", [0, 1])
-def test_unchanged_cd3d_main_on_gpu(cpu_errors, oracle_lib, precision):
-    from parmoon_cmg_b200 import _build
-    _build.build()
-    exe = os.path.join(REF, "cd3d_main_gpu")
-    assert os.path.exists(exe), "oracle/_ref/cd3d_main_gpu is missing (oracle/build_ref.py)"
-    with tempfile.TemporaryDirectory() as tmp:
-        sol_path = os.path.join(tmp, "sol.f64")
-        l2, h1, out = run_main(exe, tmp, {"CDGPU_PRECISION": str(precision), "CDGPU_DUMP_SOLUTION": sol_path})
-        assert "libcdgpu FGMRES ITE:" in out
-        sol = np.fromfile(sol_path, dtype=np.float64)
-        xyz = np.fromfile(sol_path + ".xyz", dtype=np.float64).reshape(-1, 3)
-    # the reference's own output, digit for digit
-    assert (l2, h1) == cpu_errors, ((l2, h1), cpu_errors)
-    # the oracle's solution on cd3d_dump's numbering, matched to the main's DOFs by position
-    x_o, xyz_o = laplace_oracle_solution(oracle_lib)
-    key = lambda X: np.rint(X * 16).astype(np.int64) @ np.array([1, 17, 289])
-    order_o = np.argsort(key(xyz_o))
-    order_m = np.argsort(key(xyz))
-    assert np.array_equal(key(xyz_o)[order_o], key(xyz)[order_m])
-    x_m = np.empty_like(sol)
-    x_m[order_m] = x_o[order_o]
-    err = np.abs(sol - x_m).max() / np.abs(x_m).max()
-    assert err <= (1e-10 if precision == 0 else 1e-8), err
-
-
-def laplace_oracle_solution(oracle):
-    """The oracle's FP64 solution of the same discrete problem on the reference's own mesh and
-    DOF numbering (cd3d_dump with the same .dat): coefficients of Laplace.h at the oracle's
-    quadrature points, its exact solution at the Dirichlet nodes, solved to 1e-14."""
-    import refdump
-    with tempfile.TemporaryDirectory() as tmp:
-        dat = os.path.join(tmp, "d.dat")
-        with open(dat, "w") as f:
-            f.write(DAT.format(out=os.path.join(tmp, "d.out"), mesh=os.path.join(ROOT, "oracle", "meshes")))
-        out = os.path.join(tmp, "dump")
-        os.makedirs(out)
-        subprocess.run([os.path.join(REF, "cd3d_dump"), dat, out, "1", "0", "0", "0", "0", "0", "0"], cwd=tmp,
-                       check=True, capture_output=True)
-        d = refdump.load_dir(out)
-    L = int(d["levels"])
-    lv = [refdump.level(d, l) for l in range(L)]
-    levels, rhs = [], None
-    for l, S in enumerate(lv):
-        nc = len(S["begin_index"]) - 1
-        q = oracle.quad_points(3, 2, S["coords"], nc)
-        tab = np.zeros(q.shape[:2] + (6,))
-        tab[..., 0] = 1.0
-        tab[..., 5] = 3 * np.pi ** 2 * np.sin(np.pi * q[..., 0]) * np.sin(np.pi * q[..., 1]) * np.sin(np.pi * q[..., 2])
-        xyz = oracle.dof_coords(3, 2, S["coords"], S["global_numbers"], S["begin_index"], S["n_dof"])
-        na = S["n_active"]
-        g = np.sin(np.pi * xyz[na:, 0]) * np.sin(np.pi * xyz[na:, 1]) * np.sin(np.pi * xyz[na:, 2])
-        rp, kc = oracle.pattern(S["global_numbers"], S["begin_index"], S["n_dof"], na)
-        ent, rhs = oracle.assemble(3, 2, 1, S["coords"], S["global_numbers"], S["begin_index"], S["n_dof"], na,
-                                   rp, kc, oracle.coeffs(3), coeff_tab=tab, dir_vals=g)
-        e = dict(n_dof=S["n_dof"], n_active=na, row_ptr=rp, kcol=kc, entries=ent)
-        if l > 0:
-            e["p_row"], e["p_col"], e["p_val"] = oracle.prolongation(3, 2, lv[l - 1], S, S["parent"])
-        levels.append(e)
-    fin = lv[-1]
-    sol0 = np.zeros(fin["n_dof"])
-    sol0[fin["n_active"]:] = rhs[fin["n_active"]:]
-    prm = oracle.solver_params(red_factor=0.0, res_norm_min=1e-14 * np.linalg.norm(rhs), maxit=300)
-    x, _, _, _ = oracle.solve(levels, prm, rhs, sol0)
-    return x, oracle.dof_coords(3, 2, fin["coords"], fin["global_numbers"], fin["begin_index"], fin["n_dof"])
-
-
-@pytest.fixture(scope="module")
-def laplace_gpu():
-    """The Laplace example solved through the C ABI on the reference's own mesh and DOF
-    numbering (cd3d_dump with the same .dat), coefficients tabulated at the library's
-    quadrature points, the exact solution as Dirichlet data."""
-    import oracle
-    import refdump
-    from parmoon_cmg_b200 import _build, _lib
-    from parmoon_cmg_b200.system import Context, coeffs, solver_params
-    _build.build()
-    with tempfile.TemporaryDirectory() as tmp:
-        dat = os.path.join(tmp, "d.dat")
-        with open(dat, "w") as f:
-            f.write(DAT.format(out=os.path.join(tmp, "d.out"), mesh=os.path.join(ROOT, "oracle", "meshes")))
-        out = os.path.join(tmp, "dump")
-        os.makedirs(out)
-        subprocess.run([os.path.join(REF, "cd3d_dump"), dat, out, "1", "0", "0", "0", "0", "0", "0"], cwd=tmp,
-                       check=True, capture_output=True)
-        d = refdump.load_dir(out)
-    lv = [refdump.level(d, l) for l in range(int(d["levels"]))]
-    ctx = Context(0)
-    sids = []
-    for S in lv:
-        sid = ctx.upload_space(dict(dim=3, order=2, coords=S["coords"], global_numbers=S["global_numbers"],
-                                    begin_index=S["begin_index"], n_dof=S["n_dof"], n_active=S["n_active"]))
-        ctx.build_pattern(sid)
-        nc = len(S["begin_index"]) - 1
-        q = ctx.quadrature_points(sid, nc, 3)
-        tab = np.zeros(q.shape[:2] + (6,))
-        tab[..., 0] = 1.0
-        tab[..., 5] = 3 * np.pi ** 2 * np.prod(np.sin(np.pi * q), axis=-1)
-        ctx.set_coeffs(sid, coeffs(_lib.COEFF_TABLE), tab)
-        sids.append(sid)
-    mg = ctx.hierarchy(sids, [None] + [S["parent"] for S in lv[1:]])
-    rhs = None
-    for S, sid in zip(lv, sids):
-        xyz = oracle.dof_coords(3, 2, S["coords"], S["global_numbers"], S["begin_index"], S["n_dof"])
-        g = np.prod(np.sin(np.pi * xyz[S["n_active"]:]), axis=-1)
-        _, rhs = ctx.assemble(sid, 1, S["n_dof"], 1, dirichlet=g, want_entries=False)
-    fin = lv[-1]
-    sol0 = np.zeros(fin["n_dof"])
-    sol0[fin["n_active"]:] = rhs[fin["n_active"]:]
-    x, info = ctx.solve(mg, solver_params(coarse_smoother=3, red_factor=1e-13, maxit=30), rhs, sol0)
-    assert info.status == 0
-    yield dict(ctx=ctx, sids=sids, lv=lv, x=x)
-    ctx.close()
-
-
-def test_errors_table_reproduces_reference_output(cpu_errors, laplace_gpu):
-    """GetErrors on the device for any exact solution (cdgpu_errors_table): the L2 and H1-semi
-    errors that the reference's CD3D main prints, digit for digit."""
-    ctx, sids, fin, x = laplace_gpu["ctx"], laplace_gpu["sids"], laplace_gpu["lv"][-1], laplace_gpu["x"]
-    nc = len(fin["begin_index"]) - 1
-    q = ctx.quadrature_points(sids[-1], nc, 3)
-    s, c = np.sin(np.pi * q), np.cos(np.pi * q)
-    ex = np.stack([s[..., 0] * s[..., 1] * s[..., 2], np.pi * c[..., 0] * s[..., 1] * s[..., 2],
-                   np.pi * s[..., 0] * c[..., 1] * s[..., 2], np.pi * s[..., 0] * s[..., 1] * c[..., 2]], -1)
-    l2, h1 = ctx.errors_table(sids[-1], x, ex)
-    assert (f"{l2:g}", f"{h1:g}") == cpu_errors, ((l2, h1), cpu_errors)
 
 
 def read_vtk(path):
@@ -227,31 +96,141 @@ def read_vtk(path):
     return pts, cells, vals
 
 
-def test_vtk_from_device_buffer_matches_reference_output(laplace_gpu):
-    """cdgpu_write_vtk from a solution held on the device writes the points, hexahedra and
-    vertex values that the reference's own TOutput3D::WriteVtk writes for the same problem
-    (its CD3D main with WRITE_VTK), up to the order of the points and the printed digits."""
-    import torch
-    ctx, sid, x = laplace_gpu["ctx"], laplace_gpu["sids"][-1], laplace_gpu["x"]
+def last_vtk(tmp):
+    vtks = sorted(f for f in os.listdir(os.path.join(tmp, "VTK")) if f.endswith(".vtk"))
+    assert vtks, "no VTK file written"
+    return read_vtk(os.path.join(tmp, "VTK", vtks[-1]))
+
+
+def pkey(P):
+    return np.rint(P * 16).astype(np.int64) @ np.array([1, 17, 289])
+
+
+def run_main(exe, env_extra=None):
+    """Run a main program on the .dat; returns its printed L2 / H1-semi errors, its VTK output
+    and, for the GPU program, the solution it solved (with the DOF positions)."""
     with tempfile.TemporaryDirectory() as tmp:
-        dat = os.path.join(tmp, "v.dat")
+        dat = os.path.join(tmp, "cd3d.dat")
         with open(dat, "w") as f:
-            f.write(DAT.format(out=os.path.join(tmp, "v.out"), mesh=os.path.join(ROOT, "oracle", "meshes"))
-                    .replace("WRITE_VTK: 0", "WRITE_VTK: 1\nVTKBASENAME: ref"))
-        subprocess.run([os.path.join(REF, "cd3d_main"), dat], cwd=tmp, check=True, capture_output=True, timeout=600)
-        vtks = sorted(f for f in os.listdir(os.path.join(tmp, "VTK")) if f.endswith(".vtk"))
-        assert vtks, "the reference wrote no VTK file"
-        p_ref, c_ref, v_ref = read_vtk(os.path.join(tmp, "VTK", vtks[-1]))
+            f.write(DAT.format(out=os.path.join(tmp, "cd3d.out"), mesh=os.path.join(ROOT, "oracle", "meshes")))
+        env = dict(os.environ)
+        env.update(env_extra or {})
+        sol_path = os.path.join(tmp, "sol.f64")
+        env["CDGPU_DUMP_SOLUTION"] = sol_path
+        p = subprocess.run([exe, dat], cwd=tmp, capture_output=True, text=True, env=env, timeout=600)
+        assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
+        l2 = re.findall(r"^L2: (\S+)", p.stdout, re.M)
+        h1 = re.findall(r"^H1-semi: (\S+)", p.stdout, re.M)
+        assert l2 and h1, p.stdout[-2000:]
+        out = dict(errors=(l2[-1], h1[-1]), vtk=last_vtk(tmp), stdout=p.stdout)
+        if os.path.exists(sol_path):
+            out["sol"] = np.fromfile(sol_path, dtype=np.float64)
+            out["xyz"] = np.fromfile(sol_path + ".xyz", dtype=np.float64).reshape(-1, 3)
+    return out
+
+
+@pytest.fixture(scope="module")
+def cpu_run():
+    exe = os.path.join(REF, "cd3d_main")
+    assert os.path.exists(exe), "oracle/_ref/cd3d_main is missing (oracle/build_ref.py)"
+    return run_main(exe)
+
+
+@pytest.fixture(scope="module")
+def gpu_runs():
+    from parmoon_cmg_b200 import _build
+    _build.build()
+    exe = os.path.join(REF, "cd3d_main_gpu")
+    assert os.path.exists(exe), "oracle/_ref/cd3d_main_gpu is missing (oracle/build_ref.py)"
+    return {prec: run_main(exe, {"CDGPU_PRECISION": str(prec)}) for prec in (0, 1)}
+
+
+def same_vtk(a, b, tol):
+    """Same points (by position), same cells (as sets of positions), values within tol of the
+    largest value."""
+    (p, c, v), (p_r, c_r, v_r) = a, b
+    assert len(p) == len(p_r) and len(c) == len(c_r)
+    o, o_r = np.argsort(pkey(p)), np.argsort(pkey(p_r))
+    assert np.array_equal(pkey(p)[o], pkey(p_r)[o_r])
+    cell_key = lambda P, C: sorted(tuple(sorted(pkey(P[cc]).tolist())) for cc in C)
+    assert cell_key(p, c) == cell_key(p_r, c_r)
+    err = np.abs(v[o] - v_r[o_r]).max() / np.abs(v_r).max()
+    assert err <= tol, err
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_unchanged_cd3d_main_on_gpu(cpu_run, gpu_runs, precision):
+    g = gpu_runs[precision]
+    assert "libcdgpu FGMRES ITE:" in g["stdout"]
+    # the solution as the reference's own VTK writer prints it (6 significant digits)
+    same_vtk(g["vtk"], cpu_run["vtk"], 2e-6)
+    assert g["errors"] == cpu_run["errors"]
+    if precision == 1:
+        x64, xm = gpu_runs[0]["sol"], g["sol"]
+        assert np.abs(xm - x64).max() <= 1e-8 * np.abs(x64).max()
+
+
+@pytest.fixture(scope="module")
+def ref_mesh():
+    """The finest level of the same mesh as the reference builds it (cd3d_dump, same .dat)."""
+    import refdump
+    with tempfile.TemporaryDirectory() as tmp:
+        dat = os.path.join(tmp, "d.dat")
+        with open(dat, "w") as f:
+            f.write(DAT.format(out=os.path.join(tmp, "d.out"), mesh=os.path.join(ROOT, "oracle", "meshes")))
+        out = os.path.join(tmp, "dump")
+        os.makedirs(out)
+        subprocess.run([os.path.join(REF, "cd3d_dump"), dat, out, "1", "0", "0", "0", "0", "0", "0"], cwd=tmp,
+                       check=True, capture_output=True)
+        d = refdump.load_dir(out)
+    return refdump.level(d, int(d["levels"]) - 1)
+
+
+def test_errors_table_reproduces_reference_output(cpu_run, ref_mesh, oracle_lib):
+    """GetErrors on the device for any exact solution (cdgpu_errors_table): for the interpolant
+    of Laplace.h's Exact() the L2 and H1-semi errors that the reference's CD3D main prints for
+    the same interpolant, digit for digit."""
+    from parmoon_cmg_b200.system import Context
+    L = ref_mesh
+    ctx = Context(0)
+    try:
+        sid = ctx.upload_space(dict(dim=3, order=2, coords=L["coords"], global_numbers=L["global_numbers"],
+                                    begin_index=L["begin_index"], n_dof=L["n_dof"], n_active=L["n_active"]))
+        xyz = oracle_lib.dof_coords(3, 2, L["coords"], L["global_numbers"], L["begin_index"], L["n_dof"])
+        u_int = np.prod(np.sin(np.pi * xyz), axis=-1)
+        nc = len(L["begin_index"]) - 1
+        q = ctx.quadrature_points(sid, nc, 3)
+        s, c = np.sin(np.pi * q), np.cos(np.pi * q)
+        ex = np.stack([s[..., 0] * s[..., 1] * s[..., 2], np.pi * c[..., 0] * s[..., 1] * s[..., 2],
+                       np.pi * s[..., 0] * c[..., 1] * s[..., 2], np.pi * s[..., 0] * s[..., 1] * c[..., 2]], -1)
+        l2, h1 = ctx.errors_table(sid, u_int, ex)
+    finally:
+        ctx.close()
+    assert (f"{l2:g}", f"{h1:g}") == cpu_run["errors"], ((l2, h1), cpu_run["errors"])
+
+
+def test_vtk_from_device_buffer_matches_reference_output(cpu_run, gpu_runs, ref_mesh, oracle_lib):
+    """cdgpu_write_vtk, from the GPU program's solution held in device memory, writes the points,
+    hexahedra and vertex values that the reference's own TOutput3D::WriteVtk wrote."""
+    import torch
+    from parmoon_cmg_b200.system import Context
+    L, g = ref_mesh, gpu_runs[0]
+    xyz = oracle_lib.dof_coords(3, 2, L["coords"], L["global_numbers"], L["begin_index"], L["n_dof"])
+    # the GPU program's solution in cd3d_dump's numbering (matched by DOF position)
+    o, o_g = np.argsort(pkey(xyz)), np.argsort(pkey(g["xyz"]))
+    assert np.array_equal(pkey(xyz)[o], pkey(g["xyz"])[o_g])
+    x = np.empty(L["n_dof"])
+    x[o] = g["sol"][o_g]
+    ctx = Context(0)
+    try:
+        sid = ctx.upload_space(dict(dim=3, order=2, coords=L["coords"], global_numbers=L["global_numbers"],
+                                    begin_index=L["begin_index"], n_dof=L["n_dof"], n_active=L["n_active"]))
         d_x = torch.tensor(x, device="cuda:0")
         torch.cuda.synchronize()
-        ours = os.path.join(tmp, "ours.vtk")
-        ctx.write_vtk(sid, d_x.data_ptr(), ours, on_device=True)
-        p, cells, v = read_vtk(ours)
-    assert len(p) == len(p_ref) and len(cells) == len(c_ref)
-    key = lambda P: np.rint(P * 8).astype(np.int64) @ np.array([1, 9, 81])
-    o, o_ref = np.argsort(key(p)), np.argsort(key(p_ref))
-    assert np.array_equal(key(p)[o], key(p_ref)[o_ref])
-    assert np.abs(v[o] - v_ref[o_ref]).max() <= 1e-5 * np.abs(v_ref).max()
-    # the same cells, as sets of vertex positions
-    cell_key = lambda P, C: sorted(tuple(sorted(key(P[c]).tolist())) for c in C)
-    assert cell_key(p, cells) == cell_key(p_ref, c_ref)
+        with tempfile.TemporaryDirectory() as tmp:
+            path = os.path.join(tmp, "ours.vtk")
+            ctx.write_vtk(sid, d_x.data_ptr(), path, name="C", on_device=True)
+            ours = read_vtk(path)
+    finally:
+        ctx.close()
+    same_vtk(ours, cpu_run["vtk"], 2e-6)
