@@ -143,7 +143,7 @@ def link_driver(ref, geo, lib, name, main_src):
     print(f"linked {exe}")
 
 
-def link_main(ref, geo, lib, name, main_src, gpu):
+def link_main(ref, geo, lib, name, main_src, gpu, shim="SystemCD3D_cdgpu.C", extra=()):
     """Link the reference's own, unchanged main program (e.g. 3DPrograms/CD3D_ParMooN.C) against
     the compiled reference; with gpu, the TSystemCD3D of parmoon_cmg_b200/shim (the
     reference-side binding of libcdgpu) comes first on the link line, so the archive's
@@ -154,10 +154,10 @@ def link_main(ref, geo, lib, name, main_src, gpu):
     srcs = [os.path.join(ref, main_src)]
     libs = []
     if gpu:
-        srcs.append(os.path.join(root, "parmoon_cmg_b200", "shim", "SystemCD3D_cdgpu.C"))
+        srcs.append(os.path.join(root, "parmoon_cmg_b200", "shim", shim))
         libs = [f"-L{os.path.join(root, 'parmoon_cmg_b200')}", "-lcdgpu",
                 "-Wl,-rpath,$ORIGIN/../../parmoon_cmg_b200"]
-    cmd = ["g++", "-O2", "-std=c++11", "-fpermissive", "-w"] + defines(geo) + includes(ref) + \
+    cmd = ["g++", "-O2", "-std=c++11", "-fpermissive", "-w"] + defines(geo) + list(extra) + includes(ref) + \
           [f"-I{os.path.join(root, 'include')}"] + srcs + [os.path.join(drv, "stubs.C"),
                                                         "-Wl,--start-group", lib, "-Wl,--end-group"] + \
           libs + ["-lm", "-o", exe]
@@ -183,11 +183,18 @@ def main():
         if not a.link_only or not os.path.exists(lib):
             lib = build_geo(a.ref, geo, a.jobs)
         link_driver(a.ref, geo, lib, f"cd{geo.lower()}_dump", f"cd{geo.lower()}_dump.C")
+        have_gpu_lib = os.path.exists(os.path.join(os.path.dirname(HERE), "parmoon_cmg_b200", "libcdgpu.so"))
         if geo == "3D":
             # the reference's CD3D main unchanged: on its own TSystemCD3D (CPU) and on libcdgpu
             link_main(a.ref, geo, lib, "cd3d_main", "3DPrograms/CD3D_ParMooN.C", gpu=False)
-            if os.path.exists(os.path.join(os.path.dirname(HERE), "parmoon_cmg_b200", "libcdgpu.so")):
+            if have_gpu_lib:
                 link_main(a.ref, geo, lib, "cd3d_main_gpu", "3DPrograms/CD3D_ParMooN.C", gpu=True)
+        elif have_gpu_lib:
+            # the reference's CD2D main unchanged, built with its own test switch (_TEST: the
+            # SineLaplace example, CD2D_ParMooN.C:21-26), on the TSystemCD2D of libcdgpu (the
+            # reference's own TSystemCD2D solves with UMFPACK, which is not available here)
+            link_main(a.ref, geo, lib, "cd2d_main_gpu", "2DPrograms/CD2D_ParMooN.C", gpu=True,
+                      shim="SystemCD2D_cdgpu.C", extra=["-D_TEST"])
 
 
 if __name__ == "__main__":

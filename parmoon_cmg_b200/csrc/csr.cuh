@@ -431,22 +431,34 @@ __global__ void __launch_bounds__((kTmaWarps + 1) * 32) csr_tma_kernel(CsrArgs<d
       if (r < m.re)
       {
         const int jb = rs[r - m.rb0] - m.nb0, je = rs[r + 1 - m.rb0] - m.nb0;
-        for (int j0 = jb + l4; j0 < je; j0 += 32)
+        // 16 entries per thread at once: every gather of a row of up to 64 entries is in
+        // flight together (longer rows take a second round)
+        for (int j0 = jb + l4; j0 < je; j0 += 64)
         {
-          int c[8];
-          double v[8];
+          int c[16];
 #pragma unroll
-          for (int u = 0; u < 8; u++)
+          for (int u = 0; u < 16; u++)
           {
             const int j = j0 + 4 * u;
             c[u] = j < je ? co[j] : -1;
-            v[u] = j < je ? va[j] : 0.0;
           }
-          double xv[8];
+          // the 16 gathers are issued in order before the first product (positions beyond
+          // the row read x[0] and are multiplied by nothing)
+          double xv[16];
 #pragma unroll
-          for (int u = 0; u < 8; u++) xv[u] = c[u] >= 0 ? __ldg(p.x + c[u]) : 0.0;
+          for (int u = 0; u < 16; u++)
+            asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(xv[u]) : "l"(p.x + (c[u] >= 0 ? c[u] : 0)));
+          // all 16 values pass through this point before any product uses one, so the compiler
+          // cannot put a product (and its wait) between two gathers
+          asm volatile("" : "+d"(xv[0]), "+d"(xv[1]), "+d"(xv[2]), "+d"(xv[3]), "+d"(xv[4]), "+d"(xv[5]),
+                       "+d"(xv[6]), "+d"(xv[7]), "+d"(xv[8]), "+d"(xv[9]), "+d"(xv[10]), "+d"(xv[11]), "+d"(xv[12]),
+                       "+d"(xv[13]), "+d"(xv[14]), "+d"(xv[15]));
 #pragma unroll
-          for (int u = 0; u < 8; u++) sum += v[u] * xv[u];
+          for (int u = 0; u < 16; u++)
+          {
+            const int j = j0 + 4 * u;
+            if (j < je) sum += va[j] * xv[u];
+          }
         }
       }
       sum = csr_group_sum<4>(sum);

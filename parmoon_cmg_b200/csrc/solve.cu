@@ -480,7 +480,7 @@ struct TmaVariant
 {
   int cap, stages;
 };
-static const TmaVariant kTmaVariants[] = {{2048, 4}, {2048, 2}, {3072, 3}, {3072, 2}, {4096, 2}};
+static const TmaVariant kTmaVariants[] = {{2048, 4}, {2048, 2}, {3072, 3}, {3072, 2}, {4096, 2}, {2048, 3}, {1536, 2}};
 constexpr int kNumTmaVariants = sizeof(kTmaVariants) / sizeof(kTmaVariants[0]);
 
 template <int MODE> static void (*tma_kernel(int v))(CsrArgs<double>, const int2 *, int, int *)
@@ -491,6 +491,8 @@ template <int MODE> static void (*tma_kernel(int v))(CsrArgs<double>, const int2
     case 2: return csr_tma_kernel<MODE, 3072, 3>;
     case 3: return csr_tma_kernel<MODE, 3072, 2>;
     case 4: return csr_tma_kernel<MODE, 4096, 2>;
+    case 5: return csr_tma_kernel<MODE, 2048, 3>;
+    case 6: return csr_tma_kernel<MODE, 1536, 2>;
     default: return csr_tma_kernel<MODE, 2048, 4>;
   }
 }
