@@ -31,6 +31,7 @@ time is the maximum over ranks.
 """
 import argparse
 import json
+import math
 import os
 import shutil
 import subprocess
@@ -44,7 +45,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 EPS = 1e-2
-B = (1 / np.sqrt(3),) * 3
+B = (1 / math.sqrt(3),) * 3
+
+
+def num(x):
+    """A number as the reference drivers read it from argv (atof of a plain decimal)."""
+    return repr(float(x))
 METRIC = "CD solves/s and p50/p99 latency at 1e-8 rel. err vs FP64; assembly Mcells/s"
 UNIT = "solves/s"
 
@@ -148,7 +154,7 @@ def reference_run(n, levels, tmp, tag="0"):
     with open(dat, "w") as f:
         f.write(DAT.format(out=os.path.join(tmp, f"w{tag}.out"), mesh=os.path.join(ROOT, "oracle", "meshes"),
                            steps=steps, levels=levels))
-    p = subprocess.run([exe, dat, "-", repr(EPS), *map(repr, B), "0", "1", "0", "1e-10"], cwd=tmp,
+    p = subprocess.run([exe, dat, "-", num(EPS), *map(num, B), "0", "1", "0", "1e-10"], cwd=tmp,
                        capture_output=True, text=True, check=True)
     line = [l for l in p.stdout.splitlines() if l.startswith("{")][-1]
     return json.loads(line)
@@ -189,7 +195,7 @@ def run_reference_arm(args, rank, world):
                     f.write(DAT.format(out=os.path.join(tmp, f"w{k}.out"),
                                        mesh=os.path.join(ROOT, "oracle", "meshes"), steps=steps_,
                                        levels=REF_LEVELS))
-                ps.append(subprocess.Popen([exe, dat, "-", repr(EPS), *map(repr, B), "0", "1", "0", "1e-10"],
+                ps.append(subprocess.Popen([exe, dat, "-", num(EPS), *map(num, B), "0", "1", "0", "1e-10"],
                                            cwd=tmp, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
                                            text=True))
             outs = [json.loads([l for l in p.communicate()[0].splitlines() if l.startswith("{")][-1]) for p in ps]
@@ -475,7 +481,7 @@ def reference_accuracy(n, sols, tmp):
                            steps=steps, levels=REF_LEVELS))
     out = os.path.join(tmp, "acc")
     os.makedirs(out, exist_ok=True)
-    subprocess.run([exe, dat, out, repr(EPS), *map(repr, B), "0", "1", "0", "1e-12"], cwd=tmp,
+    subprocess.run([exe, dat, out, num(EPS), *map(num, B), "0", "1", "0", "1e-12"], cwd=tmp,
                    capture_output=True, text=True, check=True)
     d = refdump.load_dir(out)
     L = refdump.level(d, int(d["levels"]) - 1)
@@ -655,7 +661,7 @@ def batched_cpu_baseline(work, sample_size=16):
             with open(dat, "w") as f:
                 f.write(BATCH_DAT.format(out=os.path.join(tmp, f"b{k}.out"), mesh=os.path.join(ROOT, "oracle", "meshes"),
                                          steps=int(round(np.log2(w["n0"]))), levels=w["levels"], order=w["order"]))
-            cmds.append([exe, dat, "-", "0", repr(w["eps"]), repr(w["b"][0]), repr(w["b"][1]), "0", "1"])
+            cmds.append([exe, dat, "-", "0", num(w["eps"]), num(w["b"][0]), num(w["b"][1]), "0", "1"])
         t0 = time.perf_counter()
         running, outs = [], []
         pending = list(cmds)

@@ -324,10 +324,23 @@ __global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, const double *__
   __syncthreads();
   if (!last) return;
   __threadfence();
+  // the other blocks' partials are read from L2 (ld.global.cg), eight at a time in flight, and
+  // added in block order
   for (int j = warp; j < NS; j += kBlock / 32)
   {
     double t = 0;
-    for (int b = lane; b < (int)gridDim.x; b += 32) t += *(volatile double *)(partial + (size_t)b * 33 + j);
+    for (int b0 = lane; b0 < (int)gridDim.x; b0 += 32 * 8)
+    {
+      double v[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++)
+      {
+        const int b = b0 + 32 * u;
+        v[u] = b < (int)gridDim.x ? __ldcg(partial + (size_t)b * 33 + j) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) t += v[u];
+    }
     t = group_sum<32>(t);
     if (lane == 0) out[j] = t;
   }
