@@ -290,6 +290,12 @@ int cdgpu_tcd_step_device(cdgpu_ctx *ctx, int tcd_id, const cdgpu_solver_params 
                           double theta1, double theta2, double theta3, double theta4, double *d_sol,
                           cdgpu_solve_info *info);
 int cdgpu_tcd_rhs(cdgpu_ctx *ctx, int tcd_id, double *h_rhs);
+/* Dirichlet values (n_dof - n_active values of the finest level, BoundValue at the DOFs at
+ * the current time) that the following cdgpu_tcd_assemble_mass / _stiffness calls put into
+ * the right-hand side, as the reference's assembly evaluates BoundValue at CURRENTTIME
+ * (src/System/SystemTCD3D.C:176-226 through Assemble3D); NULL = zero values (the default).
+ * The values are copied. */
+int cdgpu_tcd_set_dirichlet(cdgpu_ctx *ctx, int tcd_id, const double *h_dirichlet);
 /* copies (nnz values of level `level`, 0 = coarsest; each pointer nullable) of the mass matrix
  * M as updated in place by the steps, the stiffness matrix A, and the system matrix the last
  * step solved with: the sqmatrixM / sqmatrixA members of TSystemTCD2D / TSystemTCD3D

@@ -168,9 +168,14 @@ def link_main(ref, geo, lib, name, main_src, gpu, shim="SystemCD3D_cdgpu.C", ext
     print(f"linked {exe}")
 
 
+def default_tree():
+    """The reference tree this recipe compiles: $CDGPU_REFERENCE, else the container's copy."""
+    return os.environ.get("CDGPU_REFERENCE", "/root/reference")
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("CDGPU_REFERENCE", "/root/reference"))
+    ap.add_argument("--ref", default=default_tree())
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--geo", nargs="*", default=["2D", "3D"])
     ap.add_argument("--link-only", action="store_true")

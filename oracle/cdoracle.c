@@ -704,6 +704,52 @@ void cdo_errors_sinsin(int order, int n_cells, const double *coords, const int *
   err2[1] = sqrt(e1);
 }
 
+/* L2 and H1-semi errors against an exact solution tabulated at the quadrature points of
+ * cdo_quad_points: exact[(c * nq + q) * (1 + dim) + k] = u, du/dx, du/dy[, du/dz].  Any space
+ * of the path: TFEFunction2D::GetErrors (src/FE/FEFunction2D.C:73) and
+ * TFEFunction3D::GetErrors (src/FE/FEFunction3D.C:57) with L2H1Errors
+ * (src/General/MainUtilities.C:606), on the assembly's Gauss rule (degree 3p). */
+void cdo_errors_table(int dim, int order, int n_cells, const double *coords, const int *gn, const int *bi,
+                      const double *u, const double *exact, double *err2)
+{
+  int nbf = cdo_nbf(dim, order), nv = nverts(dim);
+  double qx[3 * MAXQ], qw[MAXQ];
+  int nq = cdo_quadrature(dim, cdo_gauss_points(order), qx, qw);
+  double e0 = 0, e1 = 0;
+  for (int c = 0; c < n_cells; c++)
+  {
+    const double *V = coords + (size_t)c * nv * dim;
+    int affine = cell_is_affine(dim, V);
+    const int *dof = gn + bi[c];
+    for (int q = 0; q < nq; q++)
+    {
+      double x[3], J[9], Ji[9], val[MAXBF], gr[MAXBF * 3];
+      ref_map(dim, affine, V, qx + dim * q, x, J);
+      double det = inv(dim, J, Ji);
+      cdo_basis(dim, order, qx + dim * q, val, gr, NULL);
+      double uh = 0, g[3] = {0, 0, 0};
+      for (int b = 0; b < nbf; b++)
+      {
+        uh += u[dof[b]] * val[b];
+        for (int a = 0; a < dim; a++)
+        {
+          double t = 0;
+          for (int k = 0; k < dim; k++) t += Ji[k * dim + a] * gr[dim * b + k];
+          g[a] += u[dof[b]] * t;
+        }
+      }
+      const double *ex = exact + ((size_t)c * nq + q) * (1 + dim);
+      double w = qw[q] * fabs(det);
+      e0 += w * (uh - ex[0]) * (uh - ex[0]);
+      double s1 = 0;
+      for (int a = 0; a < dim; a++) s1 += (g[a] - ex[1 + a]) * (g[a] - ex[1 + a]);
+      e1 += w * s1;
+    }
+  }
+  err2[0] = sqrt(e0);
+  err2[1] = sqrt(e1);
+}
+
 /* physical quadrature points of every cell (n_cells x n_quad x dim), in the order the
  * assembly reads a CDGPU_COEFF_TABLE (kind 3) */
 void cdo_quad_points(int dim, int order, int n_cells, const double *coords, double *xyz)

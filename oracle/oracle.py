@@ -88,6 +88,7 @@ def _declare(L):
     L.cdo_neumann_sine.argtypes = [C.c_int, C.c_int, _P, _P, _P, C.c_int, C.c_double, _P]
     L.cdo_errors_sine.argtypes = [C.c_int, C.c_int, _P, _P, _P, _P, _P]
     L.cdo_errors_sinsin.argtypes = [C.c_int, C.c_int, _P, _P, _P, _P, C.c_double, C.c_double, _P]
+    L.cdo_errors_table.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P]
     L.cdo_quad_points.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P]
     L.cdo_dof_coords.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P, _P, C.c_int, _P]
     L.cdo_prolongation.restype = C.c_long
@@ -154,6 +155,15 @@ def errors_sinsin(order, coords, gn, bi, u, k, amp):
     coords, gn, bi, u = _f64(coords), _i32(gn), _i32(bi), _f64(u)
     out = np.zeros(2)
     lib().cdo_errors_sinsin(order, len(bi) - 1, _p(coords), _p(gn), _p(bi), _p(u), k, amp, _p(out))
+    return out
+
+
+def errors_table(dim, order, coords, gn, bi, u, exact):
+    """L2 and H1-semi errors against an exact solution tabulated at the quadrature points
+    (n_cells x n_quad x (1 + dim): value, gradient), TFEFunction3D::GetErrors."""
+    coords, gn, bi, u, exact = _f64(coords), _i32(gn), _i32(bi), _f64(u), _f64(exact)
+    out = np.zeros(2)
+    lib().cdo_errors_table(dim, order, len(bi) - 1, _p(coords), _p(gn), _p(bi), _p(u), _p(exact), _p(out))
     return out
 
 

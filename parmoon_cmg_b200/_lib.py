@@ -87,6 +87,7 @@ SIGNATURES = {
     "cdgpu_tcd_step_device": (_I, [_P, _I, C.POINTER(SolverParams), C.c_double, C.c_double,
                                    C.c_double, C.c_double, C.c_double, _P, C.POINTER(SolveInfo)]),
     "cdgpu_tcd_rhs": (_I, [_P, _I, _P]),
+    "cdgpu_tcd_set_dirichlet": (_I, [_P, _I, _P]),
     "cdgpu_tcd_matrices": (_I, [_P, _I, _I, _P, _P, _P]),
     "cdgpu_batch_create": (_I, [_P, C.POINTER(SolverParams), C.POINTER(_I)]),
     "cdgpu_batch_submit": (_I, [_P, _I, _I, C.POINTER(Coeffs), _I, _I, C.POINTER(_I)]),

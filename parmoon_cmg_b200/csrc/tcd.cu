@@ -21,6 +21,8 @@ struct Tcd
   std::vector<double *> M, A; // per level, same CSR pattern as the level's space
   double *d_f_old = nullptr, *d_f = nullptr, *d_B = nullptr, *d_x = nullptr;
   bool have_mass = false, have_stiff = false;
+  // BoundValue at the finest level's Dirichlet DOFs for the next assemblies (empty = 0)
+  std::vector<double> h_dir;
 };
 
 static std::vector<Tcd *> &tcds(cdgpu_ctx *ctx) { return ctx->tcds; }
@@ -112,7 +114,9 @@ static int assemble_into(cdgpu_ctx *ctx, Tcd &t, int disctype, std::vector<doubl
   for (size_t l = 0; l < t.h->lev.size(); l++)
   {
     Space &s = *t.h->lev[l].sp;
-    int rc = assemble_space(ctx, s, disctype, nullptr, false);
+    const bool fine = l + 1 == t.h->lev.size();
+    const double *dir = fine && !t.h_dir.empty() ? t.h_dir.data() : nullptr;
+    int rc = assemble_space(ctx, s, disctype, dir, false);
     if (rc) return rc;
     CD_CUDA(ctx, cudaMemcpyAsync(dst[l], s.d_a, sizeof(double) * s.nnz, cudaMemcpyDeviceToDevice, ctx->stream));
     if (l + 1 == t.h->lev.size() && rhs_dst)
@@ -148,6 +152,21 @@ int cdgpu_tcd_create(cdgpu_ctx *ctx, int mg_id, int disctype, int *tcd_id)
     return rc;
   tcds(ctx).push_back(t);
   *tcd_id = (int)tcds(ctx).size() - 1;
+  return CDGPU_OK;
+}
+
+// the boundary values that the reference's assembly takes from BoundValue at the current
+// time (Assemble3D / Assemble2D set the Dirichlet entries of rhs), for the finest level's
+// Dirichlet DOFs [n_active, n_dof); NULL returns to zero values
+int cdgpu_tcd_set_dirichlet(cdgpu_ctx *ctx, int tcd_id, const double *h_dirichlet)
+{
+  Tcd *t = get_tcd(ctx, tcd_id);
+  if (!t) return fail(ctx, CDGPU_ERR_INVALID, "tcd_set_dirichlet: bad id");
+  const Space &f = *t->h->lev.back().sp;
+  if (!h_dirichlet)
+    t->h_dir.clear();
+  else
+    t->h_dir.assign(h_dirichlet, h_dirichlet + (f.n_dof - f.n_active));
   return CDGPU_OK;
 }
 

@@ -346,6 +346,16 @@ class TSystemTCD2D:
         self.ctx.check(self.ctx.lib.cdgpu_tcd_matrices(self.ctx.h, self.tcd, level, *[_p(a) for a in out]))
         return tuple(out)
 
+    def SetDirichlet(self, values=None):
+        """BoundValue at the finest level's Dirichlet DOFs (N_DOF - N_Active values) for the
+        next assemblies, at the time they are assembled for; None = zero values."""
+        if values is None:
+            self.ctx.check(self.ctx.lib.cdgpu_tcd_set_dirichlet(self.ctx.h, self.tcd, None))
+            return
+        v = _f64(values)
+        assert len(v) == self.N_DOF - self.N_Active
+        self.ctx.check(self.ctx.lib.cdgpu_tcd_set_dirichlet(self.ctx.h, self.tcd, _p(v)))
+
     def AssembleMRhs(self, sol=None):
         self.ctx.check(self.ctx.lib.cdgpu_tcd_assemble_mass(self.ctx.h, self.tcd))
         if sol is not None:

@@ -6,8 +6,9 @@ oracle/build_ref.py from the reference's own sources) on small unit-square /
 unit-cube problems and stores everything they dump -- cell vertices, DOF maps,
 CSR patterns, matrix entries, right-hand sides, parent maps, dense
 prolongations, solutions, iteration counts and (sine problem) the L2 / H1-semi
-errors -- as compressed .npz files.  Needs the reference build; the tests only
-read the .npz files.
+errors -- as compressed .npz files, and the errors that the reference's unchanged
+TCD3D program prints over a Crank-Nicolson run (tcd3d_amc_16.json).  Needs the
+reference build; the tests only read the fixtures.
 
 Usage: python tests/golden/make_golden.py [case names; default all]
 """
@@ -108,12 +109,77 @@ def run_case(name, dim, order, disc, steps, levels, example, eps, b, c, f, extra
     print(f"{name}: levels={d['levels']} n_dof={d[f'L{levels - 1}_n_dof']} its={d['iterations']}")
 
 
+# The reference's own time-dependent program, unchanged: 3DPrograms/TCD3D_ParMooN.C with its
+# example Examples/TCD_3D/amc.h, in the setting of ReadIn/tcd3d_GMG.out (Q1 on the unit cube
+# refined 4 times, Crank-Nicolson, tau 0.1082532, end time 2, multigrid fixed point).
+TCD3D_DAT = """VERSION: 1
+LOGFILE: logfile
+OUTFILE: {out}
+BNDFILE: {mesh}/unit_cube.PRM
+GEOFILE: {mesh}/unit_cube.GEO
+MESH_TYPE: 0
+ANSATZ_ORDER: 1
+LEVELS: 1
+UNIFORM_STEPS: 4
+DISCTYPE: 1
+SOLVER_TYPE: 1
+SC_MG_TYPE_SCALAR: 1
+SC_SOLVER_SCALAR: 11
+SC_PRECONDITIONER_SCALAR: 5
+SC_LIN_RED_FACTOR_SCALAR: 0.0
+SC_LIN_RES_NORM_MIN_SCALAR: 1e-11
+SC_LIN_MAXIT_SCALAR: 100
+SC_MG_CYCLE_SCALAR: 1
+SC_SMOOTHER_SCALAR: 2
+SC_PRE_SMOOTH_SCALAR: 2
+SC_POST_SMOOTH_SCALAR: 2
+SC_COARSE_SMOOTHER_SCALAR: 3
+SC_COARSE_MAXIT_SCALAR: 10
+SC_COARSE_RED_FACTOR_SCALAR: 0.1
+SC_STEP_LENGTH_CONTROL_FINE_SCALAR: 0
+SC_STEP_LENGTH_CONTROL_ALL_SCALAR: 0
+MEASURE_ERRORS: 1
+WRITE_VTK: 0
+WRITE_PS: 0
+SC_VERBOSE: 0
+TIME_DISC: 2
+STARTTIME: 0
+ENDTIME: 2
+TIMESTEPLENGTH: 0.1082532
+PE_NR: 1
+RE_NR: 1
+"""
+
+
+def run_tcd3d_amc(tmp):
+    """Run oracle/_ref/tcd3d_main (the reference's TCD3D main, unchanged) and keep what it
+    prints after the initial interpolation and after every step: time, L2, H1-semi."""
+    import json
+    import re
+    out = os.path.join(tmp, "tcd3d.out")
+    dat = os.path.join(tmp, "tcd3d.dat")
+    with open(dat, "w") as fh:
+        fh.write(TCD3D_DAT.format(out=out, mesh=MESH))
+    subprocess.run([os.path.join(REF, "tcd3d_main"), dat], check=True, cwd=tmp, capture_output=True)
+    text = open(out).read()
+    rows = re.findall(r"^time: (\S+)\nL2: (\S+)\nH1-semi: (\S+)$", text, re.M)
+    its = [int(v) for v in re.findall(r"^ FP ITE:\s+(\d+)", text, re.M)]
+    assert len(rows) == 20 and len(its) == 19, (len(rows), len(its))
+    with open(os.path.join(HERE, "tcd3d_amc_16.json"), "w") as fh:
+        json.dump({"program": "3DPrograms/TCD3D_ParMooN.C (Examples/TCD_3D/amc.h)",
+                   "dat": TCD3D_DAT.format(out="tcd3d.out", mesh="oracle/meshes"),
+                   "rows": [list(r) for r in rows], "fp_iterations": its}, fh, indent=1)
+    print(f"tcd3d_amc_16: {len(rows)} error lines, last {rows[-1]}")
+
+
 def main():
     only = set(sys.argv[1:])
     with tempfile.TemporaryDirectory() as tmp:
         for case in CASES:
             if not only or case[0] in only:
                 run_case(*case, tmp)
+        if not only or "tcd3d_amc_16" in only:
+            run_tcd3d_amc(tmp)
 
 
 if __name__ == "__main__":
