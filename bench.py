@@ -534,6 +534,7 @@ def run_batched(ctx, args):
     t_submit = time.perf_counter() - t0
     B.run(8)
     t_total = time.perf_counter() - t0
+    loop_mode, loop_launches, host_its = B.loop_info()
     its, status = [], []
     for sl in slots:
         _, info = B.fetch(sl, 0)
@@ -559,6 +560,9 @@ def run_batched(ctx, args):
         "instances": len(work), "wall_s": t_total, "submit_s": t_submit,
         "dofs_total": int(sum(W.dofs(2, w["order"], w["n_used"]) for w in work)),
         "device_bytes": int(need), "structures": len(cache.ids),
+        "iteration_loop": {"mode": {1: "device (conditional CUDA graph)", 2: "device (conditional CUDA graph, "
+                                    "no PDL in the body)", 0: "host"}.get(loop_mode, "none"),
+                           "graph_launches": loop_launches, "host_iterations": host_its},
         "converged": int(sum(1 for st in status if st == 0)),
         "iterations": {"min": int(min(its)), "median": float(np.median(its)), "p99": float(np.percentile(its, 99)),
                        "max": int(max(its))},

@@ -330,8 +330,17 @@ int cdgpu_batch_create(cdgpu_ctx *ctx, const cdgpu_solver_params *params, int *b
 int cdgpu_batch_submit(cdgpu_ctx *ctx, int batch_id, int mg_id, const cdgpu_coeffs *co, int disctype,
                        int coarse_disctype, int *slot);
 /* run up to `iterations` FGMRES iterations of every running instance; *running (nullable)
- * = instances still running afterwards */
+ * = instances still running afterwards.  The iterations run in a device-side loop: one CUDA
+ * graph per running set whose WHILE node repeats an iteration of every running solve until
+ * all have finished or `iterations` are done, so one call is one graph launch and one wait. */
 int cdgpu_batch_advance(cdgpu_ctx *ctx, int batch_id, int iterations, int *running);
+/* how cdgpu_batch_advance ran: *mode (nullable) 1 = device-side loop, 2 = device-side loop
+ * without programmatic dependent launch inside the loop body (a driver that refused it),
+ * 0 = host loop (a driver without conditional graph nodes), -1 = not yet run;
+ * *graph_launches, *host_iterations (nullable) = advance calls run as one graph launch,
+ * iterations launched from the host loop. */
+int cdgpu_batch_loop_info(cdgpu_ctx *ctx, int batch_id, int *mode, long long *graph_launches,
+                          long long *host_iterations);
 /* a time-dependent instance (theta scheme, as cdgpu_tcd_* per instance, SystemTCD2D.C:
  * 154-235): mass matrix M and stiffness matrix A (disctype, every level) with coefficients
  * co, system matrices M + tau*theta1*A on every level and K = M - tau*theta2*A on the finest,

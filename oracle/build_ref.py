@@ -192,6 +192,9 @@ def main():
         if geo == "3D":
             # the reference's CD3D main unchanged: on its own TSystemCD3D (CPU) and on libcdgpu
             link_main(a.ref, geo, lib, "cd3d_main", "3DPrograms/CD3D_ParMooN.C", gpu=False)
+            # the reference's TCD3D main unchanged (its example amc.h), for the time-dependent
+            # known answer (tests/golden/make_golden.py)
+            link_main(a.ref, geo, lib, "tcd3d_main", "3DPrograms/TCD3D_ParMooN.C", gpu=False)
             if have_gpu_lib:
                 link_main(a.ref, geo, lib, "cd3d_main_gpu", "3DPrograms/CD3D_ParMooN.C", gpu=True)
         elif have_gpu_lib:

@@ -100,6 +100,7 @@ SIGNATURES = {
     "cdgpu_batch_fetch": (_I, [_P, _I, _I, _P, C.POINTER(SolveInfo)]),
     "cdgpu_batch_release": (_I, [_P, _I, _I]),
     "cdgpu_batch_memory": (_I, [_P, _I, C.POINTER(C.c_ulonglong)]),
+    "cdgpu_batch_loop_info": (_I, [_P, _I, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "cdgpu_batch_instance_bytes": (_I, [_P, _I, _I, C.POINTER(C.c_ulonglong)]),
 }
 

@@ -182,7 +182,8 @@ int cdgpu_upload_space(cdgpu_ctx *ctx, int dim, int order, int n_cells, const do
   for (int c = 0; c < n_cells && s->all_affine; c++)
     s->all_affine = cell_is_affine(dim, &s->h_coords[(size_t)c * s->nv * dim]);
   int rc;
-  if ((rc = dev_alloc(ctx, &s->d_coords, s->h_coords.size())) || (rc = dev_alloc(ctx, &s->d_gn, s->h_gn.size())))
+  // GlobalNumbers get 4 spare ints: bulk copies of a tile's numbers round their size up to 16 bytes
+  if ((rc = dev_alloc(ctx, &s->d_coords, s->h_coords.size())) || (rc = dev_alloc(ctx, &s->d_gn, s->h_gn.size() + 4)))
   {
     free_space(s);
     return rc;

@@ -113,6 +113,12 @@ struct Batch
   BTab tcd_csr, tcd_items; // every time-dependent instance, running or idle
   cudaGraphExec_t tcd_graph = nullptr;
   int tcd_graph_k = 0;
+  // the device-side iteration loop: one graph whose WHILE node runs FGMRES iterations of the
+  // running set until every solve has finished or the call's iteration budget is spent
+  cudaGraphExec_t loop_graph = nullptr;
+  int *d_loop = nullptr;        // iterations left in the current call
+  int loop_mode = -1;           // -1 not tried, 0 host loop, 1 graph with PDL, 2 graph without
+  long long loop_launches = 0, host_iterations = 0;
   std::vector<BTab> smooth, restrict_, coarse;
   std::vector<std::vector<BTab>> color;
   std::vector<int> ncolor_max;
@@ -133,7 +139,8 @@ void free_batch(Batch *b)
   for (auto &in : b->inst)
     for (void *p : in.allocs) cudaFree(p);
   if (b->tcd_graph) cudaGraphExecDestroy(b->tcd_graph);
-  void *ptrs[] = {b->d_ctl, b->d_lev, b->d_state, b->d_partial, b->d_tab};
+  if (b->loop_graph) cudaGraphExecDestroy(b->loop_graph);
+  void *ptrs[] = {b->d_ctl, b->d_lev, b->d_state, b->d_partial, b->d_tab, b->d_loop};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (b->h_state) cudaFreeHost(b->h_state);
@@ -626,6 +633,29 @@ __global__ void b_post(BTab t, BCtl *__restrict__ ctl, int *__restrict__ state_o
   }
 }
 
+// condition of the device-side iteration loop: another iteration while any solve of the set
+// runs and the call's budget (loop[0]) lasts; consume = 1 after an iteration.  One block.
+__global__ void b_loop_ctl(BTab t, const BCtl *__restrict__ ctl, int *__restrict__ loop,
+                           cudaGraphConditionalHandle cond, int consume)
+{
+  CD_PDL_ENTRY();
+  int any = 0;
+  for (int k = threadIdx.x; k < t.K; k += blockDim.x) any |= ctl[t.item[k]].state == ST_RUN;
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0)
+  {
+    const int left = loop[0] - consume;
+    loop[0] = left;
+    cudaGraphSetConditional(cond, any && left > 0 ? 1u : 0u);
+  }
+}
+
+__global__ void b_loop_budget(int *__restrict__ loop, int iterations)
+{
+  CD_PDL_ENTRY();
+  loop[0] = iterations;
+}
+
 // restart: beta = ||b - A x||, stopping test on it, s = (beta, 0, ...), j = 0
 __global__ void b_restart(BTab t, BCtl *__restrict__ ctl, int stop_rule, double red_factor, double res_norm_min)
 {
@@ -953,6 +983,7 @@ static int build_tables(cdgpu_ctx *ctx, Batch &b)
   for (int i = 0; i < (int)b.inst.size(); i++)
     if (b.inst[i].used && (b.inst[i].state == ST_RUN || b.inst[i].tcd)) b.run.push_back(i);
   if (b.tcd_graph) { cudaGraphExecDestroy(b.tcd_graph); b.tcd_graph = nullptr; }
+  if (b.loop_graph) { cudaGraphExecDestroy(b.loop_graph); b.loop_graph = nullptr; }
   int D = 0;
   for (int i : b.run) D = std::max(D, b.inst[i].L);
   b.depth = D;
@@ -1241,6 +1272,82 @@ static int assemble_to(cdgpu_ctx *ctx, Space &s, int disctype, const cdgpu_coeff
   return rc;
 }
 
+// The device-side iteration loop as one graph: a kernel that sets the WHILE node's condition,
+// then the WHILE node whose body is one FGMRES iteration of every running solve (the kernels
+// of batch_iteration) followed by the kernel that consumes one iteration of the budget and
+// sets the condition again.  Captured once per running set.  A driver that refuses the
+// body's programmatic dependencies gets the body without them; one that refuses conditional
+// nodes leaves the host loop (loop_mode 0).  Only API calls can fail here: nothing runs.
+static int build_loop_graph(cdgpu_ctx *ctx, Batch &b, bool pdl)
+{
+  int rc;
+  if (!b.d_loop && (rc = dev_alloc(ctx, &b.d_loop, 1))) return rc;
+  cudaGraph_t g = nullptr;
+  cudaGraphConditionalHandle cond;
+  cudaGraphNode_t init = nullptr, wnode = nullptr;
+  cudaError_t e = cudaGraphCreate(&g, 0);
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&cond, g, 0, 0);
+  if (e == cudaSuccess)
+  {
+    cudaKernelNodeParams kp = {};
+    BTab items = b.items;
+    BCtl *ctl = b.d_ctl;
+    int *loop = b.d_loop;
+    int consume = 0;
+    void *args[] = {&items, &ctl, &loop, &cond, &consume};
+    kp.func = (void *)b_loop_ctl;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(256);
+    kp.kernelParams = args;
+    e = cudaGraphAddKernelNode(&init, g, nullptr, 0, &kp);
+  }
+  cudaGraph_t body = nullptr;
+  if (e == cudaSuccess)
+  {
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = cond;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    e = cudaGraphAddNode(&wnode, g, &init, 1, &np);
+    if (e == cudaSuccess) body = np.conditional.phGraph_out[0];
+  }
+  if (e != cudaSuccess)
+  {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return CDGPU_ERR_UNSUPPORTED;
+  }
+  const long long before = ctx->launches;
+  const bool pdl_was = cd_pdl_enabled();
+  cd_pdl_enabled() = pdl;
+  e = cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  rc = CDGPU_OK;
+  if (e == cudaSuccess)
+  {
+    rc = batch_iteration(ctx, b);
+    if (!rc)
+    {
+      (void)cd_launch(b_loop_ctl, 1, 256, 0, ctx->stream, b.items, (const BCtl *)b.d_ctl, b.d_loop, cond, 1);
+      if (cudaGetLastError() != cudaSuccess) rc = CDGPU_ERR_CUDA;
+    }
+    cudaGraph_t captured = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &captured);
+    if (e == cudaSuccess) e = e2;
+  }
+  cd_pdl_enabled() = pdl_was;
+  ctx->launches = before;
+  if (e == cudaSuccess && !rc) e = cudaGraphInstantiate(&b.loop_graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess || rc)
+  {
+    b.loop_graph = nullptr;
+    cudaGetLastError();
+    return rc ? rc : CDGPU_ERR_UNSUPPORTED;
+  }
+  return CDGPU_OK;
+}
+
 static int running_count(const Batch &b)
 {
   int r = 0;
@@ -1330,8 +1437,35 @@ int cdgpu_batch_advance(cdgpu_ctx *ctx, int batch_id, int iterations, int *runni
     b.check_pending = false;
   }
   if (b.dirty && (rc = build_tables(ctx, b))) return rc;
-  for (int it = 0; it < iterations && running_count(b) > 0; it++)
-    if ((rc = batch_iteration(ctx, b))) return rc;
+  if (iterations > 0 && running_count(b) > 0)
+  {
+    // the iterations run in a device-side loop (one graph launch) where the driver takes a
+    // conditional node, else from this host loop
+    if (!b.loop_graph && b.loop_mode != 0)
+    {
+      const int first = b.loop_mode < 0 ? 1 : b.loop_mode;
+      for (int mode = first; mode <= 2 && !b.loop_graph; mode++)
+      {
+        rc = build_loop_graph(ctx, b, mode == 1);
+        if (rc && rc != CDGPU_ERR_UNSUPPORTED) return rc;
+        if (!rc) b.loop_mode = mode;
+      }
+      if (!b.loop_graph) b.loop_mode = 0;
+    }
+    if (b.loop_graph)
+    {
+      (void)cd_launch(b_loop_budget, 1, 1, 0, ctx->stream, b.d_loop, iterations);
+      CD_LAUNCHED(ctx);
+      CD_CUDA(ctx, cudaGraphLaunch(b.loop_graph, ctx->stream));
+      b.loop_launches++;
+    }
+    else
+      for (int it = 0; it < iterations && running_count(b) > 0; it++)
+      {
+        if ((rc = batch_iteration(ctx, b))) return rc;
+        b.host_iterations++;
+      }
+  }
   // collect the states
   if (!b.run.empty())
   {
@@ -1492,6 +1626,17 @@ int cdgpu_batch_release(cdgpu_ctx *ctx, int batch_id, int slot)
   auto &q = b->done_queue;
   q.erase(std::remove(q.begin(), q.end(), slot), q.end());
   if (was_running) b->dirty = true;
+  return CDGPU_OK;
+}
+
+int cdgpu_batch_loop_info(cdgpu_ctx *ctx, int batch_id, int *mode, long long *graph_launches,
+                          long long *host_iterations)
+{
+  Batch *b = get_batch(ctx, batch_id);
+  if (!b) return fail(ctx, CDGPU_ERR_INVALID, "batch_loop_info: bad id");
+  if (mode) *mode = b->loop_mode;
+  if (graph_launches) *graph_launches = b->loop_launches;
+  if (host_iterations) *host_iterations = b->host_iterations;
   return CDGPU_OK;
 }
 

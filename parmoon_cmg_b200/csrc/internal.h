@@ -229,6 +229,14 @@ int cuda_fail(cdgpu_ctx *ctx, cudaError_t e, const char *what);
     CD_PDL_TRIGGER();  \
   } while (0)
 
+// false while this thread captures a graph whose kernels must not carry programmatic
+// dependencies (a conditional node's body, where a driver may refuse them)
+inline bool &cd_pdl_enabled()
+{
+  static thread_local bool on = true;
+  return on;
+}
+
 template <typename... KArgs, typename... Args>
 inline cudaError_t cd_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
                              Args &&...args)
@@ -242,7 +250,7 @@ inline cudaError_t cd_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, si
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = cd_pdl_enabled() ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 

@@ -159,6 +159,25 @@ __device__ __forceinline__ uint32_t mf_wait_parity(uint64_t *mbar, uint32_t phas
   return done;
 }
 
+// bulk copy (cp.async.bulk, 1D TMA) of `bytes` (a multiple of 16, both addresses 16-byte
+// aligned) from global to shared memory, completing on mbarrier `bar`
+__device__ __forceinline__ void mf_bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   mf_smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(mf_smem_u32(bar))
+               : "memory");
+}
+
+// dynamic shared memory of mf_cell27_tc_kernel<T>: A (128 x 32 floats), B (32T x 32 floats),
+// two stages of a tile's GlobalNumbers (128 x 27 ints) and cell coefficients (128 x T floats)
+template <int T> constexpr int mf_tc_gn_bytes() { return 128 * 27 * 4; }
+template <int T> constexpr int mf_tc_cf_bytes() { return 128 * T * 4; }
+template <int T> constexpr int mf_tc_smem_bytes()
+{
+  return 128 * 32 * 4 + 32 * T * 32 * 4 + 2 * (mf_tc_gn_bytes<T>() + mf_tc_cf_bytes<T>());
+}
+
 template <int T>
 __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const int *__restrict__ gn,
                                                               const float *__restrict__ cf32,
@@ -166,16 +185,50 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
                                                               const float *__restrict__ x, float *__restrict__ ybuf,
                                                               int *__restrict__ err, int pre)
 {
-  // with pre, the tensors, the shared-memory set-up and the first tile's DOF numbers and
-  // coefficients (written by no kernel of the cycle) come before the wait for the predecessor
+  // with pre, the tensors, the shared-memory set-up and the bulk copies of the first two
+  // tiles' DOF numbers and coefficients (written by no kernel of the cycle) come before the
+  // wait for the predecessor
   if (!pre) CD_PDL_ENTRY();
   constexpr int MT = 128, KP = 32, NB = 27, N = 32 * T, NH = N / 2;
   extern __shared__ __align__(1024) unsigned char mf_sm[];
   unsigned char *As = mf_sm;                    // 128 x 32 x 4 = 16 KB
   unsigned char *Bs = mf_sm + MT * KP * 4;      // N x 32 x 4
+  unsigned char *St = Bs + N * KP * 4;          // 2 stages of (GlobalNumbers, coefficients)
+  constexpr int GB = mf_tc_gn_bytes<T>(), CB = mf_tc_cf_bytes<T>();
   __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t sbar[2];
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int n_tiles = (n_cells + MT - 1) / MT;
+  if (tid == 0)
+  {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mf_smem_u32(&mbar)), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mf_smem_u32(&sbar[0])), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mf_smem_u32(&sbar[1])), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // the copies of a tile's numbers and coefficients: sizes rounded up to 16 bytes (the
+  // GlobalNumbers array carries 4 spare ints, the coefficient array n_cells * (14 - T) spare
+  // floats); only the tile's own cells are read back
+  // per stage: copies issued (thread 0) and waits passed, as scalars (no local memory)
+  int issued0 = 0, issued1 = 0, waited0 = 0, waited1 = 0;
+  auto issue = [&](int tile, int stage) {
+    if (stage) issued1++; else issued0++;
+    const int c0 = tile * MT, nc = min(MT, n_cells - c0);
+    const uint32_t gb = ((uint32_t)nc * NB * 4 + 15u) & ~15u, cb = ((uint32_t)nc * T * 4 + 15u) & ~15u;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mf_smem_u32(&sbar[stage])),
+                 "r"(gb + cb)
+                 : "memory");
+    unsigned char *dst = St + stage * (GB + CB);
+    mf_bulk_g2s(dst, gn + (size_t)c0 * NB, gb, &sbar[stage]);
+    mf_bulk_g2s(dst + GB, cf32 + (size_t)c0 * T, cb, &sbar[stage]);
+  };
+  __syncthreads();
+  if (tid == 0)
+  {
+    if (blockIdx.x < n_tiles) issue(blockIdx.x, 0);
+    if (blockIdx.x + gridDim.x < n_tiles) issue(blockIdx.x + gridDim.x, 1);
+  }
   // B = the tensors, zero-padded rows i >= 27 and columns k >= 27; A zero everywhere once
   for (int e = tid; e < N * KP; e += blockDim.x)
   {
@@ -184,26 +237,6 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
     *(float *)(Bs + mf_core_off(n, k, N)) = v;
   }
   for (int e = tid; e < MT * KP; e += blockDim.x) ((float *)As)[e] = 0.f;
-  if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mf_smem_u32(&mbar)), "r"(1));
-  const int n_tiles = (n_cells + MT - 1) / MT;
-  // the next tile's cell values and coefficients, one cell per thread (thread r gathers and
-  // later contracts cell c0 + r): loaded before the current tile's products are awaited, so
-  // the gather latency overlaps the tensor-core work and the epilogue
-  float vn[NB], cn[T];
-  int gq[NB];
-  auto prefetch_idx = [&](int tile) {
-    const int c = tile * MT + tid;
-    const bool in = tile < n_tiles && c < n_cells;
-#pragma unroll
-    for (int k = 0; k < NB; k++) gq[k] = in ? __ldg(gn + (size_t)c * NB + k) : -1;
-#pragma unroll
-    for (int t = 0; t < T; t++) cn[t] = in ? __ldg(cf32 + (size_t)c * T + t) : 0.f;
-  };
-  auto prefetch_x = [&]() {
-#pragma unroll
-    for (int k = 0; k < NB; k++) vn[k] = gq[k] >= 0 ? __ldg(x + gq[k]) : 0.f;
-  };
-  prefetch_idx(blockIdx.x);
   if (pre) CD_PDL_ENTRY();
   if (warp == 0)
   {
@@ -218,8 +251,42 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
   const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(NH >> 3) << 17) | ((uint32_t)(MT >> 4) << 24);
   uint32_t phase = 0, pend_phase = 0;
   bool ok = true, pending = false;
-  prefetch_x();
-  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
+  // the next tile's cell values and coefficients, one cell per thread (thread r gathers and
+  // later contracts cell c0 + r), read from the staged copy of the tile's numbers and
+  // coefficients; gathered before the current tile's products are awaited, so the gather
+  // latency overlaps the tensor-core work and the epilogue.  li = the CTA's tile counter.
+  float vn[NB], cn[T];
+  auto gather = [&](int li) {
+    const int tile = blockIdx.x + li * gridDim.x;
+    const bool have = tile < n_tiles;
+    const int stage = li & 1;
+    bool ready = true;
+    if (have && ok)
+    {
+      const uint32_t got = mf_wait_parity(&sbar[stage], (uint32_t)(li >> 1) & 1u, 1L << 24);
+      ready = __syncthreads_and(got != 0) != 0;
+      if (ready)
+      {
+        if (stage) waited1++; else waited0++;
+      }
+      else
+      {
+        if (tid == 0) atomicExch(err, 3);
+        ok = false;
+      }
+    }
+    const int c = tile * MT + tid;
+    const bool in = have && ready && ok && c < n_cells;
+    const int *gq = (const int *)(St + stage * (GB + CB));
+    const float *cq = (const float *)(St + stage * (GB + CB) + GB);
+#pragma unroll
+    for (int k = 0; k < NB; k++) vn[k] = in ? __ldg(x + gq[tid * NB + k]) : 0.f;
+#pragma unroll
+    for (int t = 0; t < T; t++) cn[t] = in ? cq[tid * T + t] : 0.f;
+  };
+  gather(0);
+  int li = 0;
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, li++)
   {
     const int c0 = tile * MT;
     float cf[T];
@@ -230,6 +297,9 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // every thread has gathered this tile from stage li & 1 (before the barrier above): refill
+    // the stage with the tile after next
+    if (tid == 0 && ok && tile + 2 * gridDim.x < n_tiles) issue(tile + 2 * gridDim.x, li & 1);
     if (tid == 0 && ok)
     {
       const uint32_t a0 = mf_smem_u32(As), b0 = mf_smem_u32(Bs);
@@ -249,8 +319,7 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
                        mf_smem_u32(&mbar))
                    : "memory");
     }
-    prefetch_idx(tile + gridDim.x);
-    prefetch_x();
+    gather(li + 1);
     // bounded wait for this tile's products (an error flag instead of a hang); the outcome is
     // made CTA-uniform, so the warp-collective TMEM loads below run with every lane or none
     const uint32_t done = ok ? mf_wait_parity(&mbar, phase, 1L << 24) : 0u;
@@ -270,11 +339,38 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
       float y[NB];
 #pragma unroll
       for (int i = 0; i < NB; i++) y[i] = 0.f;
-#pragma unroll 1
-      for (int t = 0; t < T; t++)
+      // two tensors (64 columns) per TMEM load, one wait per load
+#pragma unroll
+      for (int t = 0; t + 1 < T; t += 2)
+      {
+        uint32_t v[64];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + t * 32;
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+                     "%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,"
+                     "%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,"
+                     "%61,%62,%63}, [%64];"
+                     : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                       "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                       "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                       "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                       "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31]), "=r"(v[32]), "=r"(v[33]), "=r"(v[34]),
+                       "=r"(v[35]), "=r"(v[36]), "=r"(v[37]), "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]),
+                       "=r"(v[42]), "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]), "=r"(v[48]),
+                       "=r"(v[49]), "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]), "=r"(v[54]), "=r"(v[55]),
+                       "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]), "=r"(v[60]), "=r"(v[61]), "=r"(v[62]),
+                       "=r"(v[63])
+                     : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const float c_a = cf[t], c_b = cf[t + 1];
+#pragma unroll
+        for (int i = 0; i < NB; i++) y[i] += c_a * __uint_as_float(v[i]);
+#pragma unroll
+        for (int i = 0; i < NB; i++) y[i] += c_b * __uint_as_float(v[32 + i]);
+      }
+      if (T % 2)
       {
         uint32_t v[32];
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + t * 32;
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (T - 1) * 32;
         asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
                      "%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
                      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
@@ -284,11 +380,8 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
                        "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                      : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        float cft = cf[0];
 #pragma unroll
-        for (int u = 1; u < T; u++) cft = t == u ? cf[u] : cft;
-#pragma unroll
-        for (int i = 0; i < NB; i++) y[i] += cft * __uint_as_float(v[i]);
+        for (int i = 0; i < NB; i++) y[i] += cf[T - 1] * __uint_as_float(v[i]);
       }
       if (c < n_cells)
 #pragma unroll
@@ -298,17 +391,28 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
     __syncthreads();
   }
   // after a timed-out wait, wait once more (bounded) for the products still in flight before
-  // the accumulator columns are released
+  // the accumulator columns are released, and for the staged copies still in flight before
+  // the CTA's shared memory is given up
   if (pending)
   {
     const uint32_t late = tid == 0 ? mf_wait_parity(&mbar, pend_phase, 1L << 26) : 1u;
     __syncthreads_or(late == 0);
   }
+  if (tid == 0)
+  {
+    // a copy still in flight (after a timeout): bounded wait for it
+    if (issued0 > waited0) (void)mf_wait_parity(&sbar[0], (uint32_t)(issued0 - 1) & 1u, 1L << 24);
+    if (issued1 > waited1) (void)mf_wait_parity(&sbar[1], (uint32_t)(issued1 - 1) & 1u, 1L << 24);
+  }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
 }
 
-template <int T> inline size_t mf_tc_smem() { return (size_t)128 * 32 * 4 + (size_t)32 * T * 32 * 4; }
+template <int T> inline size_t mf_tc_smem() { return (size_t)mf_tc_smem_bytes<T>(); }
+// dynamic shared memory requested by every launch of the tensor-core kernel: more than either
+// instance needs, so that a second CTA never shares an SM (each CTA allocates 512 TMEM columns)
+constexpr int kMfTcSmem = 120 * 1024;
+static_assert(mf_tc_smem_bytes<13>() <= kMfTcSmem && mf_tc_smem_bytes<10>() <= kMfTcSmem, "tensor-core kernel smem");
 
 enum { MF_JACOBI = 0, MF_DEFECT = 1, MF_SPMV = 2 };
 
@@ -401,13 +505,13 @@ inline void mf_apply_cells(cdgpu_ctx *ctx, const Space &s, const float *x, bool 
     const int grid = std::max(1, std::min((s.n_cells + 127) / 128, ctx->sm_count));
     if (s.mf_T == 10)
     {
-      (void)cd_launch(mf_cell27_tc_kernel<10>, grid, 128, 120 * 1024, ctx->stream, s.n_cells, s.d_gn, s.d_cf32,
+      (void)cd_launch(mf_cell27_tc_kernel<10>, grid, 128, kMfTcSmem, ctx->stream, s.n_cells, s.d_gn, s.d_cf32,
                       s.d_R32, x, s.d_ybuf, ctx->d_err, ctx->pdl_pre ? 1 : 0);
       return;
     }
     if (s.mf_T == 13)
     {
-      (void)cd_launch(mf_cell27_tc_kernel<13>, grid, 128, 120 * 1024, ctx->stream, s.n_cells, s.d_gn, s.d_cf32,
+      (void)cd_launch(mf_cell27_tc_kernel<13>, grid, 128, kMfTcSmem, ctx->stream, s.n_cells, s.d_gn, s.d_cf32,
                       s.d_R32, x, s.d_ybuf, ctx->d_err, ctx->pdl_pre ? 1 : 0);
       return;
     }

@@ -1436,8 +1436,8 @@ static int prepare_mf(cdgpu_ctx *ctx, Space &s)
     CD_LAUNCHED(ctx);
     s.mf_version = s.assembly_version;
   }
-  CD_CUDA(ctx, cudaFuncSetAttribute(mf_cell27_tc_kernel<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
-  CD_CUDA(ctx, cudaFuncSetAttribute(mf_cell27_tc_kernel<13>, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
+  CD_CUDA(ctx, cudaFuncSetAttribute(mf_cell27_tc_kernel<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMfTcSmem));
+  CD_CUDA(ctx, cudaFuncSetAttribute(mf_cell27_tc_kernel<13>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMfTcSmem));
   if (!ctx->d_err)
   {
     if ((rc = dev_alloc(ctx, &ctx->d_err, 1))) return rc;

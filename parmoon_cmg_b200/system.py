@@ -477,6 +477,14 @@ class Batch:
         self.ctx.check(self.ctx.lib.cdgpu_batch_memory(self.ctx.h, self.id, C.byref(out)))
         return out.value
 
+    def loop_info(self):
+        """(mode, graph launches, host-loop iterations) of the advance calls so far: mode 1 or
+        2 = device-side iteration loop (conditional CUDA graph), 0 = host loop."""
+        mode, gl, hi = C.c_int(), C.c_longlong(), C.c_longlong()
+        self.ctx.check(self.ctx.lib.cdgpu_batch_loop_info(self.ctx.h, self.id, C.byref(mode), C.byref(gl),
+                                                          C.byref(hi)))
+        return mode.value, gl.value, hi.value
+
     def run(self, iterations_per_poll=8):
         """Advance until no instance is running; returns the finished slots in order."""
         done = []

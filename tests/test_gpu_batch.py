@@ -79,6 +79,9 @@ def test_batch_matches_fp64_solutions(ctx, oracle_lib, smoother):
         meta.append((slot, spaces, parents, dim, order, eps, b))
     done = B.run(4)
     assert sorted(done) == sorted(m[0] for m in meta)
+    # the iterations ran in the device-side loop: one conditional graph launch per advance
+    mode, graph_launches, host_iterations = B.loop_info()
+    assert mode in (1, 2) and graph_launches > 0 and host_iterations == 0, B.loop_info()
     for slot, spaces, parents, dim, order, eps, b in meta:
         x, info = B.fetch(slot, spaces[-1]["n_dof"])
         ref = oracle_solution(oracle_lib, dim, order, spaces, parents, eps, b, SUPG)
