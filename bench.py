@@ -72,6 +72,7 @@ def parse():
                     help="mean arrivals per second, swept in this order (comma separated)")
     ap.add_argument("--no-tcd", action="store_true", help="skip the time-dependent CD2D section")
     ap.add_argument("--no-cd2d", action="store_true", help="skip the CD2D plain FP64 section")
+    ap.add_argument("--no-general", action="store_true", help="skip the general-path assembly section")
     ap.add_argument("--tcd-instances", type=int, default=256)
     ap.add_argument("--tcd-steps", type=int, default=1000)
     return ap.parse_args()
@@ -783,6 +784,53 @@ def run_cd2d(ctx, args):
     return out
 
 
+def run_general_assembly(ctx, args):
+    """Assembly on the general path (local matrices by FP64 Gauss quadrature, as for any
+    example whose BilinearCoeffs vary in space): CD3D Q2 at 32^3 cells, Galerkin, coefficients
+    tabulated at the quadrature points (eps 1e-2, b = (0.5 - y, x - 0.5, 0.25), c = 0, f = 1).
+    One step = the finest level's local matrices + the row gather into CSR (f64 + f32 entries,
+    rhs); device time with CUDA events on the library's stream, the inputs in HBM."""
+    import torch
+    from parmoon_cmg_b200 import _lib, mesh
+    from parmoon_cmg_b200.system import GALERKIN, coeffs
+    spaces, _ = mesh.structured_hierarchy(3, 2, args.n, 1)
+    sp = spaces[0]
+    n_cells = len(sp["begin_index"]) - 1
+    sid = ctx.upload_space(sp)
+    ctx.build_pattern(sid)
+    xq = ctx.quadrature_points(sid, n_cells, 3)
+    tab = np.zeros(xq.shape[:-1] + (6,))
+    tab[..., 0] = 1e-2
+    tab[..., 1] = 0.5 - xq[..., 1]
+    tab[..., 2] = xq[..., 0] - 0.5
+    tab[..., 3] = 0.25
+    tab[..., 5] = 1.0
+    ctx.set_coeffs(sid, coeffs(_lib.COEFF_TABLE), tab)
+    mg = ctx.hierarchy([sid], [None])
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", torch.cuda.current_device()))
+    for _ in range(max(3, args.warmup)):
+        ctx.assemble_hierarchy(mg, GALERKIN, GALERKIN)
+    torch.cuda.synchronize()
+    reps = 10
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        ctx.assemble_hierarchy(mg, GALERKIN, GALERKIN)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    nq, nbf = xq.shape[1], 27
+    # algorithmic FP64 work of the local matrices: per cell, quadrature point and entry the
+    # diffusion (3 + 3 products and sums), convection and reaction terms (~20 flops)
+    flops = n_cells * nq * (nbf * nbf + nbf) * 20.0
+    return {"metric": "general-path assembly (CD3D Q2, tabulated coefficients) cells/s",
+            "value": n_cells / (ms * 1e-3), "unit": "cells/s", "ms_per_assembly": ms, "n_cells": n_cells,
+            "quadrature_points": nq, "fp64_gflops_local_matrices": flops / (ms * 1e-3) / 1e9,
+            "config": f"{args.n}^3 Q2 hexahedra, Galerkin, coefficient table per quadrature point, "
+                      "finest level only (local matrices + CSR row gather)"}
+
+
 def run_tcd(ctx, args):
     """Time-dependent CD2D: instances of 128^2 Q2 on the unit square, Crank-Nicolson with
     tau = 1e-3, rotating convection b = (0.5 - y, x - 0.5), eps log-uniform in [1e-5, 1e-2]
@@ -857,6 +905,8 @@ def main():
             result["serving"] = run_serving(ctx, args)
         if not args.no_tcd:
             result["tcd"] = run_tcd(ctx, args)
+        if not args.no_general:
+            result["general_assembly"] = run_general_assembly(ctx, args)
         if rank == 0:
             if not args.no_cpu_baseline:
                 tmp = tempfile.mkdtemp()

@@ -253,121 +253,330 @@ __global__ void cell_coef_kernel(CellCoefArgs a)
 }
 
 // ---------------------------------------------------------------------------
-// quadrature path: one CTA per cell, the reference's per-point local forms
-// (src/FE/ConvDiff2D.C:32-162, src/FE/ConvDiff3D.C:61-190) summed over the Gauss points
-// in the reference's order.  Writes nbf*nbf matrix entries then nbf rhs entries.
+// quadrature path: the reference's per-point local forms (src/FE/ConvDiff2D.C:32-162,
+// src/FE/ConvDiff3D.C:61-190) summed over the Gauss points in the reference's order.  Writes
+// nbf*nbf matrix entries then nbf rhs entries per cell.
+//
+// Persistent CTAs.  The reference element's tables (Gauss points and weights, basis values
+// and gradients, 2D second derivatives) are staged in shared memory once per CTA by one bulk
+// copy (cp.async.bulk, 1D TMA); each cell's geometry (vertex coordinates) and, for tabulated
+// coefficients, its per-point coefficient records are staged by bulk copies into one of two
+// stages, the next cell's copy in flight while the current cell is computed.  Every wait is
+// bounded: on a timeout the CTA sets the assembly's error flag (5), stops, and waits (bounded)
+// for its copies still in flight.
 // ---------------------------------------------------------------------------
 struct LocalArgs
 {
   int dim, nv, nbf, nq, n_cells, disctype, affine_all;
   Coef co;
   const double *coords, *tab; // tab: n_cells x nq x 6 (kind TABLE)
-  const double *qx, *qw, *phi, *dphi, *hphi;
+  const double *qtab;         // packed qx | qw | phi | dphi | hphi
+  int n_qx, n_qw, n_phi, n_dphi, n_stage_tab; // lengths (doubles); staged table = n_stage_tab
   double *out;
+  int *err;
 };
 
-__global__ void local_quad_kernel(LocalArgs a)
+constexpr long kLqSpin = 1L << 22;
+
+__device__ __forceinline__ uint32_t lq_smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool lq_try_wait(uint64_t *bar, uint32_t parity)
 {
-  extern __shared__ double sm[];
-  const int dim = a.dim, nbf = a.nbf, nq = a.nq;
-  double *g = sm;                      // nq x nbf x dim physical gradients
-  double *lap = g + nq * nbf * dim;    // nq x nbf physical Laplacians (2D SUPG)
-  double *mult = lap + nq * nbf;       // nq
-  double *kq = mult + nq;              // nq x 6 coefficients
-  double *dl = kq + nq * 6;            // nq SUPG parameters
-  double *Jis = dl + nq;               // nq x dim*dim
-  __shared__ double V[24];
-  int c = blockIdx.x;
-  for (int k = threadIdx.x; k < a.nv * dim; k += blockDim.x) V[k] = a.coords[(size_t)c * a.nv * dim + k];
-  __syncthreads();
-  for (int q = threadIdx.x; q < nq; q += blockDim.x)
+  uint32_t done;
+  asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+               "selp.b32 %0, 1, 0, P1;\n\t}"
+               : "=r"(done)
+               : "r"(lq_smem_u32(bar)), "r"(parity)
+               : "memory");
+  return done != 0;
+}
+
+__device__ __forceinline__ bool lq_wait(uint64_t *bar, uint32_t parity)
+{
+  for (long it = 0; it < kLqSpin; it++)
+    if (lq_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void lq_bulk(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   lq_smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(lq_smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void lq_expect(uint64_t *bar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(lq_smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__host__ __device__ inline int lq_even(int n) { return (n + 1) & ~1; } // doubles -> 16-byte multiple
+
+// shared-memory layout (in doubles) of local_quad_kernel
+struct LqLayout
+{
+  int tabs, g, lap, mult, kq, dl, Jis, stage0, stage_len, total;
+  __host__ __device__ LqLayout(int dim, int nv, int nbf, int nq, int disctype, int n_stage_tab, bool table)
   {
-    const double *xi = a.qx + q * dim;
-    double x[3], J[9], Ji[9];
-    d_ref_map(dim, a.nv, a.affine_all, V, xi, x, J);
-    double det = d_invert(dim, J, Ji);
-    mult[q] = a.qw[q] * fabs(det);
-    for (int k = 0; k < dim * dim; k++) Jis[q * dim * dim + k] = Ji[k];
-    double k6[6];
-    coef_at(a.co, a.tab ? a.tab + ((size_t)c * nq + q) * 6 : nullptr, x, k6);
-    for (int k = 0; k < 6; k++) kq[q * 6 + k] = k6[k];
-    dl[q] = a.disctype == CDGPU_SUPG
-                ? sdfem_delta(d_diameter(dim, V), k6[0], k6[1], k6[2], dim == 3 ? k6[3] : 0.0,
-                              a.co.delta0, a.co.poly_degree)
-                : 0.0;
+    tabs = 0;
+    g = lq_even(n_stage_tab);
+    lap = g + nq * nbf * dim;
+    const int nlap = (dim == 2 && disctype == CDGPU_SUPG) ? nq * nbf : 0;
+    mult = lap + nlap;
+    kq = mult + nq;
+    dl = kq + nq * 6;
+    Jis = dl + nq;
+    stage0 = lq_even(Jis + nq * dim * dim);
+    stage_len = lq_even(nv * dim) + (table ? nq * 6 : 0);
+    total = stage0 + 2 * stage_len;
+  }
+};
+
+__global__ void __launch_bounds__(256) local_quad_kernel(LocalArgs a)
+{
+  CD_PDL_ENTRY();
+  extern __shared__ __align__(16) double sm[];
+  __shared__ __align__(8) uint64_t bar[3]; // tables, cell stage 0, cell stage 1
+  const int dim = a.dim, nbf = a.nbf, nq = a.nq, nv = a.nv;
+  const bool table = a.tab != nullptr;
+  const LqLayout lay(dim, nv, nbf, nq, a.disctype, a.n_stage_tab, table);
+  const double *qx = sm, *qw = sm + a.n_qx, *phi = qw + a.n_qw, *dphi = phi + a.n_phi, *hphi = dphi + a.n_dphi;
+  double *g = sm + lay.g, *lap = sm + lay.lap, *mult = sm + lay.mult, *kq = sm + lay.kq, *dl = sm + lay.dl,
+         *Jis = sm + lay.Jis;
+  const uint32_t vbytes = (uint32_t)lq_even(nv * dim) * 8u, tbytes = table ? (uint32_t)nq * 48u : 0u;
+  // stage the cell's vertex coordinates (nv*dim doubles: 64 or 192 bytes) and coefficient
+  // records (nq * 48 bytes); both sizes and both offsets are multiples of 16 bytes
+  auto issue = [&](int c, int st) {
+    double *dst = sm + lay.stage0 + st * lay.stage_len;
+    lq_expect(&bar[1 + st], (uint32_t)(nv * dim * 8) + tbytes);
+    lq_bulk(dst, a.coords + (size_t)c * nv * dim, (uint32_t)(nv * dim * 8), &bar[1 + st]);
+    if (table) lq_bulk(dst + vbytes / 8, a.tab + (size_t)c * nq * 6, tbytes, &bar[1 + st]);
+  };
+  int issued0 = 0, issued1 = 0, waited0 = 0, waited1 = 0; // thread 0's copies per stage; waits
+  if (threadIdx.x == 0)
+  {
+    for (int k = 0; k < 3; k++) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(lq_smem_u32(&bar[k])), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const uint32_t tb = (uint32_t)lq_even(a.n_stage_tab) * 8u;
+    lq_expect(&bar[0], tb);
+    lq_bulk(sm, a.qtab, tb, &bar[0]);
+    if (blockIdx.x < a.n_cells) { issue(blockIdx.x, 0); issued0++; }
+    if (blockIdx.x + gridDim.x < a.n_cells) { issue(blockIdx.x + gridDim.x, 1); issued1++; }
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < nq * nbf; t += blockDim.x)
+  bool ok = __syncthreads_and(lq_wait(&bar[0], 0u)) != 0;
+  if (!ok && threadIdx.x == 0) atomicExch(a.err, 5);
+  int li = 0;
+  for (int c = blockIdx.x; ok && c < a.n_cells; c += gridDim.x, li++)
   {
-    int q = t / nbf, b = t % nbf;
-    const double *Ji = Jis + q * dim * dim;
-    const double *dp = a.dphi + (size_t)(q * nbf + b) * dim;
-    for (int r = 0; r < dim; r++)
+    const int st = li & 1;
+    const bool got = lq_wait(&bar[1 + st], (uint32_t)(li >> 1) & 1u);
+    if (!__syncthreads_and(got))
     {
-      double s = 0;
-      for (int e = 0; e < dim; e++) s += Ji[e * dim + r] * dp[e];
-      g[(q * nbf + b) * dim + r] = s;
+      if (threadIdx.x == 0) atomicExch(a.err, 5);
+      ok = false;
+      break;
     }
-    double l = 0;
-    if (dim == 2 && a.disctype == CDGPU_SUPG)
+    if (st) waited1++; else waited0++;
+    const double *V = sm + lay.stage0 + st * lay.stage_len;
+    const double *ctab = V + vbytes / 8;
+    for (int q = threadIdx.x; q < nq; q += blockDim.x)
     {
-      // physical second derivatives Ji^T (H - G) Ji: on a bilinear cell
-      // x = c0 + c1 xi + c2 eta + c3 xi eta the mixed reference derivative also carries
-      // grad(phi) . c3 (the D11 row of the 5x5 system of QuadBilinear::GetOrigValues,
-      // src/FE/QuadBilinear.C:531-549); an affine map has c3 = 0
-      const double *hp = a.hphi + (size_t)(q * nbf + b) * 4;
-      double gm = 0;
-      if (!a.affine_all)
+      const double *xi = qx + q * dim;
+      double x[3], J[9], Ji[9];
+      d_ref_map(dim, nv, a.affine_all, V, xi, x, J);
+      double det = d_invert(dim, J, Ji);
+      mult[q] = qw[q] * fabs(det);
+      for (int k = 0; k < dim * dim; k++) Jis[q * dim * dim + k] = Ji[k];
+      double k6[6];
+      coef_at(a.co, table ? ctab + q * 6 : nullptr, x, k6);
+      for (int k = 0; k < 6; k++) kq[q * 6 + k] = k6[k];
+      dl[q] = a.disctype == CDGPU_SUPG
+                  ? sdfem_delta(d_diameter(dim, V), k6[0], k6[1], k6[2], dim == 3 ? k6[3] : 0.0,
+                                a.co.delta0, a.co.poly_degree)
+                  : 0.0;
+    }
+    __syncthreads();
+    // physical gradients, component-major: g[(q * dim + r) * nbf + b]
+    for (int t = threadIdx.x; t < nq * nbf; t += blockDim.x)
+    {
+      int q = t / nbf, b = t % nbf;
+      const double *Ji = Jis + q * dim * dim;
+      const double *dp = dphi + (size_t)(q * nbf + b) * dim;
+      for (int r = 0; r < dim; r++)
+      {
+        double s = 0;
+        for (int e = 0; e < dim; e++) s += Ji[e * dim + r] * dp[e];
+        g[(q * dim + r) * nbf + b] = s;
+      }
+      if (dim == 2 && a.disctype == CDGPU_SUPG)
+      {
+        // physical second derivatives Ji^T (H - G) Ji: on a bilinear cell
+        // x = c0 + c1 xi + c2 eta + c3 xi eta the mixed reference derivative also carries
+        // grad(phi) . c3 (the D11 row of the 5x5 system of QuadBilinear::GetOrigValues,
+        // src/FE/QuadBilinear.C:531-549); an affine map has c3 = 0
+        double l = 0;
+        const double *hp = hphi + (size_t)(q * nbf + b) * 4;
+        double gm = 0;
+        if (!a.affine_all)
+          for (int r = 0; r < 2; r++)
+            gm += g[(q * dim + r) * nbf + b] * 0.25 * (V[r] - V[2 + r] + V[4 + r] - V[6 + r]);
         for (int r = 0; r < 2; r++)
-          gm += g[(q * nbf + b) * dim + r] * 0.25 * (V[r] - V[2 + r] + V[4 + r] - V[6 + r]);
-      for (int r = 0; r < 2; r++)
-        for (int e = 0; e < 2; e++)
-          for (int f = 0; f < 2; f++) l += Ji[e * 2 + r] * Ji[f * 2 + r] * (hp[e * 2 + f] - (e != f ? gm : 0.0));
+          for (int e = 0; e < 2; e++)
+            for (int f = 0; f < 2; f++) l += Ji[e * 2 + r] * Ji[f * 2 + r] * (hp[e * 2 + f] - (e != f ? gm : 0.0));
+        lap[q * nbf + b] = l;
+      }
     }
-    lap[q * nbf + b] = l;
-  }
-  __syncthreads();
-  double *out = a.out + (size_t)c * (nbf * nbf + nbf);
-  for (int t = threadIdx.x; t < nbf * nbf + nbf; t += blockDim.x)
-  {
-    bool is_rhs = t >= nbf * nbf;
-    int i = is_rhs ? t - nbf * nbf : t / nbf, j = is_rhs ? 0 : t % nbf;
-    double acc = 0;
-    for (int q = 0; q < nq; q++)
+    __syncthreads();
+    double *out = a.out + (size_t)c * (nbf * nbf + nbf);
+    if (nbf == 27 && blockDim.x >= 256)
     {
-      const double *k6 = kq + q * 6;
-      double c0 = k6[0], c1 = k6[1], c2 = k6[2], c3 = dim == 3 ? k6[3] : 0.0, cr = k6[4], f = k6[5];
-      const double *gi = g + (q * nbf + i) * dim;
-      double phi_i = a.phi[q * nbf + i];
-      double bgradv = c1 * gi[0] + c2 * gi[1] + (dim == 3 ? c3 * gi[2] : 0.0);
-      double delta = dl[q];
-      if (is_rhs)
+      // Q2 hexahedra: 243 threads = 3 groups x 81; a group takes the Gauss points q = grp mod 3
+      // and a thread of it the 3 x 3 entries (ib + 9u, jb + 9v), so every value loaded from
+      // shared memory serves three entries; the three groups' partial sums are added in group
+      // order afterwards.  Threads 243..255 take the right-hand side.
+      const int t = threadIdx.x;
+      double acc[3][3];
+#pragma unroll
+      for (int u = 0; u < 3; u++)
+#pragma unroll
+        for (int v = 0; v < 3; v++) acc[u][v] = 0.0;
+      const int grp = t / 81, tt = t % 81, ib = tt / 9, jb = tt % 9;
+      if (t < 243)
       {
-        acc += a.disctype == CDGPU_SUPG ? mult[q] * (phi_i + delta * bgradv) * f : mult[q] * phi_i * f;
-        continue;
+        for (int q = grp; q < nq; q += 3)
+        {
+          const double *k6 = kq + q * 6;
+          const double c0 = k6[0], c1 = k6[1], c2 = k6[2], c3 = k6[3], cr = k6[4];
+          const double m = mult[q], delta = dl[q];
+          const double *g0 = g + (q * 3) * 27, *g1 = g0 + 27, *g2 = g1 + 27, *ph = phi + q * 27;
+          double gi[3][3], pi[3], bi[3], gj[3][3], pj[3], bj[3];
+#pragma unroll
+          for (int u = 0; u < 3; u++)
+          {
+            const int i = ib + 9 * u, j = jb + 9 * u;
+            gi[u][0] = g0[i]; gi[u][1] = g1[i]; gi[u][2] = g2[i]; pi[u] = ph[i];
+            gj[u][0] = g0[j]; gj[u][1] = g1[j]; gj[u][2] = g2[j]; pj[u] = ph[j];
+            bi[u] = c1 * gi[u][0] + c2 * gi[u][1] + c3 * gi[u][2];
+            bj[u] = c1 * gj[u][0] + c2 * gj[u][1] + c3 * gj[u][2];
+          }
+#pragma unroll
+          for (int u = 0; u < 3; u++)
+#pragma unroll
+            for (int v = 0; v < 3; v++)
+            {
+              double val;
+              if (a.disctype == CDGPU_MASS)
+                val = pj[v] * pi[u]; // MatrixMRhsAssemble, ConvDiff2D.C:411
+              else
+              {
+                val = c0 * (gi[u][0] * gj[v][0] + gi[u][1] * gj[v][1] + gi[u][2] * gj[v][2]);
+                val += bj[v] * pi[u];
+                val += cr * pj[v] * pi[u];
+                if (a.disctype == CDGPU_SUPG) val += delta * (bj[v] + cr * pj[v]) * bi[u];
+              }
+              acc[u][v] += val * m;
+            }
+        }
       }
-      const double *gj = g + (q * nbf + j) * dim;
-      double phi_j = a.phi[q * nbf + j];
-      if (a.disctype == CDGPU_MASS)
+      else
       {
-        acc += mult[q] * phi_j * phi_i; // MatrixMRhsAssemble, ConvDiff2D.C:411
-        continue;
+        // right-hand side rows i = t - 243 + 13 r
+        for (int r = 0; r < 3; r++)
+        {
+          const int i = t - 243 + 13 * r;
+          if (i >= 27) break;
+          double sum = 0;
+          for (int q = 0; q < nq; q++)
+          {
+            const double *k6 = kq + q * 6;
+            const double *gq = g + (q * 3) * 27;
+            const double phi_i = phi[q * 27 + i];
+            const double bgradv = k6[1] * gq[i] + k6[2] * gq[27 + i] + k6[3] * gq[54 + i];
+            sum += a.disctype == CDGPU_SUPG ? mult[q] * (phi_i + dl[q] * bgradv) * k6[5] : mult[q] * phi_i * k6[5];
+          }
+          out[729 + i] = sum;
+        }
       }
-      double val = c0 * (gi[0] * gj[0] + gi[1] * gj[1] + (dim == 3 ? gi[2] * gj[2] : 0.0));
-      double bg = c1 * gj[0] + c2 * gj[1] + (dim == 3 ? c3 * gj[2] : 0.0);
-      val += bg * phi_i;
-      val += cr * phi_j * phi_i;
-      if (a.disctype == CDGPU_SUPG)
-      {
-        if (dim == 2)
-          val += delta * (-c0 * lap[q * nbf + j] + bg + cr * phi_j) * bgradv;
-        else
-          val += delta * (bg + cr * phi_j) * bgradv;
-      }
-      val *= mult[q];
-      acc += val;
+      // the gradients are no longer needed: their space takes groups 1 and 2's partial sums
+      __syncthreads();
+      if (t >= 81 && t < 243)
+#pragma unroll
+        for (int u = 0; u < 3; u++)
+#pragma unroll
+          for (int v = 0; v < 3; v++) g[(grp - 1) * 729 + (ib + 9 * u) * 27 + jb + 9 * v] = acc[u][v];
+      __syncthreads();
+      if (t < 81)
+#pragma unroll
+        for (int u = 0; u < 3; u++)
+#pragma unroll
+          for (int v = 0; v < 3; v++)
+          {
+            const int e = (ib + 9 * u) * 27 + jb + 9 * v;
+            out[e] = (acc[u][v] + g[e]) + g[729 + e];
+          }
     }
-    out[t] = acc;
+    else
+      for (int t = threadIdx.x; t < nbf * nbf + nbf; t += blockDim.x)
+      {
+        bool is_rhs = t >= nbf * nbf;
+        int i = is_rhs ? t - nbf * nbf : t / nbf, j = is_rhs ? 0 : t % nbf;
+        double acc = 0;
+        for (int q = 0; q < nq; q++)
+        {
+          const double *k6 = kq + q * 6;
+          double c0 = k6[0], c1 = k6[1], c2 = k6[2], c3 = dim == 3 ? k6[3] : 0.0, cr = k6[4], f = k6[5];
+          const double *gq = g + q * dim * nbf;
+          const double gi0 = gq[i], gi1 = gq[nbf + i], gi2 = dim == 3 ? gq[2 * nbf + i] : 0.0;
+          double phi_i = phi[q * nbf + i];
+          double bgradv = c1 * gi0 + c2 * gi1 + (dim == 3 ? c3 * gi2 : 0.0);
+          double delta = dl[q];
+          if (is_rhs)
+          {
+            acc += a.disctype == CDGPU_SUPG ? mult[q] * (phi_i + delta * bgradv) * f : mult[q] * phi_i * f;
+            continue;
+          }
+          const double gj0 = gq[j], gj1 = gq[nbf + j], gj2 = dim == 3 ? gq[2 * nbf + j] : 0.0;
+          double phi_j = phi[q * nbf + j];
+          if (a.disctype == CDGPU_MASS)
+          {
+            acc += mult[q] * phi_j * phi_i; // MatrixMRhsAssemble, ConvDiff2D.C:411
+            continue;
+          }
+          double val = c0 * (gi0 * gj0 + gi1 * gj1 + (dim == 3 ? gi2 * gj2 : 0.0));
+          double bg = c1 * gj0 + c2 * gj1 + (dim == 3 ? c3 * gj2 : 0.0);
+          val += bg * phi_i;
+          val += cr * phi_j * phi_i;
+          if (a.disctype == CDGPU_SUPG)
+          {
+            if (dim == 2)
+              val += delta * (-c0 * lap[q * nbf + j] + bg + cr * phi_j) * bgradv;
+            else
+              val += delta * (bg + cr * phi_j) * bgradv;
+          }
+          val *= mult[q];
+          acc += val;
+        }
+        out[t] = acc;
+      }
+    // every thread is done with this stage (its geometry and coefficients went into the
+    // shared arrays above): refill it with the cell after next
+    __syncthreads();
+    if (threadIdx.x == 0 && c + 2 * gridDim.x < a.n_cells)
+    {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(c + 2 * gridDim.x, st);
+      if (st) issued1++; else issued0++;
+    }
+  }
+  // copies still in flight (after a timeout, or never consumed): bounded waits before the
+  // CTA's shared memory is released
+  if (threadIdx.x == 0)
+  {
+    if (issued0 > waited0) (void)lq_wait(&bar[1], (uint32_t)(issued0 - 1) & 1u);
+    if (issued1 > waited1) (void)lq_wait(&bar[2], (uint32_t)(issued1 - 1) & 1u);
   }
 }
 
@@ -635,6 +844,7 @@ int err_flag_status(cdgpu_ctx *ctx)
     if (e == 1) return fail(ctx, CDGPU_ERR_PATTERN, "assemble: a cell coupling is missing from the CSR pattern");
     if (e == 3) return fail(ctx, CDGPU_ERR_CUDA, "multigrid: a tensor-core product did not complete in time");
     if (e == 4) return fail(ctx, CDGPU_ERR_CUDA, "CSR product: a bulk copy of a matrix tile did not complete in time");
+    if (e == 5) return fail(ctx, CDGPU_ERR_CUDA, "assemble: a bulk copy of cell data or tables did not complete in time");
     return fail(ctx, CDGPU_ERR_UNSUPPORTED, "assemble: CSR row longer than the kernel's row buffer");
   }
   return CDGPU_OK;
@@ -651,6 +861,8 @@ static int ensure_quadtab(cdgpu_ctx *ctx, Space &s)
   packed.insert(packed.end(), re.phi.begin(), re.phi.end());
   packed.insert(packed.end(), re.dphi.begin(), re.dphi.end());
   packed.insert(packed.end(), re.hphi.begin(), re.hphi.end());
+  // two spare doubles: the bulk copy of the tables rounds its size up to 16 bytes
+  packed.resize(packed.size() + 2, 0.0);
   int rc = dev_alloc(ctx, &s.d_quadtab, packed.size());
   if (rc) return rc;
   CD_CUDA(ctx, cudaMemcpy(s.d_quadtab, packed.data(), packed.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -932,12 +1144,22 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, 
     LocalArgs a;
     a.dim = s.dim; a.nv = s.nv; a.nbf = s.nbf; a.nq = re.nq; a.n_cells = s.n_cells;
     a.disctype = disctype; a.affine_all = s.all_affine; a.co = co; a.coords = s.d_coords; a.tab = d_tab;
-    a.qx = s.d_quadtab; a.qw = a.qx + re.qx.size(); a.phi = a.qw + re.qw.size();
-    a.dphi = a.phi + re.phi.size(); a.hphi = a.dphi + re.dphi.size(); a.out = s.d_local;
-    size_t sm = sizeof(double) * ((size_t)re.nq * s.nbf * s.dim + (size_t)re.nq * s.nbf + re.nq * 8 +
-                                  (size_t)re.nq * s.dim * s.dim);
+    a.qtab = s.d_quadtab;
+    a.n_qx = (int)re.qx.size(); a.n_qw = (int)re.qw.size(); a.n_phi = (int)re.phi.size();
+    a.n_dphi = (int)re.dphi.size();
+    // the staged tables: the second derivatives only where 2D SUPG reads them
+    a.n_stage_tab = a.n_qx + a.n_qw + a.n_phi + a.n_dphi +
+                    (s.dim == 2 && disctype == CDGPU_SUPG ? (int)re.hphi.size() : 0);
+    a.out = s.d_local;
+    a.err = ctx->d_err;
+    const LqLayout lay(s.dim, s.nv, s.nbf, re.nq, disctype, a.n_stage_tab, d_tab != nullptr);
+    const size_t sm = sizeof(double) * (size_t)lay.total;
+    if (sm > 227 * 1024) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "assemble: quadrature tables exceed shared memory");
     CD_CUDA(ctx, cudaFuncSetAttribute(local_quad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    local_quad_kernel<<<s.n_cells, 256, sm, ctx->stream>>>(a);
+    int per_sm = 0;
+    CD_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, local_quad_kernel, 256, sm));
+    const int grid = std::max(1, std::min(s.n_cells, ctx->sm_count * std::max(1, per_sm)));
+    (void)cd_launch(local_quad_kernel, grid, 256, sm, ctx->stream, a);
     CD_LAUNCHED(ctx);
   }
   if ((rc = ensure_slot_map(ctx, s))) return rc;
