@@ -352,10 +352,12 @@ int cdgpu_batch_submit_tcd(cdgpu_ctx *ctx, int batch_id, int mg_id, const cdgpu_
                            const double *h_u0, int *slot);
 /* one time step of every time-dependent instance of the batch: right-hand side
  * tau*theta3*f_old + tau*theta4*f + K u_old, then FGMRES from u_old to the batch's stopping
- * rule.  The right-hand sides and the first `iterations` FGMRES iterations are one CUDA graph
- * (captured on the first step, replayed while the batch's instances are unchanged); solves
- * that need more continue in rounds of `iterations`.  *max_iterations (nullable) = the
- * iterations the slowest instance was given. */
+ * rule.  The step is one CUDA graph (captured on the first step, replayed while the batch's
+ * instances are unchanged): the right-hand sides, then the device-side iteration loop of
+ * cdgpu_batch_advance until every solve has finished (at most maxit + 1 iterations).  A
+ * driver without conditional graph nodes gets a graph of the right-hand sides and `iterations`
+ * FGMRES iterations, and solves that need more continue in rounds of `iterations`.
+ * *max_iterations (nullable) = the iterations the slowest instance was given. */
 int cdgpu_batch_tcd_step(cdgpu_ctx *ctx, int batch_id, int iterations, int *max_iterations);
 /* current solution of a time-dependent instance (same as cdgpu_batch_fetch) */
 int cdgpu_batch_tcd_solution(cdgpu_ctx *ctx, int batch_id, int slot, double *h_sol, cdgpu_solve_info *info);

@@ -113,6 +113,7 @@ struct Batch
   BTab tcd_csr, tcd_items; // every time-dependent instance, running or idle
   cudaGraphExec_t tcd_graph = nullptr;
   int tcd_graph_k = 0;
+  bool tcd_looped = false; // tcd_graph ends in the device-side iteration loop
   // the device-side iteration loop: one graph whose WHILE node runs FGMRES iterations of the
   // running set until every solve has finished or the call's iteration budget is spent
   cudaGraphExec_t loop_graph = nullptr;
@@ -1278,15 +1279,17 @@ static int assemble_to(cdgpu_ctx *ctx, Space &s, int disctype, const cdgpu_coeff
 // sets the condition again.  Captured once per running set.  A driver that refuses the
 // body's programmatic dependencies gets the body without them; one that refuses conditional
 // nodes leaves the host loop (loop_mode 0).  Only API calls can fail here: nothing runs.
-static int build_loop_graph(cdgpu_ctx *ctx, Batch &b, bool pdl)
+static int build_loop_graph(cdgpu_ctx *ctx, Batch &b, bool pdl, cudaGraph_t prefix, cudaGraphExec_t *out)
 {
   int rc;
   if (!b.d_loop && (rc = dev_alloc(ctx, &b.d_loop, 1))) return rc;
   cudaGraph_t g = nullptr;
   cudaGraphConditionalHandle cond;
-  cudaGraphNode_t init = nullptr, wnode = nullptr;
+  cudaGraphNode_t pre = nullptr, init = nullptr, wnode = nullptr;
   cudaError_t e = cudaGraphCreate(&g, 0);
   if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&cond, g, 0, 0);
+  // work that runs once before the loop (a child graph)
+  if (e == cudaSuccess && prefix) e = cudaGraphAddChildGraphNode(&pre, g, nullptr, 0, prefix);
   if (e == cudaSuccess)
   {
     cudaKernelNodeParams kp = {};
@@ -1299,7 +1302,7 @@ static int build_loop_graph(cdgpu_ctx *ctx, Batch &b, bool pdl)
     kp.gridDim = dim3(1);
     kp.blockDim = dim3(256);
     kp.kernelParams = args;
-    e = cudaGraphAddKernelNode(&init, g, nullptr, 0, &kp);
+    e = cudaGraphAddKernelNode(&init, g, pre ? &pre : nullptr, pre ? 1 : 0, &kp);
   }
   cudaGraph_t body = nullptr;
   if (e == cudaSuccess)
@@ -1337,13 +1340,16 @@ static int build_loop_graph(cdgpu_ctx *ctx, Batch &b, bool pdl)
   }
   cd_pdl_enabled() = pdl_was;
   ctx->launches = before;
-  if (e == cudaSuccess && !rc) e = cudaGraphInstantiate(&b.loop_graph, g, 0);
+  *out = nullptr;
+  if (e == cudaSuccess && !rc) e = cudaGraphInstantiate(out, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess || rc)
   {
-    b.loop_graph = nullptr;
+    // a launch or capture refused inside the body (the driver's rules for conditional
+    // bodies): nothing ran; the caller tries the next form
+    *out = nullptr;
     cudaGetLastError();
-    return rc ? rc : CDGPU_ERR_UNSUPPORTED;
+    return CDGPU_ERR_UNSUPPORTED;
   }
   return CDGPU_OK;
 }
@@ -1446,7 +1452,7 @@ int cdgpu_batch_advance(cdgpu_ctx *ctx, int batch_id, int iterations, int *runni
       const int first = b.loop_mode < 0 ? 1 : b.loop_mode;
       for (int mode = first; mode <= 2 && !b.loop_graph; mode++)
       {
-        rc = build_loop_graph(ctx, b, mode == 1);
+        rc = build_loop_graph(ctx, b, mode == 1, nullptr, &b.loop_graph);
         if (rc && rc != CDGPU_ERR_UNSUPPORTED) return rc;
         if (!rc) b.loop_mode = mode;
       }
@@ -1508,8 +1514,12 @@ int cdgpu_batch_tcd_step(cdgpu_ctx *ctx, int batch_id, int iterations, int *max_
   for (auto &in : b.inst)
     if (in.used && in.tcd) in.state = ST_RUN;
   // the step -- right-hand sides, restart of every time-dependent solve from its previous
-  // solution, `iterations` FGMRES iterations of everything running -- is one CUDA graph,
-  // captured on first use and replayed for every step while the instance set is unchanged
+  // solution, FGMRES iterations of everything running -- is one CUDA graph, captured on first
+  // use and replayed for every step while the instance set is unchanged.  Where the driver
+  // takes conditional nodes the iterations are the device-side loop (until every solve has
+  // finished, at most maxit + 1 iterations); otherwise the graph holds `iterations` of them
+  // and solves that need more continue in rounds of `iterations` from the host.
+  const int budget = b.p.maxit + 1;
   if (!b.tcd_graph || b.tcd_graph_k != iterations)
   {
     if (b.tcd_graph) { cudaGraphExecDestroy(b.tcd_graph); b.tcd_graph = nullptr; }
@@ -1522,28 +1532,71 @@ int cdgpu_batch_tcd_step(cdgpu_ctx *ctx, int batch_id, int iterations, int *max_
     }
     if (sm > 48 * 1024)
       CD_CUDA(ctx, cudaFuncSetAttribute(b_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    if (!b.d_loop && (rc = dev_alloc(ctx, &b.d_loop, 1))) return rc;
     const long long before = ctx->launches;
-    CD_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    (void)cd_launch(b_tcd_rhs, std::max(1, std::min(b.tcd_csr.total, ctx->sm_count * 8)), kNT, 0, ctx->stream, b.tcd_csr, b.d_ctl);
-    rc = cudaGetLastError() == cudaSuccess ? CDGPU_OK : CDGPU_ERR_CUDA;
-    if (!rc)
+    bool looped = false;
+    if (b.loop_mode != 0)
     {
-      (void)cd_launch(b_tcd_begin, 1, 256, 0, ctx->stream, b.tcd_items, b.d_ctl);
-      for (int it = 0; it < iterations && !rc; it++) rc = batch_iteration(ctx, b);
+      const int first = b.loop_mode < 0 ? 1 : b.loop_mode;
+      for (int mode = first; mode <= 2 && !looped; mode++)
+      {
+        // the work before the loop, as a child graph (without programmatic dependencies in
+        // the form that leaves them out of the loop body too)
+        cudaGraph_t pg = nullptr;
+        const bool pdl_was = cd_pdl_enabled();
+        cd_pdl_enabled() = mode == 1;
+        cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess)
+        {
+          (void)cd_launch(b_tcd_rhs, std::max(1, std::min(b.tcd_csr.total, ctx->sm_count * 8)), kNT, 0, ctx->stream,
+                          b.tcd_csr, b.d_ctl);
+          (void)cd_launch(b_tcd_begin, 1, 256, 0, ctx->stream, b.tcd_items, b.d_ctl);
+          (void)cd_launch(b_loop_budget, 1, 1, 0, ctx->stream, b.d_loop, budget);
+          e = cudaGetLastError();
+          cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &pg);
+          if (e == cudaSuccess) e = e2;
+        }
+        cd_pdl_enabled() = pdl_was;
+        if (e != cudaSuccess)
+        {
+          if (pg) cudaGraphDestroy(pg);
+          return cuda_fail(ctx, e, "capture of the time step's right-hand sides");
+        }
+        rc = build_loop_graph(ctx, b, mode == 1, pg, &b.tcd_graph);
+        cudaGraphDestroy(pg);
+        if (rc && rc != CDGPU_ERR_UNSUPPORTED) return rc;
+        if (!rc) { looped = true; b.loop_mode = mode; }
+      }
+      if (!looped && b.loop_mode < 0) b.loop_mode = 0;
     }
-    cudaGraph_t g = nullptr;
-    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (!looped)
+    {
+      CD_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      (void)cd_launch(b_tcd_rhs, std::max(1, std::min(b.tcd_csr.total, ctx->sm_count * 8)), kNT, 0, ctx->stream, b.tcd_csr,
+                      b.d_ctl);
+      rc = cudaGetLastError() == cudaSuccess ? CDGPU_OK : CDGPU_ERR_CUDA;
+      if (!rc)
+      {
+        (void)cd_launch(b_tcd_begin, 1, 256, 0, ctx->stream, b.tcd_items, b.d_ctl);
+        for (int it = 0; it < iterations && !rc; it++) rc = batch_iteration(ctx, b);
+      }
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+      ctx->launches = before;
+      if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "capture of the time step");
+      e = cudaGraphInstantiate(&b.tcd_graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) { b.tcd_graph = nullptr; return cuda_fail(ctx, e, "graph instantiate"); }
+    }
     ctx->launches = before;
-    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture of the time step");
-    e = cudaGraphInstantiate(&b.tcd_graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) { b.tcd_graph = nullptr; return cuda_fail(ctx, e, "graph instantiate"); }
     b.tcd_graph_k = iterations;
+    b.tcd_looped = looped;
   }
   CD_CUDA(ctx, cudaGraphLaunch(b.tcd_graph, ctx->stream));
+  if (b.tcd_looped) b.loop_launches++;
   // solves that need more iterations continue outside the graph
-  int r = 1, rounds = 0;
+  int r = 1, rounds = 0, extra = 0;
   while (true)
   {
     CD_CUDA(ctx, cudaMemcpyAsync(b.h_state, b.d_state, sizeof(int) * b.cap, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1561,10 +1614,24 @@ int cdgpu_batch_tcd_step(cdgpu_ctx *ctx, int batch_id, int iterations, int *max_
     }
     if (r == 0) break;
     for (int it = 0; it < iterations; it++)
+    {
       if ((rc = batch_iteration(ctx, b))) return rc;
+      b.host_iterations++;
+    }
+    extra += iterations;
     rounds++;
   }
-  if (max_iterations) *max_iterations = iterations * (rounds + 1);
+  if (max_iterations)
+  {
+    if (b.tcd_looped)
+    {
+      int left = 0;
+      CD_CUDA(ctx, cudaMemcpy(&left, b.d_loop, sizeof(int), cudaMemcpyDeviceToHost));
+      *max_iterations = (budget - std::max(0, left)) + extra;
+    }
+    else
+      *max_iterations = iterations * (rounds + 1);
+  }
   return CDGPU_OK;
 }
 
