@@ -334,6 +334,10 @@ struct LqLayout
   }
 };
 
+// Q27: Q2 hexahedra (27 local DOFs) with the register-tiled entry phase; the other elements
+// take the one-entry-per-thread loop in an instance of their own, so that its register count
+// (and with it the resident CTAs per SM) is not the tiled phase's
+template <bool Q27>
 __global__ void __launch_bounds__(256) local_quad_kernel(LocalArgs a)
 {
   CD_PDL_ENTRY();
@@ -431,7 +435,7 @@ __global__ void __launch_bounds__(256) local_quad_kernel(LocalArgs a)
     }
     __syncthreads();
     double *out = a.out + (size_t)c * (nbf * nbf + nbf);
-    if (nbf == 27 && blockDim.x >= 256)
+    if constexpr (Q27)
     {
       // Q2 hexahedra: 243 threads = 3 groups x 81; a group takes the Gauss points q = grp mod 3
       // and a thread of it the 3 x 3 entries (ib + 9u, jb + 9v), so every value loaded from
@@ -1155,11 +1159,12 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, 
     const LqLayout lay(s.dim, s.nv, s.nbf, re.nq, disctype, a.n_stage_tab, d_tab != nullptr);
     const size_t sm = sizeof(double) * (size_t)lay.total;
     if (sm > 227 * 1024) return fail(ctx, CDGPU_ERR_UNSUPPORTED, "assemble: quadrature tables exceed shared memory");
-    CD_CUDA(ctx, cudaFuncSetAttribute(local_quad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    auto kern = s.nbf == 27 ? local_quad_kernel<true> : local_quad_kernel<false>;
+    CD_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     int per_sm = 0;
-    CD_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, local_quad_kernel, 256, sm));
+    CD_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, sm));
     const int grid = std::max(1, std::min(s.n_cells, ctx->sm_count * std::max(1, per_sm)));
-    (void)cd_launch(local_quad_kernel, grid, 256, sm, ctx->stream, a);
+    (void)cd_launch(kern, grid, 256, sm, ctx->stream, a);
     CD_LAUNCHED(ctx);
   }
   if ((rc = ensure_slot_map(ctx, s))) return rc;
