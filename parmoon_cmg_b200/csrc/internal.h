@@ -149,6 +149,7 @@ struct Hierarchy
   // captured multigrid cycle per precision (0 FP64, 1 FP32) and its in/out pointer slot
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   unsigned mf_mask = 0; // levels whose FP32 cycle in gexec[1] uses the matrix-free operator
+  int cl_top = -1;      // FP32 V-cycle: levels 0..cl_top on one thread-block cluster (-1 none)
   cdgpu_solver_params gparams[2] = {};
   long long graph_nodes[2] = {0, 0};
   double **d_io = nullptr;
@@ -186,6 +187,7 @@ struct cdgpu_ctx
   // set while the multigrid cycle is recorded into its graph: its kernels load the data that
   // no kernel of the cycle writes before waiting for their predecessor
   bool pdl_pre = false;
+  int cluster_size = -1; // thread-block cluster size of the FP32 coarse cycle (-1 not probed, 0 none)
   int *d_err = nullptr; // assembly error flag (device) and its pinned host mirror
   int *h_err = nullptr;
 };

@@ -29,6 +29,7 @@
 #include "internal.h"
 #include "csr.cuh"
 #include "mf.cuh"
+#include "mgcluster.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -701,8 +702,130 @@ template <typename T> static int coarse_solve(cdgpu_ctx *ctx, Hierarchy &h, Cycl
   return CDGPU_OK;
 }
 
+// the highest level that, with every level below it, runs on one thread-block cluster in the
+// FP32 V-cycle (-1: none); fixed per hierarchy
+static int cluster_top(const Hierarchy &h)
+{
+  int top = -1;
+  // never the finest level: its cycle starts in mg_start_first_kernel
+  for (int l = 0; l + 1 < (int)h.lev.size() && l < kClusterMaxLevels; l++)
+  {
+    if (h.lev[l].sp->n_dof > kClusterMaxRows || use_mf(*h.lev[l].sp)) break;
+    top = l;
+  }
+  return top >= 1 ? top : -1;
+}
+
+// cluster size for mg_cluster_kernel on this device (16, else 8, 0 = none), found once outside
+// any capture; the kernel's attributes are set on the way
+static int cluster_size(cdgpu_ctx *ctx, size_t smem)
+{
+  if (ctx->cluster_size >= 0) return ctx->cluster_size;
+  ctx->cluster_size = 0;
+  if (cudaFuncSetAttribute(mg_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
+      cudaFuncSetAttribute(mg_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 48 * 1024) != cudaSuccess)
+  {
+    cudaGetLastError();
+    return 0;
+  }
+  for (int cs : {16, 8})
+  {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(kClusterThreads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, mg_cluster_kernel, &cfg) == cudaSuccess && n >= 1)
+    {
+      ctx->cluster_size = cs;
+      break;
+    }
+    cudaGetLastError();
+  }
+  return ctx->cluster_size;
+}
+
+// levels 0 .. i of an FP32 V-cycle as one cluster launch (mgcluster.cuh); false when the
+// cycle or the device does not take it (the per-level launches run instead)
+static bool cycle_on_cluster(cdgpu_ctx *ctx, Hierarchy &h, CycleState &cs, int i)
+{
+  const cdgpu_solver_params &p = *cs.p;
+  if (i != h.cl_top || p.cycle != 1 || p.coarse_smoother != 17 || !cs.active_zero[i] || !cs.sol_zero[i] ||
+      cs.pre_done[i] != 0 || ctx->cluster_size <= 0)
+    return false;
+  ClusterCycle c;
+  c.nl = i + 1;
+  c.pre = p.pre;
+  c.post = p.post;
+  c.omega = (float)p.omega;
+  c.damp = (float)p.gmg_damp;
+  c.a64 = h.lev[0].sp->d_a;
+  c.cinv = h.d_cinv;
+  for (int l = 0; l <= i; l++)
+  {
+    Level &L = h.lev[l];
+    const Space &sp = *L.sp;
+    LevelVec<float> &v = L.v32;
+    ClusterLevel &q = c.lev[l];
+    q.n = sp.n_dof;
+    q.na = sp.n_active;
+    q.rp = sp.d_row_ptr;
+    q.kc = sp.d_kcol;
+    q.dir_start = sp.d_dir_start;
+    q.a = sp.d_a32;
+    q.diag = sp.d_diag32;
+    q.sol = v.sol;
+    q.alt = v.alt;
+    q.rhs = v.rhs;
+    q.def = v.def;
+    if (l > 0)
+    {
+      q.r_rp = L.d_r_row; q.r_kc = L.d_r_col; q.r_val = L.d_r_val32;
+      q.p_rp = L.d_p_row; q.p_kc = L.d_p_col; q.p_val = L.d_p_val32;
+    }
+  }
+  const Space &s0 = *h.lev[0].sp;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ctx->cluster_size);
+  cfg.blockDim = dim3(kClusterThreads);
+  cfg.dynamicSmemBytes = sizeof(double) * (s0.n_dof + s0.n_active);
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[2];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = ctx->cluster_size;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = cd_pdl_enabled() ? 2 : 1;
+  if (cudaLaunchKernelEx(&cfg, mg_cluster_kernel, c) != cudaSuccess)
+  {
+    cudaGetLastError();
+    return false;
+  }
+  // the sweeps swapped every level's working pointers inside the kernel: the same here
+  for (int l = 1; l <= i; l++)
+    if ((p.pre + p.post) & 1) std::swap(h.lev[l].v32.sol, h.lev[l].v32.alt);
+  for (int l = 0; l <= i; l++) cs.sol_zero[l] = cs.active_zero[l] = false;
+  return true;
+}
+
 template <typename T> static int cycle(cdgpu_ctx *ctx, Hierarchy &h, CycleState &cs, int i)
 {
+  if constexpr (std::is_same<T, float>::value)
+    if (cycle_on_cluster(ctx, h, cs, i))
+    {
+      ctx->launches++;
+      return CDGPU_OK;
+    }
   if (i == 0) return coarse_solve<T>(ctx, h, cs);
   Level &L = h.lev[i], &C = h.lev[i - 1];
   const Space &s = *L.sp, &sc = *C.sp;
@@ -804,6 +927,9 @@ static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, 
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_exact_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm1));
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_smooth_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm2));
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_smooth_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm2));
+    h.cl_top = k == 1 ? cluster_top(h) : -1;
+    if (h.cl_top >= 1 && sm1 <= 48 * 1024) (void)cluster_size(ctx, (size_t)sm1);
+    else h.cl_top = -1;
     cudaGraph_t g = nullptr;
     const long long before = ctx->launches;
     CD_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
