@@ -19,6 +19,10 @@
 constexpr int kClusterMaxLevels = 4;
 constexpr int kClusterMaxRows = 8192; // levels with at most this many rows go to the cluster
 constexpr int kClusterThreads = 1024;
+// off: with the vectors and matrices read from L2 in every step the cluster launch took
+// ~127 us per V-cycle against ~85 us for the per-level launches on all SMs (170.6 against
+// 194.1 solves/s)
+constexpr bool kClusterCycleOn = false;
 
 struct ClusterLevel
 {
@@ -42,12 +46,29 @@ struct ClusterCycle
   const double *a64 = nullptr, *cinv = nullptr;
 };
 
-// sum of a row of A times x over entries [jb, je), 4 threads per row (lane4 = 0..3)
+// sum of a row of A times x over entries [jb, je), 4 threads per row (lane4 = 0..3): in rounds
+// of 32 entries, each thread issues its 8 column and value loads, then its 8 gathers of x,
+// before the first product, so a round costs two L2 latencies whatever its length
 __device__ __forceinline__ float cl_row(const int *__restrict__ kc, const float *__restrict__ a,
                                         const float *x, int jb, int je, int lane4)
 {
   float s = 0.f;
-  for (int j = jb + lane4; j < je; j += 4) s += __ldg(a + j) * __ldcg(x + __ldg(kc + j));
+  for (int j0 = jb + lane4; j0 < je; j0 += 32)
+  {
+    int c[8];
+    float v[8], xv[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++)
+    {
+      const int j = j0 + 4 * u;
+      c[u] = j < je ? __ldg(kc + j) : -1;
+      v[u] = j < je ? __ldg(a + j) : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) xv[u] = c[u] >= 0 ? __ldcg(x + c[u]) : 0.f;
+#pragma unroll
+    for (int u = 0; u < 8; u++) s += v[u] * xv[u];
+  }
   s += __shfl_xor_sync(0xffffffffu, s, 1, 4);
   s += __shfl_xor_sync(0xffffffffu, s, 2, 4);
   return s;

@@ -927,7 +927,7 @@ static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, 
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_exact_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm1));
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_smooth_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm2));
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_smooth_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm2));
-    h.cl_top = k == 1 ? cluster_top(h) : -1;
+    h.cl_top = k == 1 && kClusterCycleOn ? cluster_top(h) : -1;
     if (h.cl_top >= 1 && sm1 <= 48 * 1024) (void)cluster_size(ctx, (size_t)sm1);
     else h.cl_top = -1;
     cudaGraph_t g = nullptr;
