@@ -508,9 +508,11 @@ int cdgpu_cycle_report(cdgpu_ctx *ctx, int mg_id, char *buf, int len)
   const Hierarchy &h = *ctx->mgs[mg_id];
   if (!h.gexec[1])
     snprintf(buf, len, "no FP32 cycle recorded yet");
-  else if (h.cl_top >= 1 && ctx->cluster_size > 0)
-    snprintf(buf, len, "levels 0..%d (%d..%d rows) in one launch on a %d-CTA thread-block cluster", h.cl_top,
-             h.lev[0].sp->n_dof, h.lev[h.cl_top].sp->n_dof, ctx->cluster_size);
+  else if (h.cl_top >= 1)
+    snprintf(buf, len,
+             "levels 0..%d (%d..%d rows) in one launch on a %d-CTA thread-block cluster, %zu bytes of shared "
+             "memory per CTA",
+             h.cl_top, h.lev[0].sp->n_dof, h.lev[h.cl_top].sp->n_dof, kClusterCtas, h.cl_smem);
   else
     snprintf(buf, len, "every level in its own launches");
   return CDGPU_OK;
