@@ -393,7 +393,6 @@ def run_ours(args, rank, world, local):
     spmv_ms = e0.elapsed_time(e1) / reps
     spmv_bytes = 12 * nnz + 4 * (n + 1) + 16 * n
     tuning = ctx.product_tuning(sids[-1])
-    fp32_cycle = ctx.cycle_report(mg)
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
         hbm = json.load(open(peaks_path))["hbm_gbs"]
@@ -444,7 +443,7 @@ def run_ours(args, rank, world, local):
                         f"+ FGMRES(30) with one V(2,2) damped-Jacobi (0.8) cycle to ||r|| <= 1e-10 ||r0||",
             "form": "mixed (FP32 multigrid, FP64 FGMRES, FP64 defect, FP64 exact coarse solve)",
             "multigrid": f"{args.levels} levels {n0}^3..{args.n}^3 Q2, SUPG coarse-grid operators "
-                         f"(delta0 = 1/3), exact coarse solve; FP32 cycle: {fp32_cycle}",
+                         f"(delta0 = 1/3), exact coarse solve",
             "n_dof": n, "nnz_finest": nnz, "l2": "inputs larger than L2 (finest matrix 192 MB)",
             "parallelism": f"replicas x{world}",
         },

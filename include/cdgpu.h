@@ -210,10 +210,6 @@ int cdgpu_spmv_device(cdgpu_ctx *ctx, int space_id, const double *d_x, double *d
  * This copies a one-line report of that choice (or "not tuned yet") into buf.  No reference
  * counterpart (MatVect / Defect, src/FE/Blas2.C:11-99, are the operations). */
 int cdgpu_product_tuning(cdgpu_ctx *ctx, int space_id, char *buf, int len);
-/* how the FP32 multigrid cycle of a hierarchy runs (known after its first mixed-precision
- * solve), as text: which coarse levels run as one thread-block cluster launch and the cluster
- * size, or that every level runs as its own launches */
-int cdgpu_cycle_report(cdgpu_ctx *ctx, int mg_id, char *buf, int len);
 /* y = A x with an FP32 form of the assembled operator, the forms the mixed multigrid cycle
  * applies (TMGLevel3D's MatVect/Defect on the FP32 levels, src/FE/MGLevel3D.C:194-252):
  * form 0 the FP32 copy of the CSR entries; 1 the matrix-free per-cell products

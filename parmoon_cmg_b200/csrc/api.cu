@@ -501,23 +501,6 @@ int cdgpu_product_tuning(cdgpu_ctx *ctx, int space_id, char *buf, int len)
   return CDGPU_OK;
 }
 
-int cdgpu_cycle_report(cdgpu_ctx *ctx, int mg_id, char *buf, int len)
-{
-  if (!ctx || mg_id < 0 || mg_id >= (int)ctx->mgs.size() || !buf || len <= 0)
-    return fail(ctx, CDGPU_ERR_INVALID, "cycle_report: bad argument");
-  const Hierarchy &h = *ctx->mgs[mg_id];
-  if (!h.gexec[1])
-    snprintf(buf, len, "no FP32 cycle recorded yet");
-  else if (h.cl_top >= 1)
-    snprintf(buf, len,
-             "levels 0..%d (%d..%d rows) in one launch on a %d-CTA thread-block cluster, %zu bytes of shared "
-             "memory per CTA",
-             h.cl_top, h.lev[0].sp->n_dof, h.lev[h.cl_top].sp->n_dof, kClusterCtas, h.cl_smem);
-  else
-    snprintf(buf, len, "every level in its own launches");
-  return CDGPU_OK;
-}
-
 // Legacy-VTK output of a solution, in the form TOutput3D::WriteVtk / TOutput2D::WriteVtk write
 // it (src/FE/Output3D.C:1747-2010): ASCII UNSTRUCTURED_GRID, the mesh vertices as POINTS, one
 // hexahedron (type 12) or quadrilateral (type 9) per cell, the function's values at the vertices

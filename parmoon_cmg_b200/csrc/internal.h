@@ -134,47 +134,6 @@ struct Level
   LevelVec<float> v32, c32;
 };
 
-// the coarse end of the FP32 V-cycle on one thread-block cluster (mgcluster.cuh)
-constexpr int kClusterMaxLevels = 4;
-constexpr int kClusterMaxRows = 8192; // levels with at most this many rows go to the cluster
-constexpr int kClusterThreads = 1024;
-constexpr int kClusterCtas = 16;
-constexpr int kClusterSmem = 227 * 1024;
-
-struct ClusterLevel
-{
-  int n = 0, na = 0;
-  // rows [rb[k], rb[k+1]) of this level's A, [pb[k], pb[k+1]) of its active rows (P) and
-  // [cb[k], cb[k+1]) of the next coarser level (R) belong to CTA k: each split so that every
-  // CTA holds about the same number of entries
-  int rb[kClusterCtas + 1] = {}, pb[kClusterCtas + 1] = {}, cb[kClusterCtas + 1] = {};
-  const int *rp = nullptr, *kc = nullptr;
-  const float *a = nullptr, *diag = nullptr;
-  // restriction to the next coarser level (rows = coarser DOFs) and the prolongation from it
-  // (rows = this level's DOFs); unused on level 0
-  const int *r_rp = nullptr, *r_kc = nullptr, *p_rp = nullptr, *p_kc = nullptr;
-  const float *r_val = nullptr, *p_val = nullptr;
-  // byte offsets in shared memory: the CTA's rows of A (row pointers rebased to 0, 16-bit
-  // columns, values), its diagonal and right-hand side, the full iterate (two buffers) and
-  // defect, its rows of R and P
-  int o_rp = 0, o_kc = 0, o_a = 0, o_diag = 0, o_rhs = 0, o_x0 = 0, o_x1 = 0, o_def = 0;
-  int o_rrp = 0, o_rkc = 0, o_rval = 0, o_prp = 0, o_pkc = 0, o_pval = 0;
-};
-
-struct ClusterCycle
-{
-  int nl = 0; // levels 0 .. nl-1; nl-1 the top one, whose rhs the restriction above wrote
-  ClusterLevel lev[kClusterMaxLevels];
-  int pre = 2, post = 2;
-  float omega = 0.8f, damp = 1.0f;
-  const float *top_rhs = nullptr; // global rhs of the top level
-  float *top_out = nullptr;       // global buffer that receives the top level's final iterate
-  // level 0: exact solve with the FP64 matrix's Dirichlet columns and the explicit inverse
-  const int *dir_start0 = nullptr;
-  const double *a64 = nullptr, *cinv = nullptr;
-  int o_b = 0; // byte offset of the first CTA's (n0 + na0) doubles of coarse-solve scratch
-};
-
 struct Hierarchy
 {
   std::vector<Level> lev;
@@ -190,9 +149,6 @@ struct Hierarchy
   // captured multigrid cycle per precision (0 FP64, 1 FP32) and its in/out pointer slot
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   unsigned mf_mask = 0; // levels whose FP32 cycle in gexec[1] uses the matrix-free operator
-  int cl_top = -1;      // FP32 V-cycle: levels 0..cl_top on one thread-block cluster (-1 none)
-  ClusterCycle cl_plan;  // its shared-memory plan (mgcluster.cuh)
-  size_t cl_smem = 0;
   cdgpu_solver_params gparams[2] = {};
   long long graph_nodes[2] = {0, 0};
   double **d_io = nullptr;

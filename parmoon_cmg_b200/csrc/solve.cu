@@ -29,7 +29,6 @@
 #include "internal.h"
 #include "csr.cuh"
 #include "mf.cuh"
-#include "mgcluster.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -702,191 +701,8 @@ template <typename T> static int coarse_solve(cdgpu_ctx *ctx, Hierarchy &h, Cycl
   return CDGPU_OK;
 }
 
-// the highest level that, with every level below it, runs on one thread-block cluster in the
-// FP32 V-cycle (-1: none); never the finest level (its cycle starts in mg_start_first_kernel)
-static int cluster_top(const Hierarchy &h)
-{
-  int top = -1;
-  for (int l = 0; l + 1 < (int)h.lev.size() && l < kClusterMaxLevels; l++)
-  {
-    if (h.lev[l].sp->n_dof > kClusterMaxRows || use_mf(*h.lev[l].sp)) break;
-    top = l;
-  }
-  return top >= 1 ? top : -1;
-}
-
-// split rows [0, n) of a CSR matrix into kClusterCtas consecutive blocks of about equal
-// entries: b[k] = the first row whose entries start at or after k/kClusterCtas of all
-static void balanced_split(const std::vector<int> &rp, int n, int *b)
-{
-  const long nnz = rp[n];
-  int r = 0;
-  b[0] = 0;
-  for (int k = 1; k < kClusterCtas; k++)
-  {
-    const long target = nnz * k / kClusterCtas;
-    while (r < n && rp[r] < target) r++;
-    b[k] = r;
-  }
-  b[kClusterCtas] = n;
-}
-
-// largest rows and entries of one block of a split
-static void split_caps(const std::vector<int> &rp, const int *b, int &rows, int &ents)
-{
-  rows = ents = 0;
-  for (int k = 0; k < kClusterCtas; k++)
-  {
-    rows = std::max(rows, b[k + 1] - b[k]);
-    ents = std::max(ents, rp[b[k + 1]] - rp[b[k]]);
-  }
-}
-
-static int device_row_ptr(const int *d_rp, int n, std::vector<int> &h)
-{
-  h.resize((size_t)n + 1);
-  return cudaMemcpy(h.data(), d_rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : 1;
-}
-
-// The shared-memory plan of levels 0..top for mg_cluster_kernel (offsets of every CTA's
-// slices and copies, identical on every CTA, sized for the largest slice); false when it does
-// not fit or the device cannot run a 16-CTA cluster of it.  Set up once, outside any capture.
-static bool plan_cluster(cdgpu_ctx *ctx, Hierarchy &h, int top)
-{
-  ClusterCycle &c = h.cl_plan;
-  c = ClusterCycle();
-  c.nl = top + 1;
-  const int nb = kClusterCtas;
-  size_t off = 0;
-  auto take = [&](size_t bytes) {
-    const size_t o = off;
-    off += (bytes + 15) & ~(size_t)15;
-    return (int)o;
-  };
-  for (int l = 0; l <= top; l++)
-  {
-    Level &L = h.lev[l];
-    const Space &sp = *L.sp;
-    ClusterLevel &q = c.lev[l];
-    q.n = sp.n_dof;
-    q.na = sp.n_active;
-    q.rp = sp.d_row_ptr;
-    q.kc = sp.d_kcol;
-    q.a = sp.d_a32;
-    q.diag = sp.d_diag32;
-    if (q.n > 65535) return false; // 16-bit column indices
-    q.o_x0 = take(sizeof(float) * q.n);
-    if (l == 0) continue;
-    const int nc = h.lev[l - 1].sp->n_dof;
-    q.r_rp = L.d_r_row; q.r_kc = L.d_r_col; q.r_val = L.d_r_val32;
-    q.p_rp = L.d_p_row; q.p_kc = L.d_p_col; q.p_val = L.d_p_val32;
-    std::vector<int> rrp, prp;
-    if (device_row_ptr(L.d_r_row, nc, rrp) || device_row_ptr(L.d_p_row, q.n, prp)) { cudaGetLastError(); return false; }
-    balanced_split(sp.h_row_ptr, q.n, q.rb);
-    balanced_split(rrp, nc, q.cb);
-    balanced_split(prp, q.na, q.pb);
-    int rows, ents, crows, rents, prows, pents;
-    split_caps(sp.h_row_ptr, q.rb, rows, ents);
-    split_caps(rrp, q.cb, crows, rents);
-    split_caps(prp, q.pb, prows, pents);
-    q.o_x1 = take(sizeof(float) * q.n);
-    q.o_def = take(sizeof(float) * q.n);
-    q.o_rp = take(sizeof(int) * (rows + 1));
-    q.o_kc = take(sizeof(unsigned short) * ents);
-    q.o_a = take(sizeof(float) * ents);
-    q.o_diag = take(sizeof(float) * rows);
-    q.o_rhs = take(sizeof(float) * rows);
-    q.o_rrp = take(sizeof(int) * (crows + 1));
-    q.o_rkc = take(sizeof(unsigned short) * rents);
-    q.o_rval = take(sizeof(float) * rents);
-    q.o_prp = take(sizeof(int) * (prows + 1));
-    q.o_pkc = take(sizeof(unsigned short) * pents);
-    q.o_pval = take(sizeof(float) * pents);
-  }
-  const Space &s0 = *h.lev[0].sp;
-  c.o_b = take(sizeof(double) * (s0.n_dof + s0.n_active));
-  c.dir_start0 = s0.d_dir_start;
-  c.a64 = s0.d_a;
-  c.cinv = h.d_cinv;
-  if (off > (size_t)kClusterSmem) return false;
-  h.cl_smem = off;
-  if (cudaFuncSetAttribute(mg_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
-      cudaFuncSetAttribute(mg_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)off) != cudaSuccess)
-  {
-    cudaGetLastError();
-    return false;
-  }
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(nb);
-  cfg.blockDim = dim3(kClusterThreads);
-  cfg.dynamicSmemBytes = off;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = nb;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  int clusters = 0;
-  if (cudaOccupancyMaxActiveClusters(&clusters, mg_cluster_kernel, &cfg) != cudaSuccess || clusters < 1)
-  {
-    cudaGetLastError();
-    return false;
-  }
-  return true;
-}
-
-// levels 0 .. i of an FP32 V-cycle as one cluster launch (mgcluster.cuh); false when the
-// cycle does not take it (the per-level launches run instead)
-static bool cycle_on_cluster(cdgpu_ctx *ctx, Hierarchy &h, CycleState &cs, int i)
-{
-  const cdgpu_solver_params &p = *cs.p;
-  if (i != h.cl_top || p.cycle != 1 || p.coarse_smoother != 17 || !cs.active_zero[i] || !cs.sol_zero[i] ||
-      cs.pre_done[i] != 0)
-    return false;
-  ClusterCycle c = h.cl_plan;
-  c.pre = p.pre;
-  c.post = p.post;
-  c.omega = (float)p.omega;
-  c.damp = (float)p.gmg_damp;
-  LevelVec<float> &top = h.lev[i].v32;
-  c.top_rhs = top.rhs;
-  // the host's pointer bookkeeping: every sweep swaps the top level's (sol, alt); the final
-  // iterate goes where sol points afterwards
-  if ((p.pre + p.post) & 1) std::swap(top.sol, top.alt);
-  c.top_out = top.sol;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(kClusterCtas);
-  cfg.blockDim = dim3(kClusterThreads);
-  cfg.dynamicSmemBytes = h.cl_smem;
-  cfg.stream = ctx->stream;
-  cudaLaunchAttribute attr[2];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = kClusterCtas;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[1].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = cd_pdl_enabled() ? 2 : 1;
-  if (cudaLaunchKernelEx(&cfg, mg_cluster_kernel, c) != cudaSuccess)
-  {
-    cudaGetLastError();
-    if ((p.pre + p.post) & 1) std::swap(top.sol, top.alt);
-    return false;
-  }
-  for (int l = 0; l <= i; l++) cs.sol_zero[l] = cs.active_zero[l] = false;
-  return true;
-}
-
 template <typename T> static int cycle(cdgpu_ctx *ctx, Hierarchy &h, CycleState &cs, int i)
 {
-  if constexpr (std::is_same<T, float>::value)
-    if (cycle_on_cluster(ctx, h, cs, i))
-    {
-      ctx->launches++;
-      return CDGPU_OK;
-    }
   if (i == 0) return coarse_solve<T>(ctx, h, cs);
   Level &L = h.lev[i], &C = h.lev[i - 1];
   const Space &s = *L.sp, &sc = *C.sp;
@@ -988,8 +804,6 @@ static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, 
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_exact_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm1));
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_smooth_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm2));
     CD_CUDA(ctx, cudaFuncSetAttribute(coarse_smooth_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm2));
-    h.cl_top = k == 1 ? cluster_top(h) : -1;
-    if (h.cl_top >= 1 && !plan_cluster(ctx, h, h.cl_top)) h.cl_top = -1;
     cudaGraph_t g = nullptr;
     const long long before = ctx->launches;
     CD_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));

@@ -160,12 +160,6 @@ class Context:
         self.check(self.lib.cdgpu_product_tuning(self.h, sid, buf, 1024))
         return buf.value.decode()
 
-    def cycle_report(self, mg):
-        """How the FP32 multigrid cycle of a hierarchy runs (after its first mixed solve)."""
-        buf = C.create_string_buffer(512)
-        self.check(self.lib.cdgpu_cycle_report(self.h, mg, buf, 512))
-        return buf.value.decode()
-
     def apply_fp32(self, sid, x, form):
         """y = A x with an FP32 form of the operator: 0 CSR copy, 1 matrix-free on CUDA cores,
         2 matrix-free on the tensor cores."""
