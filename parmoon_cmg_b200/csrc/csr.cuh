@@ -321,7 +321,9 @@ struct TmaMeta
   int rb, re, rb0, nb0; // rows [rb, re); row-pointer and nonzero copies start at rb0, nb0
 };
 
-template <int MODE, int CAP, int STAGES>
+// TPR threads per row (4: 64-row tiles, 16 gathers per thread and round; 8: 32-row tiles,
+// 8 gathers per thread and round -- the same 64 entries of a row in flight per round)
+template <int MODE, int CAP, int STAGES, int TPR = 4>
 __global__ void __launch_bounds__((kTmaWarps + 1) * 32) csr_tma_kernel(CsrArgs<double> p, const int2 *__restrict__ tiles,
                                                                          int n_tiles, int *__restrict__ err)
 {
@@ -407,7 +409,8 @@ __global__ void __launch_bounds__((kTmaWarps + 1) * 32) csr_tma_kernel(CsrArgs<d
   else
   {
     CD_PDL_WAIT(); // x (and, in the Jacobi sweep, f) are read only after the predecessor completed
-    const int g = lane / 4, l4 = lane % 4;
+    constexpr int G = 64 / TPR, RW = 32 / TPR; // gathers per thread and round, rows per warp
+    const int g = lane / TPR, lt = lane % TPR;
     for (int k = 0; k < my_tiles; k++)
     {
       const int s = k % kTmaStages, f = k / kTmaStages;
@@ -426,45 +429,49 @@ __global__ void __launch_bounds__((kTmaWarps + 1) * 32) csr_tma_kernel(CsrArgs<d
       const TmaMeta m = meta[s];
       const double *va = stage_vals(s);
       const int *co = stage_cols(s), *rs = stage_rp(s);
-      const int r = m.rb + warp * 8 + g;
+      const int r = m.rb + warp * RW + g;
       double sum = 0;
       if (r < m.re)
       {
         const int jb = rs[r - m.rb0] - m.nb0, je = rs[r + 1 - m.rb0] - m.nb0;
-        // 16 entries per thread at once: every gather of a row of up to 64 entries is in
+        // G entries per thread at once: every gather of a row of up to 64 entries is in
         // flight together (longer rows take a second round)
-        for (int j0 = jb + l4; j0 < je; j0 += 64)
+        for (int j0 = jb + lt; j0 < je; j0 += 64)
         {
-          int c[16];
+          int c[G];
 #pragma unroll
-          for (int u = 0; u < 16; u++)
+          for (int u = 0; u < G; u++)
           {
-            const int j = j0 + 4 * u;
+            const int j = j0 + TPR * u;
             c[u] = j < je ? co[j] : -1;
           }
-          // the 16 gathers are issued in order before the first product (positions beyond
+          // the G gathers are issued in order before the first product (positions beyond
           // the row read x[0] and are multiplied by nothing)
-          double xv[16];
+          double xv[G];
 #pragma unroll
-          for (int u = 0; u < 16; u++)
+          for (int u = 0; u < G; u++)
             asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(xv[u]) : "l"(p.x + (c[u] >= 0 ? c[u] : 0)));
-          // all 16 values pass through this point before any product uses one, so the compiler
+          // all G values pass through this point before any product uses one, so the compiler
           // cannot put a product (and its wait) between two gathers
-          asm volatile("" : "+d"(xv[0]), "+d"(xv[1]), "+d"(xv[2]), "+d"(xv[3]), "+d"(xv[4]), "+d"(xv[5]),
-                       "+d"(xv[6]), "+d"(xv[7]), "+d"(xv[8]), "+d"(xv[9]), "+d"(xv[10]), "+d"(xv[11]), "+d"(xv[12]),
-                       "+d"(xv[13]), "+d"(xv[14]), "+d"(xv[15]));
+          if constexpr (G == 16)
+            asm volatile("" : "+d"(xv[0]), "+d"(xv[1]), "+d"(xv[2]), "+d"(xv[3]), "+d"(xv[4]), "+d"(xv[5]),
+                         "+d"(xv[6]), "+d"(xv[7]), "+d"(xv[8]), "+d"(xv[9]), "+d"(xv[10]), "+d"(xv[11]), "+d"(xv[12]),
+                         "+d"(xv[13]), "+d"(xv[14]), "+d"(xv[15]));
+          else
+            asm volatile("" : "+d"(xv[0]), "+d"(xv[1]), "+d"(xv[2]), "+d"(xv[3]), "+d"(xv[4]), "+d"(xv[5]),
+                         "+d"(xv[6]), "+d"(xv[7]));
 #pragma unroll
-          for (int u = 0; u < 16; u++)
+          for (int u = 0; u < G; u++)
           {
-            const int j = j0 + 4 * u;
+            const int j = j0 + TPR * u;
             if (j < je) sum += va[j] * xv[u];
           }
         }
       }
-      sum = csr_group_sum<4>(sum);
+      sum = csr_group_sum<TPR>(sum);
       __syncwarp();
       if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tma_smem_u32(&empty[s])) : "memory");
-      if (r < m.re && l4 == 0) csr_epilogue<double, MODE>(p, r, sum, acc);
+      if (r < m.re && lt == 0) csr_epilogue<double, MODE>(p, r, sum, acc);
     }
   }
   if (MODE == CM_DEFECT && p.partial)

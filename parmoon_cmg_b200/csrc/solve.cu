@@ -491,9 +491,11 @@ template <typename T> static CsrArgs<T> csr_args(const Space &s, const T *x)
 // there are tiles
 struct TmaVariant
 {
-  int cap, stages;
+  int cap, stages, tpr; // nonzeros per tile, shared-memory stages, threads per row
 };
-static const TmaVariant kTmaVariants[] = {{2048, 4}, {2048, 2}, {3072, 3}, {3072, 2}, {4096, 2}, {2048, 3}, {1536, 2}};
+static const TmaVariant kTmaVariants[] = {{2048, 4, 4}, {2048, 2, 4}, {3072, 3, 4}, {3072, 2, 4}, {4096, 2, 4},
+                                          {2048, 3, 4}, {1536, 2, 4}, {2048, 2, 8}, {2048, 3, 8}, {1536, 2, 8},
+                                          {2048, 4, 8}};
 constexpr int kNumTmaVariants = sizeof(kTmaVariants) / sizeof(kTmaVariants[0]);
 
 template <int MODE> static void (*tma_kernel(int v))(CsrArgs<double>, const int2 *, int, int *)
@@ -506,9 +508,15 @@ template <int MODE> static void (*tma_kernel(int v))(CsrArgs<double>, const int2
     case 4: return csr_tma_kernel<MODE, 4096, 2>;
     case 5: return csr_tma_kernel<MODE, 2048, 3>;
     case 6: return csr_tma_kernel<MODE, 1536, 2>;
+    case 7: return csr_tma_kernel<MODE, 2048, 2, 8>;
+    case 8: return csr_tma_kernel<MODE, 2048, 3, 8>;
+    case 9: return csr_tma_kernel<MODE, 1536, 2, 8>;
+    case 10: return csr_tma_kernel<MODE, 2048, 4, 8>;
     default: return csr_tma_kernel<MODE, 2048, 4>;
   }
 }
+// rows per tile of a variant: the consumer warps' rows (8 warps x 32 / threads per row)
+static int tma_rows(int v) { return kTmaWarps * 32 / kTmaVariants[v].tpr; }
 static int tma_smem(int v) { return tma_smem_bytes(kTmaVariants[v].cap, kTmaVariants[v].stages); }
 static int tma_var(const Space &s) { return s.tma_var < 0 ? 0 : s.tma_var; }
 
@@ -836,7 +844,7 @@ static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, 
 // kernels.
 constexpr long kTmaMinNnz = 4L << 20;
 
-static bool make_tiles(const Space &s, int cap, std::vector<int2> &tiles)
+static bool make_tiles(const Space &s, int cap, int rows, std::vector<int2> &tiles)
 {
   tiles.clear();
   const int *rp = s.h_row_ptr.data();
@@ -845,7 +853,7 @@ static bool make_tiles(const Space &s, int cap, std::vector<int2> &tiles)
   {
     if (rp[r + 1] - rp[r] > cap) return false;
     int e = r;
-    while (e < s.n_dof && e - r < kTmaRows && rp[e + 1] - rp[r] <= cap) e++;
+    while (e < s.n_dof && e - r < rows && rp[e + 1] - rp[r] <= cap) e++;
     tiles.push_back(make_int2(r, rp[r]));
     r = e;
   }
@@ -861,7 +869,7 @@ int build_csr_tiles(cdgpu_ctx *ctx, Space &s)
   s.tma_report.clear();
   if (s.nnz < kTmaMinNnz) return CDGPU_OK;
   std::vector<int2> tiles;
-  if (!make_tiles(s, kTmaVariants[0].cap, tiles)) return CDGPU_OK;
+  if (!make_tiles(s, kTmaVariants[0].cap, tma_rows(0), tiles)) return CDGPU_OK;
   int rc;
   if ((rc = ensure_err_flag(ctx))) return rc;
   if ((rc = dev_alloc(ctx, &s.d_tiles, tiles.size()))) return rc;
@@ -898,7 +906,7 @@ static int tune_tma(cdgpu_ctx *ctx, Space &s)
   {
     std::vector<int2> tiles;
     const int ctas = tma_ctas_per_sm(v);
-    if (ctas <= 0 || !make_tiles(s, kTmaVariants[v].cap, tiles)) continue;
+    if (ctas <= 0 || !make_tiles(s, kTmaVariants[v].cap, tma_rows(v), tiles)) continue;
     int2 *dt = nullptr;
     if ((rc = dev_alloc(ctx, &dt, tiles.size()))) break;
     CD_CUDA(ctx, cudaMemcpy(dt, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
@@ -918,8 +926,8 @@ static int tune_tma(cdgpu_ctx *ctx, Space &s)
     CD_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
     ms /= 5;
     char line[128];
-    snprintf(line, sizeof(line), "%scap %d stages %d ctas/SM %d: %.1f us", report.empty() ? "" : "; ",
-             kTmaVariants[v].cap, kTmaVariants[v].stages, ctas, 1e3 * ms);
+    snprintf(line, sizeof(line), "%scap %d rows %d stages %d ctas/SM %d: %.1f us", report.empty() ? "" : "; ",
+             kTmaVariants[v].cap, tma_rows(v), kTmaVariants[v].stages, ctas, 1e3 * ms);
     report += line;
     if (ms < best_ms)
     {
@@ -946,8 +954,8 @@ static int tune_tma(cdgpu_ctx *ctx, Space &s)
   s.tma_var = best;
   s.tma_ctas = best_ctas;
   char sel[96];
-  snprintf(sel, sizeof(sel), "chosen: cap %d stages %d ctas/SM %d; ", kTmaVariants[best].cap, kTmaVariants[best].stages,
-           best_ctas);
+  snprintf(sel, sizeof(sel), "chosen: cap %d rows %d stages %d ctas/SM %d; ", kTmaVariants[best].cap, tma_rows(best),
+           kTmaVariants[best].stages, best_ctas);
   s.tma_report = sel + report;
   return CDGPU_OK;
 }
