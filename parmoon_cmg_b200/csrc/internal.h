@@ -96,6 +96,7 @@ struct Space
   long mf_version = -1;         // assembly the FP32 copies were made from
   float *d_cf32 = nullptr;      // n_cells x T cell coefficients
   float *d_R32 = nullptr;       // T x nbf x nbf reference tensors, [t][i][j]
+  float *d_R32img = nullptr;    // the tensor-core kernel's B operand as its shared-memory image
   float *d_ybuf = nullptr;      // nbf x n_cells per-cell products
   double *d_local = nullptr;    // quadrature path: n_cells x (nbf*nbf + nbf)
   double *d_dir = nullptr;      // Dirichlet values

@@ -178,10 +178,25 @@ template <int T> constexpr int mf_tc_smem_bytes()
   return 128 * 32 * 4 + 32 * T * 32 * 4 + 2 * (mf_tc_gn_bytes<T>() + mf_tc_cf_bytes<T>());
 }
 
+// the B operand of mf_cell27_tc_kernel as its shared-memory image (32T x 32 floats in the
+// core-matrix layout, rows i >= 27 and columns k >= 27 zero), written once per assembly so
+// that the kernel stages it with one bulk copy
+__global__ void mf_tc_tensor_image_kernel(int T, const float *__restrict__ R32, float *__restrict__ img)
+{
+  CD_PDL_ENTRY();
+  constexpr int KP = 32, NB = 27;
+  const int N = 32 * T;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N * KP; e += gridDim.x * blockDim.x)
+  {
+    const int n = e / KP, k = e % KP, t = n / 32, i = n % 32;
+    img[mf_core_off(n, k, N) / 4] = (i < NB && k < NB) ? R32[(t * NB + i) * NB + k] : 0.f;
+  }
+}
+
 template <int T>
 __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const int *__restrict__ gn,
                                                               const float *__restrict__ cf32,
-                                                              const float *__restrict__ R32,
+                                                              const float *__restrict__ Bimg,
                                                               const float *__restrict__ x, float *__restrict__ ybuf,
                                                               int *__restrict__ err, int pre)
 {
@@ -197,6 +212,7 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
   constexpr int GB = mf_tc_gn_bytes<T>(), CB = mf_tc_cf_bytes<T>();
   __shared__ __align__(8) uint64_t mbar;
   __shared__ __align__(8) uint64_t sbar[2];
+  __shared__ __align__(8) uint64_t bbar; // the B image's bulk copy
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   const int n_tiles = (n_cells + MT - 1) / MT;
@@ -205,6 +221,7 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mf_smem_u32(&mbar)), "r"(1));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mf_smem_u32(&sbar[0])), "r"(1));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mf_smem_u32(&sbar[1])), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mf_smem_u32(&bbar)), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   // the copies of a tile's numbers and coefficients: sizes rounded up to 16 bytes (the
@@ -226,16 +243,15 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
   __syncthreads();
   if (tid == 0)
   {
+    // B = the tensors' shared-memory image (N x 32 floats, a multiple of 16 bytes), one copy
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mf_smem_u32(&bbar)),
+                 "r"((uint32_t)(N * KP * 4))
+                 : "memory");
+    mf_bulk_g2s(Bs, Bimg, (uint32_t)(N * KP * 4), &bbar);
     if (blockIdx.x < n_tiles) issue(blockIdx.x, 0);
     if (blockIdx.x + gridDim.x < n_tiles) issue(blockIdx.x + gridDim.x, 1);
   }
-  // B = the tensors, zero-padded rows i >= 27 and columns k >= 27; A zero everywhere once
-  for (int e = tid; e < N * KP; e += blockDim.x)
-  {
-    const int n = e / KP, k = e % KP, t = n / 32, i = n % 32;
-    const float v = (i < NB && k < NB) ? R32[(t * NB + i) * NB + k] : 0.f;
-    *(float *)(Bs + mf_core_off(n, k, N)) = v;
-  }
+  // A zero everywhere once (rows of absent cells and columns k >= 27 stay zero)
   for (int e = tid; e < MT * KP; e += blockDim.x) ((float *)As)[e] = 0.f;
   if (pre) CD_PDL_ENTRY();
   if (warp == 0)
@@ -285,6 +301,14 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
     for (int t = 0; t < T; t++) cn[t] = in ? cq[tid * T + t] : 0.f;
   };
   gather(0);
+  // the B image must have landed before the first product (bounded, CTA-uniform)
+  bool b_in_flight = false;
+  if (ok && !__syncthreads_and(mf_wait_parity(&bbar, 0u, 1L << 24) != 0))
+  {
+    if (tid == 0) atomicExch(err, 3);
+    ok = false;
+    b_in_flight = true;
+  }
   int li = 0;
   for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, li++)
   {
@@ -403,6 +427,7 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
     // a copy still in flight (after a timeout): bounded wait for it
     if (issued0 > waited0) (void)mf_wait_parity(&sbar[0], (uint32_t)(issued0 - 1) & 1u, 1L << 24);
     if (issued1 > waited1) (void)mf_wait_parity(&sbar[1], (uint32_t)(issued1 - 1) & 1u, 1L << 24);
+    if (b_in_flight) (void)mf_wait_parity(&bbar, 0u, 1L << 24);
   }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
@@ -506,13 +531,13 @@ inline void mf_apply_cells(cdgpu_ctx *ctx, const Space &s, const float *x, bool 
     if (s.mf_T == 10)
     {
       (void)cd_launch(mf_cell27_tc_kernel<10>, grid, 128, kMfTcSmem, ctx->stream, s.n_cells, s.d_gn, s.d_cf32,
-                      s.d_R32, x, s.d_ybuf, ctx->d_err, ctx->pdl_pre ? 1 : 0);
+                      s.d_R32img, x, s.d_ybuf, ctx->d_err, ctx->pdl_pre ? 1 : 0);
       return;
     }
     if (s.mf_T == 13)
     {
       (void)cd_launch(mf_cell27_tc_kernel<13>, grid, 128, kMfTcSmem, ctx->stream, s.n_cells, s.d_gn, s.d_cf32,
-                      s.d_R32, x, s.d_ybuf, ctx->d_err, ctx->pdl_pre ? 1 : 0);
+                      s.d_R32img, x, s.d_ybuf, ctx->d_err, ctx->pdl_pre ? 1 : 0);
       return;
     }
   }
