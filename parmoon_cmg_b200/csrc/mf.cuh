@@ -251,8 +251,10 @@ __global__ void __launch_bounds__(128, 1) mf_cell27_tc_kernel(int n_cells, const
     if (blockIdx.x < n_tiles) issue(blockIdx.x, 0);
     if (blockIdx.x + gridDim.x < n_tiles) issue(blockIdx.x + gridDim.x, 1);
   }
-  // A zero everywhere once (rows of absent cells and columns k >= 27 stay zero)
-  for (int e = tid; e < MT * KP; e += blockDim.x) ((float *)As)[e] = 0.f;
+  // A: the padding columns k >= 27 zero once (every tile writes columns 0..26 of all 128 rows,
+  // zeros for absent cells)
+#pragma unroll
+  for (int k = NB; k < KP; k++) *(float *)(As + mf_core_off(tid, k, MT)) = 0.f;
   if (pre) CD_PDL_ENTRY();
   if (warp == 0)
   {
