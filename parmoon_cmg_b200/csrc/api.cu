@@ -75,6 +75,10 @@ static void free_mg(Hierarchy *h)
   if (h->h_slot) cudaFreeHost(h->h_slot);
   for (auto &e : h->ev_slot)
     if (e) cudaEventDestroy(e);
+  for (auto &e : h->ev_ready)
+    if (e) cudaEventDestroy(e);
+  if (h->ev_beta) cudaEventDestroy(h->ev_beta);
+  if (h->cstream) cudaStreamDestroy(h->cstream);
   delete h;
 }
 

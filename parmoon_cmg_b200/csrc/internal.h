@@ -157,6 +157,10 @@ struct Hierarchy
   unsigned io_slot = 0;
   double *h_slot = nullptr;            // pinned: two slots of an FGMRES iteration's control block
   cudaEvent_t ev_slot[2] = {nullptr, nullptr}; // recorded behind each slot's copy
+  // the slots' copies run on their own stream, after the iteration's Gram-Schmidt passes
+  // (ev_ready) and beside the rest of the iteration; ev_beta: the initial residual's copy
+  cudaStream_t cstream = nullptr;
+  cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_beta = nullptr;
   int *h_cflag = nullptr;     // pinned copy of the coarse inversion's zero-pivot flag
   bool cflag_pending = false; // copy enqueued, not yet checked
   unsigned *d_gs_count = nullptr; // arrival counter of the Gram-Schmidt passes' last-block reduction

@@ -1007,6 +1007,9 @@ int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m)
     CD_CUDA(ctx, cudaMallocHost((void **)&h.h_ctl, 256 * sizeof(double)));
     CD_CUDA(ctx, cudaMallocHost((void **)&h.h_slot, 2 * 80 * sizeof(double)));
     for (auto &e : h.ev_slot) CD_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto &e : h.ev_ready) CD_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CD_CUDA(ctx, cudaEventCreateWithFlags(&h.ev_beta, cudaEventDisableTiming));
+    CD_CUDA(ctx, cudaStreamCreateWithFlags(&h.cstream, cudaStreamNonBlocking));
     CD_CUDA(ctx, cudaMallocHost((void **)&h.h_io, 128 * sizeof(double *)));
     if ((rc = dev_alloc(ctx, &h.d_io, 2))) return rc;
     if ((rc = dev_alloc(ctx, &h.d_gs_count, 1))) return rc;
@@ -1201,9 +1204,10 @@ static int precondition(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params 
 }
 
 // the host copy of the FGMRES control block: [0..k) h1, [33..33+k) h2, [66] ||w||^2
-static int read_ctl(cdgpu_ctx *ctx, Hierarchy &h, int count)
+static int read_ctl(cdgpu_ctx *ctx, Hierarchy &h, int count, const double *src = nullptr)
 {
-  CD_CUDA(ctx, cudaMemcpyAsync(h.h_ctl, h.d_ctl, sizeof(double) * count, cudaMemcpyDeviceToHost, ctx->stream));
+  CD_CUDA(ctx, cudaMemcpyAsync(h.h_ctl, src ? src : h.d_ctl, sizeof(double) * count, cudaMemcpyDeviceToHost,
+                               ctx->stream));
   CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return CDGPU_OK;
 }
@@ -1246,9 +1250,56 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
   const int blocks = (n + 255) / 256;
   auto V = [&](int k) { return h.d_V + (size_t)k * n; };
   auto Z = [&](int k) { return h.d_Z + (size_t)k * n; };
-  // r0 = f - A x, beta = ||r0|| (FgmresIte.C:275-284)
-  if ((rc = finest_defect_norm(ctx, h, x, f, V(0), h.d_ctl))) return rc;
-  if ((rc = read_ctl(ctx, h, 1))) return rc;
+  // control blocks: an iteration's Gram-Schmidt results (dots at +0 and +33, ||w||^2 at +66)
+  // alternate between two blocks by the iteration's parity, the residual norm has its own
+  // slot; the back-substitution coefficients are at +100
+  auto ctl_it = [&](int i) { return h.d_ctl + (i & 1) * 160; };
+  double *const nrm = h.d_ctl + 240;
+  // r0 = f - A x, beta = ||r0|| (FgmresIte.C:275-284); v_0 = r0 / beta is formed on the device
+  // and the first iteration enqueued while ||r0||^2 travels to the host on the copy stream
+  if ((rc = finest_defect_norm(ctx, h, x, f, V(0), nrm))) return rc;
+  CD_CUDA(ctx, cudaEventRecord(h.ev_ready[0], ctx->stream));
+  CD_CUDA(ctx, cudaStreamWaitEvent(h.cstream, h.ev_ready[0], 0));
+  CD_CUDA(ctx, cudaMemcpyAsync(h.h_ctl, nrm, sizeof(double), cudaMemcpyDeviceToHost, h.cstream));
+  CD_CUDA(ctx, cudaEventRecord(h.ev_beta, h.cstream));
+  // Iteration i on the device: the preconditioner on v_i, w = A z_i, the Gram-Schmidt passes,
+  // a copy of the control block to pinned slot i % 2 (on the copy stream, behind an event, so
+  // the iteration does not wait for it) and v_{i+1} = w / ||w||, which needs no host value.
+  // The host then applies the Givens rotations and the stopping tests.  While it waits for
+  // iteration i it has, as a rule, already enqueued iteration i + 1, so the device does not
+  // idle during the host's part; it does not when the residual predicted from the convergence
+  // so far is within a factor of 4 of the stopping threshold, because an iteration enqueued
+  // after the one that converges is wasted.  Which iterations are enqueued early changes no
+  // arithmetic.
+  auto enqueue = [&](int i) -> int {
+    int rc2;
+    if ((rc2 = precondition(ctx, h, p, V(i), Z(i)))) return rc2;
+    if ((rc2 = spmv64(ctx, s, Z(i), h.d_w))) return rc2;
+    int k = i + 1, pb = h.partial_blocks;
+    double *c = ctl_it(i);
+    // pass 1: h1 = V^T w
+    launch_gs<GS_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, nullptr, h.d_partial, c, h.d_gs_count);
+    CD_LAUNCHED(ctx);
+    // pass 2: w -= V h1, h2 = V^T w
+    launch_gs<GS_AXPY_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, c, h.d_partial, c + 33, h.d_gs_count);
+    CD_LAUNCHED(ctx);
+    // w -= V h2, ||w||^2
+    launch_gs<GS_AXPY_NORM>(k, pb, ctx->stream, n, h.d_V, h.d_w, c + 33, h.d_partial, c + 66, h.d_gs_count);
+    CD_LAUNCHED(ctx);
+    CD_CUDA(ctx, cudaEventRecord(h.ev_ready[i & 1], ctx->stream));
+    CD_CUDA(ctx, cudaStreamWaitEvent(h.cstream, h.ev_ready[i & 1], 0));
+    CD_CUDA(ctx, cudaMemcpyAsync(h.h_slot + (i & 1) * 80, c, sizeof(double) * 67, cudaMemcpyDeviceToHost, h.cstream));
+    CD_CUDA(ctx, cudaEventRecord(h.ev_slot[i & 1], h.cstream));
+    (void)cd_launch(scale_norm_kernel, blocks, 256, 0, ctx->stream, n, c + 66, h.d_w, V(i + 1));
+    CD_LAUNCHED(ctx);
+    return CDGPU_OK;
+  };
+  // the first restart cycle's v_0 and iteration 0, before ||r0|| is known on the host (if the
+  // start already satisfies the stopping test they are discarded: x is not touched)
+  (void)cd_launch(scale_norm_kernel, blocks, 256, 0, ctx->stream, n, (const double *)nrm, V(0), V(0));
+  CD_LAUNCHED(ctx);
+  if ((rc = enqueue(0))) return rc;
+  CD_CUDA(ctx, cudaEventSynchronize(h.ev_beta));
   double res = std::sqrt(h.h_ctl[0]), res0 = res, beta = res;
   info->initial_residual = res;
   int maxite = p.maxit, ret = 0, status = CDGPU_OK;
@@ -1256,6 +1307,8 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
   {
     if (p.minit == 0 || beta < 1e-20)
     {
+      CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      CD_CUDA(ctx, cudaStreamSynchronize(h.cstream));
       info->iterations = 0;
       info->final_residual = res;
       info->status = CDGPU_OK;
@@ -1264,47 +1317,21 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
     maxite = p.minit;
   }
   int j = 1;
-  bool done = false;
+  bool done = false, first_cycle = true;
   while (j <= maxite && !done)
   {
-    (void)cd_launch(scale_kernel, blocks, 256, 0, ctx->stream, n, 1.0 / beta, V(0), V(0));
-    CD_LAUNCHED(ctx);
+    if (!first_cycle)
+    {
+      (void)cd_launch(scale_norm_kernel, blocks, 256, 0, ctx->stream, n, (const double *)nrm, V(0), V(0));
+      CD_LAUNCHED(ctx);
+    }
     std::fill(sv.begin(), sv.end(), 0.0);
     sv[0] = beta;
-    // Iteration i on the device: the preconditioner on v_i, w = A z_i, the Gram-Schmidt passes,
-    // a copy of the control block to pinned slot i % 2 (and an event behind it), and
-    // v_{i+1} = w / ||w||, which needs no host value.  The host then applies the Givens
-    // rotations and the stopping tests.  While it waits for iteration i it has, as a rule,
-    // already enqueued iteration i + 1, so the device does not idle during the host's part;
-    // it does not when the residual predicted from the convergence so far is within a factor
-    // of 4 of the stopping threshold, because an iteration enqueued after the one that
-    // converges is wasted.  Which iterations are enqueued early changes no arithmetic.
-    auto enqueue = [&](int i) -> int {
-      int rc2;
-      if ((rc2 = precondition(ctx, h, p, V(i), Z(i)))) return rc2;
-      if ((rc2 = spmv64(ctx, s, Z(i), h.d_w))) return rc2;
-      int k = i + 1, pb = h.partial_blocks;
-      // pass 1: h1 = V^T w
-      launch_gs<GS_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, nullptr, h.d_partial, h.d_ctl, h.d_gs_count);
-      CD_LAUNCHED(ctx);
-      // pass 2: w -= V h1, h2 = V^T w
-      launch_gs<GS_AXPY_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, h.d_ctl, h.d_partial, h.d_ctl + 33, h.d_gs_count);
-      CD_LAUNCHED(ctx);
-      // w -= V h2, ||w||^2
-      launch_gs<GS_AXPY_NORM>(k, pb, ctx->stream, n, h.d_V, h.d_w, h.d_ctl + 33, h.d_partial, h.d_ctl + 66,
-                              h.d_gs_count);
-      CD_LAUNCHED(ctx);
-      CD_CUDA(ctx, cudaMemcpyAsync(h.h_slot + (i & 1) * 80, h.d_ctl, sizeof(double) * 67, cudaMemcpyDeviceToHost,
-                                   ctx->stream));
-      CD_CUDA(ctx, cudaEventRecord(h.ev_slot[i & 1], ctx->stream));
-      (void)cd_launch(scale_norm_kernel, blocks, 256, 0, ctx->stream, n, h.d_ctl + 66, h.d_w, V(i + 1));
-      CD_LAUNCHED(ctx);
-      return CDGPU_OK;
-    };
     const double thr = std::max(p.res_norm_min, p.red_factor * res0);
     double last = beta, rate = 0.5;
     int i;
-    if ((rc = enqueue(0))) return rc;
+    if (!first_cycle && (rc = enqueue(0))) return rc;
+    first_cycle = false;
     for (i = 0; i < m && j <= maxite; i++, j++)
     {
       bool next_enqueued = false;
@@ -1365,8 +1392,8 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
     CD_CUDA(ctx, cudaMemcpyAsync(h.d_ctl + 100, y.data(), sizeof(double) * m, cudaMemcpyHostToDevice, ctx->stream));
     (void)cd_launch(update_kernel, blocks, 256, 0, ctx->stream, n, m, h.d_ctl + 100, h.d_Z, x);
     CD_LAUNCHED(ctx);
-    if ((rc = finest_defect_norm(ctx, h, x, f, V(0), h.d_ctl))) return rc;
-    if ((rc = read_ctl(ctx, h, 1))) return rc;
+    if ((rc = finest_defect_norm(ctx, h, x, f, V(0), nrm))) return rc;
+    if ((rc = read_ctl(ctx, h, 1, nrm))) return rc;
     res = beta = std::sqrt(h.h_ctl[0]);
     if (p.stop_rule == 0) res0 = res; // the reference measures the next cycle against this residual
   }
@@ -1378,6 +1405,7 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
   if (ctx->d_err && ctx->h_err)
     CD_CUDA(ctx, cudaMemcpyAsync(ctx->h_err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  CD_CUDA(ctx, cudaStreamSynchronize(h.cstream));
   info->iterations = ret;
   info->final_residual = res;
   info->status = status;
