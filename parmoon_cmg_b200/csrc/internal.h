@@ -191,6 +191,7 @@ struct cdgpu_ctx
   // set while the multigrid cycle is recorded into its graph: its kernels load the data that
   // no kernel of the cycle writes before waiting for their predecessor
   bool pdl_pre = false;
+  bool mf_attr_set = false; // the tensor-core kernel's shared-memory attribute is set
   int *d_err = nullptr; // assembly error flag (device) and its pinned host mirror
   int *h_err = nullptr;
 };

@@ -393,6 +393,13 @@ __global__ void scale_norm_kernel(int n, const double *__restrict__ nrm2, const 
   if (hn != 0 && i < n) y[i] = (1.0 / hn) * x[i];
 }
 
+__global__ void set_io_kernel(double **io, const double *r, double *z)
+{
+  CD_PDL_ENTRY();
+  io[0] = const_cast<double *>(r);
+  io[1] = z;
+}
+
 __global__ void scale_kernel(int n, double alpha, const double *__restrict__ x, double *__restrict__ y)
 {
   CD_PDL_ENTRY();
@@ -825,11 +832,11 @@ static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, 
     if (e != cudaSuccess) { h.gexec[k] = nullptr; return cuda_fail(ctx, e, "graph instantiate"); }
     h.gparams[k] = p;
   }
-  int slot = (h.io_slot++) & 63;
-  h.h_io[2 * slot] = const_cast<double *>(r);
-  h.h_io[2 * slot + 1] = z;
-  CD_CUDA(ctx, cudaMemcpyAsync(h.d_io, h.h_io + 2 * slot, 2 * sizeof(double *), cudaMemcpyHostToDevice,
-                               ctx->stream));
+  // the application's (in, out) pointers into the graph's slot: a one-thread kernel in the
+  // stream's launch chain (a host-to-device copy would hold the stream for the copy engine's
+  // round trip)
+  (void)cd_launch(set_io_kernel, 1, 1, 0, ctx->stream, h.d_io, r, z);
+  CD_LAUNCHED(ctx);
   CD_CUDA(ctx, cudaGraphLaunch(h.gexec[k], ctx->stream));
   ctx->launches += h.graph_nodes[k];
   return CDGPU_OK;
@@ -1476,8 +1483,12 @@ static int prepare_mf(cdgpu_ctx *ctx, Space &s)
     }
     s.mf_version = s.assembly_version;
   }
-  CD_CUDA(ctx, cudaFuncSetAttribute(mf_cell27_tc_kernel<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMfTcSmem));
-  CD_CUDA(ctx, cudaFuncSetAttribute(mf_cell27_tc_kernel<13>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMfTcSmem));
+  if (!ctx->mf_attr_set)
+  {
+    CD_CUDA(ctx, cudaFuncSetAttribute(mf_cell27_tc_kernel<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMfTcSmem));
+    CD_CUDA(ctx, cudaFuncSetAttribute(mf_cell27_tc_kernel<13>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMfTcSmem));
+    ctx->mf_attr_set = true;
+  }
   if (!ctx->d_err)
   {
     if ((rc = dev_alloc(ctx, &ctx->d_err, 1))) return rc;
