@@ -70,6 +70,9 @@ struct Space
   // pattern (index into the variant table of solve.cu; -1 = not tuned yet) and its report
   int tma_var = -1;
   int tma_ctas = 0; // resident CTAs per SM of the chosen variant
+  // assembly_version at the last bulk-copy launch that waited for its predecessor before
+  // streaming the matrix: later launches of the same assembly may stream it before their wait
+  mutable long tma_safe_version = -1;
   std::string tma_report;
   // DOF -> (cell, local index) incidence, ascending cell per DOF
   int *d_inc_ptr = nullptr, *d_inc = nullptr;

@@ -552,7 +552,12 @@ template <typename T, int MODE> static bool launch_tma(cdgpu_ctx *ctx, const Spa
     if (s.n_tiles > 0 && ctx->d_err)
     {
       CsrArgs<double> p = pa;
-      p.pre = ctx->pdl_pre ? 1 : 0;
+      // the producer streams the matrix before waiting for the predecessor when no kernel
+      // that writes the matrix can still be running: inside the captured cycle, or once a
+      // launch of the same assembly has waited (every later kernel starts after that one's
+      // wait, hence after the assembly)
+      p.pre = ctx->pdl_pre || s.tma_safe_version == s.assembly_version ? 1 : 0;
+      if (!p.pre) s.tma_safe_version = s.assembly_version;
       const int v = tma_var(s);
       (void)cd_launch(tma_kernel<MODE>(v), grid, (kTmaWarps + 1) * 32, tma_smem(v), ctx->stream, p,
                       (const int2 *)s.d_tiles, s.n_tiles, ctx->d_err);
