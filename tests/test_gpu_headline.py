@@ -222,3 +222,37 @@ def test_bench_stopping_rule_error(ctx, case, reference, precision):
     err = rel(x, x_ref)
     print(f"precision {precision}: {info.iterations} iterations, rel. error vs reference {err:.3e}")
     assert err <= TOL_MIXED, err
+
+
+def test_bulk_copy_product_follows_reassembly(ctx):
+    """The finest matrix (15.8M nonzeros) takes the bulk-copy product, whose launches stream the
+    matrix ahead of their dependency wait once a launch of the same assembly has waited.  A
+    product enqueued right behind an asynchronous re-assembly with other coefficients (device
+    vectors, nothing between the two launches) must still read the new matrix: every product
+    against the oracle's CSR product of that assembly's own entries."""
+    import torch
+    import oracle
+    spaces, _ = mesh.structured_hierarchy(3, 2, N_FINE, 1)
+    sp = spaces[0]
+    sid = ctx.upload_space(sp)
+    nnz = ctx.build_pattern(sid)
+    rp, kc = ctx.get_pattern(sid, sp["n_dof"], nnz)
+    mg = ctx.hierarchy([sid], [None])
+    x = np.random.default_rng(5).standard_normal(sp["n_dof"])
+    dx = torch.tensor(x, dtype=torch.float64, device="cuda")
+    dy = torch.zeros_like(dx)
+    cases = [(EPS, B3), (1.0, (0.0, 0.0, 0.0)), (1e-3, (1.0, 0.0, 0.0))]
+    refs = []
+    for eps, b in cases:
+        ctx.set_coeffs(sid, coeffs(0, eps=eps, b=b, f=1.0))
+        ent, _ = ctx.assemble(sid, GALERKIN, sp["n_dof"], nnz)
+        refs.append(oracle.spmv(rp, kc, ent, x))
+    torch.cuda.synchronize()
+    for (eps, b), y_ref in zip(cases, refs):
+        ctx.set_coeffs(sid, coeffs(0, eps=eps, b=b, f=1.0))
+        ctx.assemble_hierarchy(mg, GALERKIN, GALERKIN)  # enqueued, not waited for
+        for _ in range(3):  # the later launches of one assembly stream the matrix early
+            ctx.check(ctx.lib.cdgpu_spmv_device(ctx.h, sid, dx.data_ptr(), dy.data_ptr()))
+        torch.cuda.synchronize()
+        y = dy.cpu().numpy()
+        assert rel(y, y_ref) <= 1e-14, (eps, rel(y, y_ref))
