@@ -218,6 +218,15 @@ int cdgpu_product_tuning(cdgpu_ctx *ctx, int space_id, char *buf, int len);
  * need Q2 hexahedra assembled from affine cells with constant coefficients
  * (CDGPU_ERR_UNSUPPORTED otherwise).  h_x, h_y: host arrays of n_dof floats. */
 int cdgpu_apply_fp32(cdgpu_ctx *ctx, int space_id, int form, const float *h_x, float *h_y);
+/* y = A x with an FP64 form of the assembled operator (MatVect, src/FE/Blas2.C:11-99):
+ * form 0 the CSR entries (what cdgpu_spmv applies); 1 the matrix-free sum-factorised per-cell
+ * products A_c x_c = sum_t coef_{c,t} R_t x_c, values and gradients at the 3 x 3 x 3 Gauss
+ * points by one-dimensional passes, the form the mixed solve (precision 1) applies in its
+ * FGMRES iteration on a finest level of at least 16,384 such cells.  Equal to form 0 up to
+ * rounding; Dirichlet rows are identity rows.  Form 1 needs Q2 hexahedra assembled from affine
+ * cells with constant coefficients (CDGPU_ERR_UNSUPPORTED otherwise).  h_x, h_y: host arrays
+ * of n_dof doubles. */
+int cdgpu_apply_fp64(cdgpu_ctx *ctx, int space_id, int form, const double *h_x, double *h_y);
 /* The defect d = f - A x and *h_res = ||d||, like cdgpu_defect, for callers that cannot
  * allocate device memory (for example while another allocator holds the whole device, or
  * where the device synchronisation of cudaFree is not acceptable).  No counterpart in the

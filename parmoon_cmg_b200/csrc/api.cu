@@ -46,7 +46,7 @@ static void free_space(Space *s)
   void *ptrs[] = {s->d_coords, s->d_gn,  s->d_row_ptr, s->d_kcol,     s->d_dir_start, s->d_dir_rows, s->d_slot, s->d_inc_ptr, s->d_tiles,
                   s->d_inc,    s->d_a,   s->d_rhs,     s->d_diag,     s->d_a32,       s->d_diag32,
                   s->d_tab,    s->d_cellcoef, s->d_local, s->d_dir, s->d_ref, s->d_quadtab,
-                  s->d_cf32,   s->d_R32, s->d_R32img, s->d_ybuf};
+                  s->d_cf32,   s->d_R32, s->d_R32img, s->d_ybuf, s->d_ybuf64};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete s;
@@ -448,6 +448,33 @@ int cdgpu_spmv(cdgpu_ctx *ctx, int space_id, const double *h_x, double *h_y)
     CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (ctx->d_err) rc = assemble_check(ctx); // wait flag of the bulk-copy product
   }
+  cudaFree(dx);
+  cudaFree(dy);
+  return rc;
+}
+
+int cdgpu_apply_fp64(cdgpu_ctx *ctx, int space_id, int form, const double *h_x, double *h_y)
+{
+  Space *s = get_space(ctx, space_id);
+  if (!s || !s->assembled || !h_x || !h_y || form < 0 || form > 1)
+    return fail(ctx, CDGPU_ERR_INVALID, "apply_fp64: bad argument");
+  cudaSetDevice(ctx->device);
+  double *dx = nullptr, *dy = nullptr;
+  int rc;
+  if ((rc = dev_alloc(ctx, &dx, s->n_dof)) || (rc = dev_alloc(ctx, &dy, s->n_dof)))
+  {
+    if (dx) cudaFree(dx);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpyAsync(dx, h_x, sizeof(double) * s->n_dof, cudaMemcpyHostToDevice, ctx->stream);
+  rc = e == cudaSuccess ? apply_fp64_form(ctx, *s, form, dx, dy) : cuda_fail(ctx, e, "apply_fp64: copy");
+  if (!rc)
+  {
+    e = cudaMemcpyAsync(h_y, dy, sizeof(double) * s->n_dof, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "apply_fp64: copy back");
+  }
+  cudaStreamSynchronize(ctx->stream);
   cudaFree(dx);
   cudaFree(dy);
   return rc;

@@ -101,6 +101,11 @@ struct Space
   float *d_R32 = nullptr;       // T x nbf x nbf reference tensors, [t][i][j]
   float *d_R32img = nullptr;    // the tensor-core kernel's B operand as its shared-memory image
   float *d_ybuf = nullptr;      // nbf x n_cells per-cell products
+  // matrix-free FP64 operator (mf64.cuh) of the mixed form's FGMRES products: nbf x n_cells
+  // per-cell products, and the assembly at the last launch that waited for its predecessor
+  // before reading the cell data (later launches of that assembly may read it before the wait)
+  double *d_ybuf64 = nullptr;
+  mutable long mf64_safe_version = -1;
   double *d_local = nullptr;    // quadrature path: n_cells x (nbf*nbf + nbf)
   double *d_dir = nullptr;      // Dirichlet values
   double *d_ref = nullptr;      // reference tensors (affine path)
@@ -153,6 +158,9 @@ struct Hierarchy
   // captured multigrid cycle per precision (0 FP64, 1 FP32) and its in/out pointer slot
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   unsigned mf_mask = 0; // levels whose FP32 cycle in gexec[1] uses the matrix-free operator
+  // the running solve applies the finest operator matrix-free in FP64 (mixed form, Q2
+  // hexahedra from the affine constant-coefficient assembly), not from the CSR entries
+  bool mf64 = false;
   cdgpu_solver_params gparams[2] = {};
   long long graph_nodes[2] = {0, 0};
   double **d_io = nullptr;
@@ -302,6 +310,7 @@ int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m);
 int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *d_rhs,
               double *d_sol, cdgpu_solve_info *info);
 int apply_fp32_form(cdgpu_ctx *ctx, Space &s, int form, const float *d_x, float *d_y);
+int apply_fp64_form(cdgpu_ctx *ctx, Space &s, int form, const double *d_x, double *d_y);
 // the CSR pattern built on the device (pattern.cu)
 int build_pattern_device(cdgpu_ctx *ctx, Space &s, int **d_kcol_out, bool *fallback);
 // tiles of the TMA product for a freshly installed pattern (solve.cu)

@@ -29,6 +29,7 @@
 #include "internal.h"
 #include "csr.cuh"
 #include "mf.cuh"
+#include "mf64.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -1172,10 +1173,84 @@ static int refresh_coarse_inverse(cdgpu_ctx *ctx, Hierarchy &h)
 // ---------------------------------------------------------------------------
 // FP64 building blocks on the finest level
 // ---------------------------------------------------------------------------
+int spmv64(cdgpu_ctx *ctx, const Space &s, const double *x, double *y)
+{
+  csr_spmv<double>(ctx, s, x, y);
+  CD_LAUNCHED(ctx);
+  return CDGPU_OK;
+}
+
+// the matrix-free FP64 operator (mf64.cuh) applies to Q2 hexahedra assembled by the affine
+// constant-coefficient path: the cell coefficients of the last assembly are on the device
+static bool use_mf64(const Space &s)
+{
+  return s.assembled && s.mf_T > 0 && s.d_cellcoef && mf_shape_ok(s.nbf, s.mf_T) && s.dim == 3;
+}
+
+static int ensure_mf64(cdgpu_ctx *ctx, Space &s)
+{
+  if (!s.d_ybuf64) return dev_alloc(ctx, &s.d_ybuf64, (size_t)s.nbf * s.n_cells);
+  return CDGPU_OK;
+}
+
+// phase 1 of the matrix-free FP64 product: the per-cell products A_c x_c into d_ybuf64
+static void mf64_cells(cdgpu_ctx *ctx, const Space &s, const double *x)
+{
+  static const Mf64Tab tab = mf64_tables();
+  const int groups = (s.n_cells + kMf64Cells - 1) / kMf64Cells;
+  const int grid = std::max(1, std::min(groups, ctx->sm_count * 2));
+  const int cstride = s.mf_T + n_rhs_tensors(s.dim, s.ref_disctype);
+  // the cell data is read before the wait once a launch of this assembly has waited
+  const int pre = s.mf64_safe_version == s.assembly_version ? 1 : 0;
+  if (!pre) s.mf64_safe_version = s.assembly_version;
+  if (s.mf_T == 10)
+    (void)cd_launch(mf64_cell27_kernel<10>, grid, kMf64Warps * 32, 0, ctx->stream, s.n_cells, (const int *)s.d_gn,
+                    (const double *)s.d_cellcoef, cstride, tab, x, s.d_ybuf64, pre);
+  else
+    (void)cd_launch(mf64_cell27_kernel<13>, grid, kMf64Warps * 32, 0, ctx->stream, s.n_cells, (const int *)s.d_gn,
+                    (const double *)s.d_cellcoef, cstride, tab, x, s.d_ybuf64, pre);
+}
+
+// phase 2: y = A x, or d = f - A x with per-block sums of d^2 in partial (grid <= 8 per SM)
+static int mf64_rows_grid(const cdgpu_ctx *ctx, const Space &s)
+{
+  return std::max(1, std::min((s.n_dof + 255) / 256, ctx->sm_count * 8));
+}
+template <int MODE>
+static void mf64_rows(cdgpu_ctx *ctx, const Space &s, const double *x, const double *f, double *out, double *partial)
+{
+  (void)cd_launch(mf64_row_kernel<MODE>, mf64_rows_grid(ctx, s), 256, 0, ctx->stream, s.n_dof, s.n_active,
+                  s.n_cells, (const int *)s.d_inc_ptr, (const int *)s.d_inc, (const double *)s.d_ybuf64, x, f, out,
+                  partial);
+}
+
+// y = A x on the finest level: matrix-free in FP64 where the solve chose it, else the CSR entries
+static int finest_spmv(cdgpu_ctx *ctx, Hierarchy &h, const double *x, double *y)
+{
+  const Space &s = *h.lev.back().sp;
+  if (!h.mf64) return spmv64(ctx, s, x, y);
+  mf64_cells(ctx, s, x);
+  CD_LAUNCHED(ctx);
+  mf64_rows<MF64_SPMV>(ctx, s, x, nullptr, y, nullptr);
+  CD_LAUNCHED(ctx);
+  return CDGPU_OK;
+}
+
 static int finest_defect_norm(cdgpu_ctx *ctx, Hierarchy &h, const double *x, const double *f, double *d,
                               double *norm_out_dev)
 {
   const Space &s = *h.lev.back().sp;
+  if (h.mf64)
+  {
+    mf64_cells(ctx, s, x);
+    CD_LAUNCHED(ctx);
+    mf64_rows<MF64_DEFECT>(ctx, s, x, f, d, h.d_partial);
+    CD_LAUNCHED(ctx);
+    (void)cd_launch(sum_blocks_kernel, 1, 256, 0, ctx->stream, mf64_rows_grid(ctx, s), h.d_partial,
+                    norm_out_dev);
+    CD_LAUNCHED(ctx);
+    return CDGPU_OK;
+  }
   const int grid = defect_grid<double>(ctx, s); // <= 8 blocks per SM, within d_partial
   csr_defect<double>(ctx, s, x, f, d, h.d_partial, grid);
   CD_LAUNCHED(ctx);
@@ -1184,12 +1259,6 @@ static int finest_defect_norm(cdgpu_ctx *ctx, Hierarchy &h, const double *x, con
   return CDGPU_OK;
 }
 
-int spmv64(cdgpu_ctx *ctx, const Space &s, const double *x, double *y)
-{
-  csr_spmv<double>(ctx, s, x, y);
-  CD_LAUNCHED(ctx);
-  return CDGPU_OK;
-}
 
 int defect64(cdgpu_ctx *ctx, const Space &s, const double *x, const double *f, double *d, double *res)
 {
@@ -1286,7 +1355,7 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
   auto enqueue = [&](int i) -> int {
     int rc2;
     if ((rc2 = precondition(ctx, h, p, V(i), Z(i)))) return rc2;
-    if ((rc2 = spmv64(ctx, s, Z(i), h.d_w))) return rc2;
+    if ((rc2 = finest_spmv(ctx, h, Z(i), h.d_w))) return rc2;
     int k = i + 1, pb = h.partial_blocks;
     double *c = ctl_it(i);
     // pass 1: h1 = V^T w
@@ -1541,6 +1610,13 @@ int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const 
   if ((rc = tune_tma(ctx, *h.lev.back().sp))) return rc; // once per pattern, before any capture
   if (p.coarse_smoother == 17 && (rc = refresh_coarse_inverse(ctx, h))) return rc;
   if (p.precision == 1 && (rc = refresh_mf(ctx, h))) return rc;
+  // the mixed form applies the finest operator of its FGMRES iteration matrix-free in FP64 on
+  // levels large enough for the per-cell form to pay off; the FP64 form keeps the CSR entries
+  {
+    Space &fs = *h.lev.back().sp;
+    h.mf64 = p.precision == 1 && use_mf64(fs) && fs.n_cells >= kMfMinCells;
+    if (h.mf64 && (rc = ensure_mf64(ctx, fs))) return rc;
+  }
   cdgpu_solve_info local{};
   if (!info) info = &local;
   if (p.solver == 11) rc = fixed_point(ctx, h, p, d_rhs, d_sol, info);
@@ -1561,6 +1637,30 @@ int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const 
   if (rc == CDGPU_OK && ctx->d_err && ctx->h_err)
     rc = p.solver == 16 ? err_flag_status(ctx) : assemble_check(ctx);
   return rc;
+}
+
+// y = A x with one of the FP64 forms of a space's operator: form 0 the assembled CSR entries,
+// 1 the matrix-free sum-factorised per-cell products the mixed form's FGMRES iteration applies
+// on its finest level.  Dirichlet rows are identity rows in both.  Form 1 needs a Q2
+// hexahedral space assembled by the affine constant-coefficient path.
+int apply_fp64_form(cdgpu_ctx *ctx, Space &s, int form, const double *d_x, double *d_y)
+{
+  if (form == 0)
+  {
+    csr_spmv<double>(ctx, s, d_x, d_y);
+    CD_LAUNCHED(ctx);
+    return ctx->d_err ? assemble_check(ctx) : CDGPU_OK;
+  }
+  if (!use_mf64(s))
+    return fail(ctx, CDGPU_ERR_UNSUPPORTED,
+                "apply_fp64: the matrix-free form needs Q2 hexahedra assembled from affine cells with constant coefficients");
+  int rc = ensure_mf64(ctx, s);
+  if (rc) return rc;
+  mf64_cells(ctx, s, d_x);
+  CD_LAUNCHED(ctx);
+  mf64_rows<MF64_SPMV>(ctx, s, d_x, nullptr, d_y, nullptr);
+  CD_LAUNCHED(ctx);
+  return CDGPU_OK;
 }
 
 // y = A x with one of the FP32 forms of a space's operator that the mixed multigrid cycle uses:

@@ -168,6 +168,14 @@ class Context:
         self.check(self.lib.cdgpu_apply_fp32(self.h, sid, form, _p(x), _p(y)))
         return y
 
+    def apply_fp64(self, sid, x, form):
+        """y = A x with an FP64 form of the operator: 0 the CSR entries, 1 matrix-free (sum
+        factorisation, the mixed solve's FGMRES product)."""
+        x = _f64(x)
+        y = np.zeros_like(x)
+        self.check(self.lib.cdgpu_apply_fp64(self.h, sid, form, _p(x), _p(y)))
+        return y
+
     def defect(self, sid, x, f):
         x, f = _f64(x), _f64(f)
         d = np.zeros_like(x)

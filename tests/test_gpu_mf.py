@@ -1,6 +1,7 @@
-"""Direct tests of the FP32 operator forms the mixed multigrid cycle applies.
+"""Direct tests of the operator forms the mixed solve applies: the FP32 forms of its multigrid
+cycle and the matrix-free FP64 form of its FGMRES product.
 
-One product y = A x of each form through the C ABI (cdgpu_apply_fp32), against the FP64 CSR
+One product y = A x of each form through the C ABI (cdgpu_apply_fp32, cdgpu_apply_fp64), against the FP64 CSR
 product of the same assembled level (itself pinned to the reference by the golden and
 headline tests):
   form 0  the FP32 copy of the CSR entries,
@@ -66,6 +67,30 @@ def test_fp32_operator_forms(ctx, n, disc):
     assert abs(y[2][worst] - y64[worst]) <= 4e-3 * scale
 
 
+@pytest.mark.parametrize("n", [5, 27, 32])
+@pytest.mark.parametrize("disc", [GALERKIN, SUPG])
+def test_fp64_matrix_free_form(ctx, n, disc):
+    """The mixed solve's FGMRES product: the sum-factorised FP64 per-cell products (values and
+    gradients at the 3 x 3 x 3 Gauss points by one-dimensional passes) against the FP64 CSR
+    product of the same assembly (library and scipy), normwise 1e-14: the same matrix up to
+    rounding.  5^3 cells leave a partial 32-cell group; 27^3 and 32^3 give more groups than
+    the persistent grid has blocks."""
+    sp, sid, A = assembled(ctx, n, disc)
+    x = np.random.default_rng(7 * n + disc).uniform(-1, 1, sp["n_dof"])
+    y_csr = ctx.apply_fp64(sid, x, 0)
+    y_mf = ctx.apply_fp64(sid, x, 1)
+    y_ref = A @ x
+    scale = np.abs(abs(A) @ np.abs(x)).max()
+    na = sp["n_active"]
+    assert np.array_equal(y_mf[na:], x[na:]), "Dirichlet rows are identity rows"
+    err_csr = np.abs(y_mf - y_csr).max() / scale
+    err_ref = np.abs(y_mf - y_ref).max() / scale
+    print(f"n={n} disc={disc}: matrix-free vs CSR {err_csr:.2e}, vs scipy {err_ref:.2e}")
+    assert err_csr <= 1e-14 and err_ref <= 1e-14
+    # deterministic: the rows sum their cells in a fixed order
+    assert np.array_equal(ctx.apply_fp64(sid, x, 1), y_mf)
+
+
 def test_fp32_operator_forms_unsupported(ctx):
     """The matrix-free forms exist for Q2 hexahedra only; the CSR form for every space."""
     sp = mesh.structured_space(2, 1, 8)
@@ -78,4 +103,7 @@ def test_fp32_operator_forms_unsupported(ctx):
     assert np.isfinite(y).all()
     with pytest.raises(_lib.CdgpuError) as e:
         ctx.apply_fp32(sid, x, 2)
+    assert e.value.status == _lib.ERR_UNSUPPORTED
+    with pytest.raises(_lib.CdgpuError) as e:
+        ctx.apply_fp64(sid, x.astype(np.float64), 1)
     assert e.value.status == _lib.ERR_UNSUPPORTED
