@@ -587,19 +587,24 @@ __global__ void __launch_bounds__(256) local_quad_kernel(LocalArgs a)
 // local matrices and right-hand sides of affine cells from their reference-tensor
 // coefficients: A_c[i][j] = sum_t coef_{c,t} R_t[i][j], F_c[i] = sum_u coef_{c,T+u} r_u[i]
 // (a [cells x T] x [T x nbf^2] product).  Each thread owns one entry q of the local layout
-// and keeps its tensor column R_q in registers; blocks walk a range of cells, so the cell
-// coefficients are broadcast loads and the writes are coalesced.
+// and keeps its tensor column R_q in registers; blocks walk a range of cells whose
+// coefficients they first copy into shared memory with coalesced loads, so the loop over the
+// cells reads them as shared-memory broadcasts (no global-memory latency per cell) and the
+// writes are coalesced.  TM bounds the number of tensors at compile time (the exact count of
+// the common forms, so the loop carries no predicate; CD_MAXT for any other).
+template <int TM>
 __global__ void __launch_bounds__(256) affine_local_kernel(int n_cells, int nbf, int T, int Tr,
                                                            const double *__restrict__ cellcoef,
                                                            const double *__restrict__ R,
                                                            const double *__restrict__ r, double *__restrict__ out,
                                                            int cells_per_block)
 {
+  extern __shared__ double cf_s[]; // cells_per_block x (T + Tr)
   CD_PDL_ENTRY();
   const int per = nbf * nbf + nbf;
   const int q = blockIdx.y * blockDim.x + threadIdx.x;
   const bool act = q < per;
-  double Rq[CD_MAXT];
+  double Rq[TM];
   int nt = 0, off = T;
   if (act)
   {
@@ -608,25 +613,36 @@ __global__ void __launch_bounds__(256) affine_local_kernel(int n_cells, int nbf,
       nt = T;
       off = 0;
 #pragma unroll
-      for (int u = 0; u < CD_MAXT; u++) Rq[u] = u < T ? R[(size_t)q * T + u] : 0.0;
+      for (int u = 0; u < TM; u++) Rq[u] = u < T ? R[(size_t)q * T + u] : 0.0;
     }
     else
     {
       nt = Tr;
       const int i = q - nbf * nbf;
 #pragma unroll
-      for (int u = 0; u < CD_MAXT; u++) Rq[u] = u < Tr ? r[i * Tr + u] : 0.0;
+      for (int u = 0; u < TM; u++) Rq[u] = u < Tr ? r[i * Tr + u] : 0.0;
     }
   }
   const int c0 = blockIdx.x * cells_per_block, c1 = min(n_cells, c0 + cells_per_block);
+  const int TT = T + Tr;
+  for (int e = threadIdx.x; e < (c1 - c0) * TT; e += blockDim.x) cf_s[e] = __ldg(cellcoef + (size_t)c0 * TT + e);
+  __syncthreads();
+  if (!act) return;
   for (int c = c0; c < c1; c++)
   {
-    if (!act) continue;
-    const double *cf = cellcoef + (size_t)c * (T + Tr) + off;
+    const double *cf = cf_s + (c - c0) * TT + off;
     double v = 0.0;
+    if (nt == TM)
+    {
 #pragma unroll
-    for (int u = 0; u < CD_MAXT; u++)
-      if (u < nt) v += __ldg(cf + u) * Rq[u];
+      for (int u = 0; u < TM; u++) v += cf[u] * Rq[u];
+    }
+    else
+    {
+#pragma unroll
+      for (int u = 0; u < TM; u++)
+        if (u < nt) v += cf[u] * Rq[u];
+    }
     out[(size_t)c * per + q] = v;
   }
 }
@@ -755,6 +771,141 @@ __global__ void __launch_bounds__(256) row_gather_kernel(GatherArgs p)
   }
 }
 
+// Row gather of an element with NBF <= 32 local DOFs (Q2 hexahedra): one warp per row, lane j =
+// local column j.  Each warp owns a contiguous range of at most kGatherRows rows; it first
+// copies the range's CSR and incidence pointers and its incidence entries (contiguous in the
+// incidence array) into shared memory with coalesced loads, so a row costs one level of global
+// loads: the local-matrix rows and slot-map rows of all its incidences (up to CH at once),
+// then the sum into the shared-memory row in ascending cell order (the order of the plain
+// gather: the entries are the same bit for bit) and the write.  The diagonal's position comes
+// from the slot map (the row's own local column), so column indices are read only for
+// Dirichlet rows.  Incidences beyond the first CH, or beyond the staged ones, are loaded and
+// added one by one after them.
+constexpr int kGatherRows = 64, kGatherInc = 512;
+
+template <int NBF, int MAXROW>
+__global__ void __launch_bounds__(256, 4) row_gather_lean_kernel(GatherArgs p, int rows_per_warp)
+{
+  CD_PDL_ENTRY();
+  static_assert(NBF <= 32, "one lane per local column");
+  constexpr int CH = 8, PER = NBF * NBF + NBF, NW = 8;
+  __shared__ double acc_s[NW][MAXROW];
+  __shared__ int rp_s[NW][kGatherRows + 1], ip_s[NW][kGatherRows + 1], e_s[NW][kGatherInc];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double *acc = acc_s[w];
+  const int r0 = (blockIdx.x * NW + w) * rows_per_warp, nrows = min(p.n_dof - r0, rows_per_warp);
+  if (nrows <= 0) return; // warp-uniform
+  const bool col = lane < NBF;
+  for (int k = lane; k <= nrows; k += 32)
+  {
+    rp_s[w][k] = __ldg(p.row_ptr + r0 + k);
+    ip_s[w][k] = __ldg(p.inc_ptr + r0 + k);
+  }
+  __syncwarp();
+  const int T0 = ip_s[w][0], n_staged = min(ip_s[w][nrows] - T0, kGatherInc);
+  for (int t = lane; t < n_staged; t += 32) e_s[w][t] = __ldg(p.inc + T0 + t);
+  __syncwarp();
+  auto entry = [&](int t) { return t - T0 < n_staged ? e_s[w][t - T0] : __ldg(p.inc + t); };
+  for (int k = 0; k < nrows; k++)
+  {
+    const int r = r0 + k, base = rp_s[w][k], len = rp_s[w][k + 1] - base;
+    const int t0 = ip_s[w][k], nt = ip_s[w][k + 1] - t0;
+    if (r >= p.n_active)
+    {
+      // Dirichlet row: identity row (Assemble2D.C:512, AssembleMat3D.C:811-816)
+      for (int s = lane; s < len; s += 32)
+      {
+        const bool d = p.kcol[base + s] == r;
+        p.a[base + s] = d ? 1.0 : 0.0;
+        if (p.a32) p.a32[base + s] = d ? 1.0f : 0.0f;
+      }
+      if (lane == 0)
+      {
+        p.rhs[r] = p.dir ? p.dir[r - p.n_active] : 0.0;
+        p.diag[r] = 1.0;
+        if (p.diag32) p.diag32[r] = 1.0f;
+      }
+      continue;
+    }
+    if (len > MAXROW)
+    {
+      if (lane == 0) atomicExch(p.err, 2);
+      continue;
+    }
+    const int n1 = min(nt, CH);
+    // every load of the row's first CH incidences at once
+    double v[CH];
+    int sl[CH];
+#pragma unroll
+    for (int q = 0; q < CH; q++)
+    {
+      v[q] = 0.0;
+      sl[q] = 0;
+      if (q < n1 && col)
+      {
+        const int eq = entry(t0 + q), K = eq / NBF, li = eq - K * NBF;
+        v[q] = __ldg(p.local + (size_t)K * PER + li * NBF + lane);
+        sl[q] = __ldg(p.slot + (size_t)(t0 + q) * NBF + lane);
+      }
+    }
+    double F = 0.0; // lane q: the local right-hand side of incidence q
+    int e_lane = 0;
+    if (lane < n1)
+    {
+      e_lane = entry(t0 + lane);
+      const int K = e_lane / NBF, li = e_lane - K * NBF;
+      F = __ldg(p.local + (size_t)K * PER + NBF * NBF + li);
+    }
+    for (int s = lane; s < len; s += 32) acc[s] = 0.0;
+    __syncwarp();
+    double racc = 0.0;
+#pragma unroll
+    for (int q = 0; q < CH; q++)
+      if (q < n1)
+      {
+        if (col)
+        {
+          if (sl[q] >= len) atomicExch(p.err, 1);
+          else acc[sl[q]] += v[q];
+        }
+        racc += __shfl_sync(0xffffffffu, F, q);
+        __syncwarp();
+      }
+    for (int t = t0 + CH; t < t0 + nt; t++)
+    {
+      const int eq = entry(t), K = eq / NBF, li = eq - K * NBF;
+      if (col)
+      {
+        const double vv = __ldg(p.local + (size_t)K * PER + li * NBF + lane);
+        const int ss = __ldg(p.slot + (size_t)t * NBF + lane);
+        if (ss >= len) atomicExch(p.err, 1);
+        else acc[ss] += vv;
+      }
+      racc += __ldg(p.local + (size_t)K * PER + NBF * NBF + li);
+      __syncwarp();
+    }
+    // the diagonal: the slot of the row's own local column in its first incidence
+    const int e0 = __shfl_sync(0xffffffffu, e_lane, 0), li0 = e0 - (e0 / NBF) * NBF;
+    const int dslot = __shfl_sync(0xffffffffu, sl[0], li0);
+    for (int s = lane; s < len; s += 32)
+    {
+      const double x = acc[s];
+      p.a[base + s] = x;
+      if (p.a32) p.a32[base + s] = (float)x;
+    }
+    if (lane == 0)
+    {
+      p.rhs[r] = racc;
+      if (n1 > 0 && dslot < len)
+      {
+        p.diag[r] = acc[dslot];
+        if (p.diag32) p.diag32[r] = (float)acc[dslot];
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // slot map: for every incidence t of an active row and local column j, the position of the
 // column within the row (binary search, once per pattern); 255 and the error flag when the
 // coupling is missing from the pattern
@@ -823,6 +974,18 @@ static int launch_gather(cdgpu_ctx *ctx, const GatherArgs &g, int n_dof)
   long grid = std::min<long>(need, (long)ctx->sm_count * blocks_per_sm);
   if (grid < 1) grid = 1;
   (void)cd_launch(row_gather_kernel<GS, MAXROW>, (int)grid, 256, sm, ctx->stream, g);
+  CD_LAUNCHED(ctx);
+  return CDGPU_OK;
+}
+
+template <int NBF, int MAXROW> static int launch_gather_lean(cdgpu_ctx *ctx, const GatherArgs &g, int n_dof)
+{
+  // about four blocks of 8 warps per SM, every warp a contiguous range of at most kGatherRows rows
+  const long warps = (long)ctx->sm_count * 4 * 8;
+  const int rows_per_warp = (int)std::min<long>(kGatherRows, std::max<long>(1, (n_dof + warps - 1) / warps));
+  const long need = ((long)n_dof + rows_per_warp - 1) / rows_per_warp;
+  const int grid = (int)std::max<long>(1, (need + 7) / 8);
+  (void)cd_launch(row_gather_lean_kernel<NBF, MAXROW>, grid, 256, 0, ctx->stream, g, rows_per_warp);
   CD_LAUNCHED(ctx);
   return CDGPU_OK;
 }
@@ -1128,9 +1291,13 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, 
       return rc;
     const int per = s.nbf * s.nbf + s.nbf;
     const int qblocks = (per + 255) / 256;
-    const int cpb = std::max(1, (int)((long)s.n_cells * qblocks / ((long)ctx->sm_count * 8)));
+    // cells per block: about 8 blocks per SM, at most 256 (their coefficients in shared memory)
+    const int cpb = std::max(1, std::min(256, (int)((long)s.n_cells * qblocks / ((long)ctx->sm_count * 8))));
     dim3 grid((s.n_cells + cpb - 1) / cpb, qblocks);
-    (void)cd_launch(affine_local_kernel, grid, 256, 0, ctx->stream, s.n_cells, s.nbf, T, Tr, s.d_cellcoef, s.d_ref,
+    const size_t cf_bytes = sizeof(double) * (size_t)cpb * (T + Tr);
+    auto kern = T == 10 ? affine_local_kernel<10> : T == 13 ? affine_local_kernel<13> : T == 6 ? affine_local_kernel<6>
+              : T == 14 ? affine_local_kernel<14> : affine_local_kernel<CD_MAXT>;
+    (void)cd_launch(kern, grid, 256, cf_bytes, ctx->stream, s.n_cells, s.nbf, T, Tr, s.d_cellcoef, s.d_ref,
                                                        s.d_ref + (size_t)s.nbf * s.nbf * T, s.d_local, cpb);
     CD_LAUNCHED(ctx);
   }
@@ -1177,6 +1344,7 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, 
   if (s.dim == 2 && s.order == 1) rc = launch_gather<4, 16>(ctx, g, s.n_dof);
   else if (s.dim == 2) rc = launch_gather<16, 32>(ctx, g, s.n_dof);
   else if (s.order == 1) rc = launch_gather<8, 32>(ctx, g, s.n_dof);
+  else if (s.nbf == 27) rc = launch_gather_lean<27, CD_MAXROW>(ctx, g, s.n_dof);
   else rc = launch_gather<32, CD_MAXROW>(ctx, g, s.n_dof);
   if (rc) return rc;
   s.assembled = true;

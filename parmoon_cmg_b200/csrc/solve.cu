@@ -1607,16 +1607,15 @@ int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const 
   if (p.coarse_smoother != 17 && h.lev[0].sp->n_dof > 6000)
     return fail(ctx, CDGPU_ERR_UNSUPPORTED, "solve: coarse smoother loop needs a coarsest level below 6000 DOFs");
   int rc;
-  if ((rc = tune_tma(ctx, *h.lev.back().sp))) return rc; // once per pattern, before any capture
+  // the mixed form applies the finest operator of its FGMRES iteration matrix-free in FP64 on
+  // levels large enough for the per-cell form to pay off; the FP64 form keeps the CSR entries,
+  // whose bulk-copy kernels are tuned once per pattern, before any capture
+  Space &fs = *h.lev.back().sp;
+  h.mf64 = p.precision == 1 && use_mf64(fs) && fs.n_cells >= kMfMinCells;
+  if (h.mf64 && (rc = ensure_mf64(ctx, fs))) return rc;
+  if (!h.mf64 && (rc = tune_tma(ctx, fs))) return rc;
   if (p.coarse_smoother == 17 && (rc = refresh_coarse_inverse(ctx, h))) return rc;
   if (p.precision == 1 && (rc = refresh_mf(ctx, h))) return rc;
-  // the mixed form applies the finest operator of its FGMRES iteration matrix-free in FP64 on
-  // levels large enough for the per-cell form to pay off; the FP64 form keeps the CSR entries
-  {
-    Space &fs = *h.lev.back().sp;
-    h.mf64 = p.precision == 1 && use_mf64(fs) && fs.n_cells >= kMfMinCells;
-    if (h.mf64 && (rc = ensure_mf64(ctx, fs))) return rc;
-  }
   cdgpu_solve_info local{};
   if (!info) info = &local;
   if (p.solver == 11) rc = fixed_point(ctx, h, p, d_rhs, d_sol, info);
