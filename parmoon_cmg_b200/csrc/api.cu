@@ -78,6 +78,9 @@ static void free_mg(Hierarchy *h)
   for (auto &e : h->ev_ready)
     if (e) cudaEventDestroy(e);
   if (h->ev_beta) cudaEventDestroy(h->ev_beta);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
+  if (h->astream) cudaStreamDestroy(h->astream);
   if (h->cstream) cudaStreamDestroy(h->cstream);
   delete h;
 }
@@ -730,15 +733,35 @@ int cdgpu_assemble_hierarchy(cdgpu_ctx *ctx, int mg_id, int disctype, int coarse
   if (!h) return fail(ctx, CDGPU_ERR_INVALID, "assemble_hierarchy: bad id");
   cudaSetDevice(ctx->device);
   bool need_check = false;
-  for (size_t l = 0; l < h->lev.size(); l++)
+  for (auto &L : h->lev) need_check = need_check || !L.sp->pattern_checked;
+  const size_t nl = h->lev.size();
+  int rc = CDGPU_OK;
+  // The levels are independent: the coarse ones are assembled on the hierarchy's side stream
+  // beside the finest one, and so is the exact coarse inverse once a solve has used it (it
+  // depends on the coarsest level only); the stream of the context waits for both at the end.
+  if (nl > 1)
   {
-    int d = l + 1 == h->lev.size() ? disctype : coarse_disctype;
-    int rc = assemble_space(ctx, *h->lev[l].sp, d, nullptr, false);
+    if (!h->astream)
+    {
+      CD_CUDA(ctx, cudaStreamCreateWithFlags(&h->astream, cudaStreamNonBlocking));
+      CD_CUDA(ctx, cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+      CD_CUDA(ctx, cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+    }
+    CD_CUDA(ctx, cudaEventRecord(h->ev_fork, ctx->stream));
+    CD_CUDA(ctx, cudaStreamWaitEvent(h->astream, h->ev_fork, 0));
+    cudaStream_t main_stream = ctx->stream;
+    ctx->stream = h->astream;
+    for (size_t l = 0; l + 1 < nl && !rc; l++) rc = assemble_space(ctx, *h->lev[l].sp, coarse_disctype, nullptr, false);
+    if (!rc && h->d_cinv) rc = refresh_coarse_inverse(ctx, *h);
+    ctx->stream = main_stream;
     if (rc) return rc;
-    need_check = need_check || !h->lev[l].sp->pattern_checked;
+    CD_CUDA(ctx, cudaEventRecord(h->ev_join, h->astream));
   }
+  rc = assemble_space(ctx, *h->lev[nl - 1].sp, disctype, nullptr, false);
+  if (nl > 1) CD_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, h->ev_join, 0));
+  if (rc) return rc;
   if (!need_check) return CDGPU_OK; // the checks depend on the patterns only
-  int rc = assemble_check(ctx);
+  rc = assemble_check(ctx);
   if (!rc)
     for (auto &L : h->lev) L.sp->pattern_checked = true;
   return rc;

@@ -16,6 +16,7 @@
 //     (cell_coef_kernel) and the row kernel evaluates local entries on the fly;
 //   * quadrature path: local matrices by Gauss quadrature with the reference's
 //     per-point formulas (local_quad_kernel), stored and then gathered.
+#include <climits>
 #include <cooperative_groups.h>
 
 #include <cmath>
@@ -790,7 +791,9 @@ __global__ void __launch_bounds__(256, 4) row_gather_lean_kernel(GatherArgs p, i
   static_assert(NBF <= 32, "one lane per local column");
   constexpr int CH = 8, PER = NBF * NBF + NBF, NW = 8;
   __shared__ double acc_s[NW][MAXROW];
-  __shared__ int rp_s[NW][kGatherRows + 1], ip_s[NW][kGatherRows + 1], e_s[NW][kGatherInc];
+  // per staged incidence: its entry (cell * NBF + local row) and the offset of its local-matrix
+  // row in the local array (cell * PER + local row * NBF)
+  __shared__ int rp_s[NW][kGatherRows + 1], ip_s[NW][kGatherRows + 1], e_s[NW][kGatherInc], o_s[NW][kGatherInc];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double *acc = acc_s[w];
   const int r0 = (blockIdx.x * NW + w) * rows_per_warp, nrows = min(p.n_dof - r0, rows_per_warp);
@@ -803,9 +806,19 @@ __global__ void __launch_bounds__(256, 4) row_gather_lean_kernel(GatherArgs p, i
   }
   __syncwarp();
   const int T0 = ip_s[w][0], n_staged = min(ip_s[w][nrows] - T0, kGatherInc);
-  for (int t = lane; t < n_staged; t += 32) e_s[w][t] = __ldg(p.inc + T0 + t);
+  for (int t = lane; t < n_staged; t += 32)
+  {
+    const int e = __ldg(p.inc + T0 + t), K = e / NBF, li = e - K * NBF;
+    e_s[w][t] = e;
+    o_s[w][t] = K * PER + li * NBF;
+  }
   __syncwarp();
   auto entry = [&](int t) { return t - T0 < n_staged ? e_s[w][t - T0] : __ldg(p.inc + t); };
+  auto local_row = [&](int t) {
+    if (t - T0 < n_staged) return p.local + o_s[w][t - T0];
+    const int e = __ldg(p.inc + t), K = e / NBF;
+    return p.local + (size_t)K * PER + (e - K * NBF) * NBF;
+  };
   for (int k = 0; k < nrows; k++)
   {
     const int r = r0 + k, base = rp_s[w][k], len = rp_s[w][k + 1] - base;
@@ -836,6 +849,7 @@ __global__ void __launch_bounds__(256, 4) row_gather_lean_kernel(GatherArgs p, i
     // every load of the row's first CH incidences at once
     double v[CH];
     int sl[CH];
+    const unsigned char *srow = p.slot + (size_t)t0 * NBF + lane;
 #pragma unroll
     for (int q = 0; q < CH; q++)
     {
@@ -843,9 +857,8 @@ __global__ void __launch_bounds__(256, 4) row_gather_lean_kernel(GatherArgs p, i
       sl[q] = 0;
       if (q < n1 && col)
       {
-        const int eq = entry(t0 + q), K = eq / NBF, li = eq - K * NBF;
-        v[q] = __ldg(p.local + (size_t)K * PER + li * NBF + lane);
-        sl[q] = __ldg(p.slot + (size_t)(t0 + q) * NBF + lane);
+        v[q] = __ldg(local_row(t0 + q) + lane);
+        sl[q] = __ldg(srow + q * NBF);
       }
     }
     double F = 0.0; // lane q: the local right-hand side of incidence q
@@ -1344,7 +1357,9 @@ int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, 
   if (s.dim == 2 && s.order == 1) rc = launch_gather<4, 16>(ctx, g, s.n_dof);
   else if (s.dim == 2) rc = launch_gather<16, 32>(ctx, g, s.n_dof);
   else if (s.order == 1) rc = launch_gather<8, 32>(ctx, g, s.n_dof);
-  else if (s.nbf == 27) rc = launch_gather_lean<27, CD_MAXROW>(ctx, g, s.n_dof);
+  // (the lean gather keeps local-matrix offsets as 32-bit integers)
+  else if (s.nbf == 27 && (long)s.n_cells * (27 * 27 + 27) < (long)INT_MAX)
+    rc = launch_gather_lean<27, CD_MAXROW>(ctx, g, s.n_dof);
   else rc = launch_gather<32, CD_MAXROW>(ctx, g, s.n_dof);
   if (rc) return rc;
   s.assembled = true;

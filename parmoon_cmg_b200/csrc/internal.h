@@ -172,6 +172,10 @@ struct Hierarchy
   // (ev_ready) and beside the rest of the iteration; ev_beta: the initial residual's copy
   cudaStream_t cstream = nullptr;
   cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_beta = nullptr;
+  // side stream of the hierarchy's assembly: the coarse levels (and the exact coarse inverse,
+  // once a solve has used it) are assembled there beside the finest level
+  cudaStream_t astream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int *h_cflag = nullptr;     // pinned copy of the coarse inversion's zero-pivot flag
   bool cflag_pending = false; // copy enqueued, not yet checked
   unsigned *d_gs_count = nullptr; // arrival counter of the Gram-Schmidt passes' last-block reduction
@@ -311,6 +315,9 @@ int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const 
               double *d_sol, cdgpu_solve_info *info);
 int apply_fp32_form(cdgpu_ctx *ctx, Space &s, int form, const float *d_x, float *d_y);
 int apply_fp64_form(cdgpu_ctx *ctx, Space &s, int form, const double *d_x, double *d_y);
+// the explicit inverse of the coarsest level's matrix for the exact coarse solve, when its
+// assembly changed since the last inversion (enqueued on ctx->stream)
+int refresh_coarse_inverse(cdgpu_ctx *ctx, Hierarchy &h);
 // the CSR pattern built on the device (pattern.cu)
 int build_pattern_device(cdgpu_ctx *ctx, Space &s, int **d_kcol_out, bool *fallback);
 // tiles of the TMA product for a freshly installed pattern (solve.cu)

@@ -1134,7 +1134,7 @@ __global__ void __launch_bounds__(1024) gj_invert_kernel(int n, double *__restri
     for (int i = t; i < n * n; i += nt) g[i] = A[i];
 }
 
-static int refresh_coarse_inverse(cdgpu_ctx *ctx, Hierarchy &h)
+int refresh_coarse_inverse(cdgpu_ctx *ctx, Hierarchy &h)
 {
   Space &s = *h.lev[0].sp;
   if (h.d_cinv && h.cinv_version == s.assembly_version) return CDGPU_OK;
