@@ -46,7 +46,7 @@ static void free_space(Space *s)
   void *ptrs[] = {s->d_coords, s->d_gn,  s->d_row_ptr, s->d_kcol,     s->d_dir_start, s->d_dir_rows, s->d_slot, s->d_inc_ptr, s->d_tiles,
                   s->d_inc,    s->d_a,   s->d_rhs,     s->d_diag,     s->d_a32,       s->d_diag32,
                   s->d_tab,    s->d_cellcoef, s->d_local, s->d_dir, s->d_ref, s->d_quadtab,
-                  s->d_cf32,   s->d_R32, s->d_R32img, s->d_ybuf, s->d_ybuf64};
+                  s->d_cf32,   s->d_R32, s->d_R32img, s->d_ybuf, s->d_ybuf64, s->d_inc8};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete s;

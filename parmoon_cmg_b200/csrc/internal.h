@@ -106,6 +106,10 @@ struct Space
   // before reading the cell data (later launches of that assembly may read it before the wait)
   double *d_ybuf64 = nullptr;
   mutable long mf64_safe_version = -1;
+  // the active rows' incidences as 8-wide records of per-cell-buffer indices (mf.cuh,
+  // mf_inc8_kernel); null when not built or when a row has more than 8 cells
+  int *d_inc8 = nullptr;
+  bool inc8_tried = false;
   double *d_local = nullptr;    // quadrature path: n_cells x (nbf*nbf + nbf)
   double *d_dir = nullptr;      // Dirichlet values
   double *d_ref = nullptr;      // reference tensors (affine path)

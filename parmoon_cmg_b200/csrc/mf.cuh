@@ -489,6 +489,68 @@ __global__ void mf_row_kernel(int n, int na, int n_cells, const int *__restrict_
   out[r] = MODE == MF_JACOBI ? x[r] + omega * (f[r] - s) / diag[r] : MODE == MF_DEFECT ? f[r] - s : s;
 }
 
+// The DOF -> (cell, local index) incidence of every active row as up to 8 indices into the
+// per-cell buffer, li * n_cells + cell, in ascending cell order and padded with -1: the row
+// kernels then read one 32-byte record per row instead of the row's incidence pointers and,
+// after them, its entries (one dependent load fewer).  Rows with more than 8 cells raise
+// *overflow, and the space keeps the incidence lists.
+__global__ void mf_inc8_kernel(int n_active, int nbf, int n_cells, const int *__restrict__ inc_ptr,
+                               const int *__restrict__ inc, int *__restrict__ inc8, int *overflow)
+{
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_active) return;
+  const int b = inc_ptr[r], e = inc_ptr[r + 1];
+  if (e - b > 8) atomicExch(overflow, 1);
+#pragma unroll
+  for (int j = 0; j < 8; j++)
+  {
+    int v = -1;
+    if (b + j < e)
+    {
+      const int t = inc[b + j], K = t / nbf, li = t - K * nbf;
+      v = li * n_cells + K;
+    }
+    inc8[(size_t)r * 8 + j] = v;
+  }
+}
+
+// mf_row_kernel with the 8-wide incidence records (same sums in the same order)
+template <int MODE>
+__global__ void mf_row8_kernel(int n, int na, const int *__restrict__ inc8, const float *__restrict__ ybuf,
+                               const float *__restrict__ x, const float *__restrict__ f,
+                               const float *__restrict__ diag, float *__restrict__ out, float omega, int pre)
+{
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  int4 i0 = make_int4(-1, -1, -1, -1), i1 = i0;
+  if (pre && r < na)
+  {
+    i0 = __ldg((const int4 *)(inc8 + (size_t)r * 8));
+    i1 = __ldg((const int4 *)(inc8 + (size_t)r * 8) + 1);
+  }
+  CD_PDL_ENTRY();
+  if (r >= na)
+  {
+    // Dirichlet rows are identity rows
+    out[r] = MODE == MF_JACOBI ? f[r] : MODE == MF_DEFECT ? f[r] - x[r] : x[r];
+    return;
+  }
+  if (!pre)
+  {
+    i0 = __ldg((const int4 *)(inc8 + (size_t)r * 8));
+    i1 = __ldg((const int4 *)(inc8 + (size_t)r * 8) + 1);
+  }
+  const int ix[8] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y, i1.z, i1.w};
+  float yv[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) yv[j] = ix[j] >= 0 ? __ldg(ybuf + ix[j]) : 0.f;
+  float s = 0.f;
+#pragma unroll
+  for (int j = 0; j < 8; j++)
+    if (ix[j] >= 0) s += yv[j];
+  out[r] = MODE == MF_JACOBI ? x[r] + omega * (f[r] - s) / diag[r] : MODE == MF_DEFECT ? f[r] - s : s;
+}
+
 // FP32 copies of the cell coefficients (first T of each cell's T + Tr) and of the tensors
 // R[(i*nbf + j)*T + t] -> R32[(t*nbf + i)*nbf + j]
 __global__ void mf_convert_kernel(int n_cells, int T, int Tr, int nbf, const double *__restrict__ cellcoef,
@@ -566,6 +628,12 @@ inline void mf_rows(cdgpu_ctx *ctx, const Space &s, const float *x, const float 
                     float omega)
 {
   const int grid = (s.n_dof + 255) / 256;
+  if (s.d_inc8)
+  {
+    (void)cd_launch(mf_row8_kernel<MODE>, grid, 256, 0, ctx->stream, s.n_dof, s.n_active, (const int *)s.d_inc8,
+                    (const float *)s.d_ybuf, x, f, diag, out, omega, ctx->pdl_pre ? 1 : 0);
+    return;
+  }
   switch (s.nbf)
   {
     case 27: (void)cd_launch(mf_row_kernel<27, MODE>, grid, 256, 0, ctx->stream, s.n_dof, s.n_active, s.n_cells, s.d_inc_ptr, s.d_inc, s.d_ybuf, x, f, diag, out, omega, ctx->pdl_pre ? 1 : 0); break;
