@@ -221,9 +221,12 @@ enum { MF64_SPMV = 0, MF64_DEFECT = 1 };
 // y = sum over a DOF's cells of their contributions (ascending cell order), or d = f - y;
 // Dirichlet rows: y = x, d = f - x.  With partial (defect form), per-block sums of d^2 over
 // all rows, as the CSR defect leaves them.  Grid-stride over rows.
+// With inc8 (the 8-wide incidence records of mf_inc8_kernel) a row reads one record and then
+// its cells' contributions; without, its incidence pointers and entries.
 template <int MODE>
 __global__ void __launch_bounds__(256) mf64_row_kernel(int n, int na, int n_cells, const int *__restrict__ inc_ptr,
-                                                       const int *__restrict__ inc, const double *__restrict__ ybuf,
+                                                       const int *__restrict__ inc, const int *__restrict__ inc8,
+                                                       const double *__restrict__ ybuf,
                                                        const double *__restrict__ x, const double *__restrict__ f,
                                                        double *__restrict__ out, double *__restrict__ partial)
 {
@@ -234,6 +237,18 @@ __global__ void __launch_bounds__(256) mf64_row_kernel(int n, int na, int n_cell
     double s;
     if (r >= na)
       s = x[r];
+    else if (inc8)
+    {
+      const int4 i0 = __ldg((const int4 *)(inc8 + (size_t)r * 8)), i1 = __ldg((const int4 *)(inc8 + (size_t)r * 8) + 1);
+      const int ix[8] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y, i1.z, i1.w};
+      double yv[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) yv[j] = ix[j] >= 0 ? ybuf[ix[j]] : 0.0;
+      s = 0;
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        if (ix[j] >= 0) s += yv[j];
+    }
     else
     {
       const int b = inc_ptr[r], e = inc_ptr[r + 1];

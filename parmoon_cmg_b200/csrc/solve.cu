@@ -18,6 +18,7 @@
 // (two fused passes over the basis) instead of modified Gram-Schmidt (one kernel
 // launch per basis vector).  Both are accurate to working precision; iterates
 // differ from the reference's by rounding only.
+#include <climits>
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -264,46 +265,14 @@ __global__ void coarse_smooth_kernel(int n, int n_active, const int *__restrict_
 // partial[block * 33 + slot] and are summed in block order by the pass's last block.
 enum { GS_DOTS = 0, GS_AXPY_DOTS = 1, GS_AXPY_NORM = 2 };
 
-// The last block to finish (an arrival counter, reset by that block) sums the per-block
-// partials of every slot in block order into out[slot] (lanes over blocks, then a fixed
-// warp tree), so no separate reduction kernel is launched.
-template <int K, int MODE>
-__global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, const double *__restrict__ Y,
-                                                         double *__restrict__ w,
-                                                         const double *__restrict__ coef,
-                                                         double *__restrict__ partial,
-                                                         double *__restrict__ out, unsigned *__restrict__ counter)
+// Block partials of NS sums and their reduction by the last block to arrive (an arrival
+// counter, reset by that block): partial[block * 33 + slot], then out[slot] summed in block
+// order (lanes over blocks, then a fixed warp tree).  Every thread of the block calls it.
+template <int NS>
+__device__ __forceinline__ void gs_reduce(const double (&acc)[NS], double *__restrict__ partial,
+                                          double *__restrict__ out, unsigned *__restrict__ counter)
 {
-  CD_PDL_ENTRY();
-  constexpr int NS = MODE == GS_AXPY_NORM ? 1 : K;
   __shared__ double red[kBlock / 32][NS];
-  double acc[NS];
-#pragma unroll
-  for (int j = 0; j < NS; j++) acc[j] = 0;
-  double cf[K];
-#pragma unroll
-  for (int j = 0; j < K; j++) cf[j] = MODE == GS_DOTS ? 0.0 : coef[j];
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-  {
-    double y[K];
-#pragma unroll
-    for (int j = 0; j < K; j++) y[j] = __ldg(Y + (size_t)j * n + i);
-    double wi = w[i];
-    if (MODE != GS_DOTS)
-    {
-#pragma unroll
-      for (int j = 0; j < K; j++) wi -= cf[j] * y[j];
-      w[i] = wi;
-    }
-    if (MODE == GS_AXPY_NORM)
-      acc[0] += wi * wi;
-    else
-    {
-#pragma unroll
-      for (int j = 0; j < K; j++) acc[j] += wi * y[j];
-    }
-  }
   const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
 #pragma unroll
   for (int j = 0; j < NS; j++)
@@ -348,6 +317,45 @@ __global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, const double *__
   if (threadIdx.x == 0) *counter = 0u;
 }
 
+template <int K, int MODE>
+__global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, const double *__restrict__ Y,
+                                                         double *__restrict__ w,
+                                                         const double *__restrict__ coef,
+                                                         double *__restrict__ partial,
+                                                         double *__restrict__ out, unsigned *__restrict__ counter)
+{
+  CD_PDL_ENTRY();
+  constexpr int NS = MODE == GS_AXPY_NORM ? 1 : K;
+  double acc[NS];
+#pragma unroll
+  for (int j = 0; j < NS; j++) acc[j] = 0;
+  double cf[K];
+#pragma unroll
+  for (int j = 0; j < K; j++) cf[j] = MODE == GS_DOTS ? 0.0 : coef[j];
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+  {
+    double y[K];
+#pragma unroll
+    for (int j = 0; j < K; j++) y[j] = __ldg(Y + (size_t)j * n + i);
+    double wi = w[i];
+    if (MODE != GS_DOTS)
+    {
+#pragma unroll
+      for (int j = 0; j < K; j++) wi -= cf[j] * y[j];
+      w[i] = wi;
+    }
+    if (MODE == GS_AXPY_NORM)
+      acc[0] += wi * wi;
+    else
+    {
+#pragma unroll
+      for (int j = 0; j < K; j++) acc[j] += wi * y[j];
+    }
+  }
+  gs_reduce<NS>(acc, partial, out, counter);
+}
+
 template <int MODE>
 static void launch_gs(int k, int grid, cudaStream_t st, int n, const double *Y, double *w, const double *coef,
                       double *partial, double *out, unsigned *counter)
@@ -361,6 +369,64 @@ static void launch_gs(int k, int grid, cudaStream_t st, int n, const double *Y, 
     CD_GS_CASE(22) CD_GS_CASE(23) CD_GS_CASE(24) CD_GS_CASE(25) CD_GS_CASE(26) CD_GS_CASE(27) CD_GS_CASE(28)
     CD_GS_CASE(29) CD_GS_CASE(30) CD_GS_CASE(31) CD_GS_CASE(32)
 #undef CD_GS_CASE
+    default: break;
+  }
+}
+
+// Phase 2 of the matrix-free FP64 product fused with the first Gram-Schmidt pass: w = A x from
+// the per-cell products (8-wide incidence records, ascending cell order; Dirichlet rows w = x)
+// and the partial dots w . Y_j of the K basis vectors, reduced like a GS_DOTS pass.
+template <int K>
+__global__ void __launch_bounds__(kBlock) mf64_row_dots_kernel(int n, int na, const int *__restrict__ inc8,
+                                                               const double *__restrict__ ybuf,
+                                                               const double *__restrict__ x, double *__restrict__ w,
+                                                               const double *__restrict__ Y, double *__restrict__ partial,
+                                                               double *__restrict__ out, unsigned *__restrict__ counter)
+{
+  CD_PDL_ENTRY();
+  double acc[K];
+#pragma unroll
+  for (int j = 0; j < K; j++) acc[j] = 0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+  {
+    double y[K];
+#pragma unroll
+    for (int j = 0; j < K; j++) y[j] = __ldg(Y + (size_t)j * n + r);
+    double s;
+    if (r >= na)
+      s = x[r];
+    else
+    {
+      const int4 i0 = __ldg((const int4 *)(inc8 + (size_t)r * 8)), i1 = __ldg((const int4 *)(inc8 + (size_t)r * 8) + 1);
+      const int ix[8] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y, i1.z, i1.w};
+      double yv[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) yv[j] = ix[j] >= 0 ? ybuf[ix[j]] : 0.0;
+      s = 0;
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        if (ix[j] >= 0) s += yv[j];
+    }
+    w[r] = s;
+#pragma unroll
+    for (int j = 0; j < K; j++) acc[j] += s * y[j];
+  }
+  gs_reduce<K>(acc, partial, out, counter);
+}
+
+static void launch_row_dots(int k, int grid, cudaStream_t st, int n, int na, const int *inc8, const double *ybuf,
+                            const double *x, double *w, const double *Y, double *partial, double *out,
+                            unsigned *counter)
+{
+  switch (k)
+  {
+#define CD_RD_CASE(K) case K: (void)cd_launch(mf64_row_dots_kernel<K>, grid, kBlock, 0, st, n, na, inc8, ybuf, x, w, Y, partial, out, counter); break;
+    CD_RD_CASE(1) CD_RD_CASE(2) CD_RD_CASE(3) CD_RD_CASE(4) CD_RD_CASE(5) CD_RD_CASE(6) CD_RD_CASE(7)
+    CD_RD_CASE(8) CD_RD_CASE(9) CD_RD_CASE(10) CD_RD_CASE(11) CD_RD_CASE(12) CD_RD_CASE(13) CD_RD_CASE(14)
+    CD_RD_CASE(15) CD_RD_CASE(16) CD_RD_CASE(17) CD_RD_CASE(18) CD_RD_CASE(19) CD_RD_CASE(20) CD_RD_CASE(21)
+    CD_RD_CASE(22) CD_RD_CASE(23) CD_RD_CASE(24) CD_RD_CASE(25) CD_RD_CASE(26) CD_RD_CASE(27) CD_RD_CASE(28)
+    CD_RD_CASE(29) CD_RD_CASE(30) CD_RD_CASE(31) CD_RD_CASE(32)
+#undef CD_RD_CASE
     default: break;
   }
 }
@@ -1187,10 +1253,36 @@ static bool use_mf64(const Space &s)
   return s.assembled && s.mf_T > 0 && s.d_cellcoef && mf_shape_ok(s.nbf, s.mf_T) && s.dim == 3;
 }
 
+// the 8-wide incidence records of the matrix-free row kernels, built once per space (kept
+// only when every active row has at most 8 cells); synchronises on the first call
+static int ensure_inc8(cdgpu_ctx *ctx, Space &s)
+{
+  if (s.inc8_tried) return CDGPU_OK;
+  s.inc8_tried = true;
+  if (s.n_active <= 0 || (long)s.nbf * s.n_cells >= (long)INT_MAX) return CDGPU_OK;
+  int rc, *flag = nullptr;
+  if ((rc = dev_alloc(ctx, &s.d_inc8, (size_t)s.n_active * 8)) || (rc = dev_alloc(ctx, &flag, 1))) return rc;
+  CD_CUDA(ctx, cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream));
+  mf_inc8_kernel<<<(s.n_active + 255) / 256, 256, 0, ctx->stream>>>(s.n_active, s.nbf, s.n_cells, s.d_inc_ptr, s.d_inc,
+                                                                   s.d_inc8, flag);
+  CD_LAUNCHED(ctx);
+  int h = 0;
+  CD_CUDA(ctx, cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  cudaFree(flag);
+  if (h)
+  {
+    cudaFree(s.d_inc8);
+    s.d_inc8 = nullptr;
+  }
+  return CDGPU_OK;
+}
+
 static int ensure_mf64(cdgpu_ctx *ctx, Space &s)
 {
-  if (!s.d_ybuf64) return dev_alloc(ctx, &s.d_ybuf64, (size_t)s.nbf * s.n_cells);
-  return CDGPU_OK;
+  int rc;
+  if (!s.d_ybuf64 && (rc = dev_alloc(ctx, &s.d_ybuf64, (size_t)s.nbf * s.n_cells))) return rc;
+  return ensure_inc8(ctx, s);
 }
 
 // phase 1 of the matrix-free FP64 product: the per-cell products A_c x_c into d_ybuf64
@@ -1220,8 +1312,8 @@ template <int MODE>
 static void mf64_rows(cdgpu_ctx *ctx, const Space &s, const double *x, const double *f, double *out, double *partial)
 {
   (void)cd_launch(mf64_row_kernel<MODE>, mf64_rows_grid(ctx, s), 256, 0, ctx->stream, s.n_dof, s.n_active,
-                  s.n_cells, (const int *)s.d_inc_ptr, (const int *)s.d_inc, (const double *)s.d_ybuf64, x, f, out,
-                  partial);
+                  s.n_cells, (const int *)s.d_inc_ptr, (const int *)s.d_inc, (const int *)s.d_inc8,
+                  (const double *)s.d_ybuf64, x, f, out, partial);
 }
 
 // y = A x on the finest level: matrix-free in FP64 where the solve chose it, else the CSR entries
@@ -1355,12 +1447,24 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
   auto enqueue = [&](int i) -> int {
     int rc2;
     if ((rc2 = precondition(ctx, h, p, V(i), Z(i)))) return rc2;
-    if ((rc2 = finest_spmv(ctx, h, Z(i), h.d_w))) return rc2;
     int k = i + 1, pb = h.partial_blocks;
     double *c = ctl_it(i);
-    // pass 1: h1 = V^T w
-    launch_gs<GS_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, nullptr, h.d_partial, c, h.d_gs_count);
-    CD_LAUNCHED(ctx);
+    if (h.mf64 && s.d_inc8)
+    {
+      // w = A z_i matrix-free, its second phase fused with pass 1: h1 = V^T w
+      mf64_cells(ctx, s, Z(i));
+      CD_LAUNCHED(ctx);
+      launch_row_dots(k, pb, ctx->stream, n, s.n_active, s.d_inc8, s.d_ybuf64, Z(i), h.d_w, h.d_V, h.d_partial, c,
+                      h.d_gs_count);
+      CD_LAUNCHED(ctx);
+    }
+    else
+    {
+      if ((rc2 = finest_spmv(ctx, h, Z(i), h.d_w))) return rc2;
+      // pass 1: h1 = V^T w
+      launch_gs<GS_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, nullptr, h.d_partial, c, h.d_gs_count);
+      CD_LAUNCHED(ctx);
+    }
     // pass 2: w -= V h1, h2 = V^T w
     launch_gs<GS_AXPY_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, c, h.d_partial, c + 33, h.d_gs_count);
     CD_LAUNCHED(ctx);
@@ -1533,6 +1637,7 @@ static int fixed_point(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &
 static int prepare_mf(cdgpu_ctx *ctx, Space &s)
 {
   int rc;
+  if ((rc = ensure_inc8(ctx, s))) return rc;
   if (!s.d_ybuf)
   {
     if ((rc = dev_alloc(ctx, &s.d_cf32, (size_t)s.n_cells * CD_MAXT)) ||
