@@ -57,7 +57,7 @@ inline Mf64Tab mf64_tables()
 constexpr int kMf64Warps = 9, kMf64Cells = 32;
 
 template <int T>
-__global__ void __launch_bounds__(kMf64Warps * 32, 2)
+__global__ void __launch_bounds__(kMf64Warps * 32, 3)
     mf64_cell27_kernel(int n_cells, const int *__restrict__ gn, const double *__restrict__ cellcoef, int cstride,
                        const Mf64Tab tb, const double *__restrict__ x, double *__restrict__ ybuf, int pre)
 {
@@ -66,17 +66,14 @@ __global__ void __launch_bounds__(kMf64Warps * 32, 2)
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int w3 = w / 3, w1 = w - 3 * w3;
   const int n_groups = (n_cells + kMf64Cells - 1) / kMf64Cells;
-  // the next group's DOF numbers (this warp's z line) and coefficients, loaded one group ahead;
-  // with pre the first group's (written by no kernel of the solve) come before the wait
+  // the next group's DOF numbers (this warp's z line), loaded one group ahead; with pre the
+  // first group's (written by no kernel of the solve) come before the wait
   int gi[3];
-  double cf[T];
   auto fetch = [&](int grp) {
     const int c = grp * kMf64Cells + lane;
     const bool live = grp < n_groups && c < n_cells;
 #pragma unroll
     for (int k = 0; k < 3; k++) gi[k] = live ? __ldg(gn + (size_t)c * 27 + 9 * k + w) : -1;
-#pragma unroll
-    for (int t = 0; t < T; t++) cf[t] = live ? __ldg(cellcoef + (size_t)c * cstride + t) : 0.0;
   };
   if (pre) fetch(blockIdx.x);
   CD_PDL_ENTRY();
@@ -87,8 +84,9 @@ __global__ void __launch_bounds__(kMf64Warps * 32, 2)
     double X[3], C[T];
 #pragma unroll
     for (int k = 0; k < 3; k++) X[k] = gi[k] >= 0 ? __ldg(x + gi[k]) : 0.0;
+    // the coefficients, first read in pass 3, are in flight during passes 1 and 2
 #pragma unroll
-    for (int t = 0; t < T; t++) C[t] = cf[t];
+    for (int t = 0; t < T; t++) C[t] = c < n_cells ? __ldg(cellcoef + (size_t)c * cstride + t) : 0.0;
     fetch(grp + gridDim.x);
     // pass 1, z: warp w = line (jy, jx); UB[qz] = sum_jz B[qz][jz] X, UG[qz] = sum_jz G[qz][jz] X
 #pragma unroll

@@ -1290,7 +1290,7 @@ static void mf64_cells(cdgpu_ctx *ctx, const Space &s, const double *x)
 {
   static const Mf64Tab tab = mf64_tables();
   const int groups = (s.n_cells + kMf64Cells - 1) / kMf64Cells;
-  const int grid = std::max(1, std::min(groups, ctx->sm_count * 2));
+  const int grid = std::max(1, std::min(groups, ctx->sm_count * 3));
   const int cstride = s.mf_T + n_rhs_tensors(s.dim, s.ref_disctype);
   // the cell data is read before the wait once a launch of this assembly has waited
   const int pre = s.mf64_safe_version == s.assembly_version ? 1 : 0;
