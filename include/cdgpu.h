@@ -227,6 +227,9 @@ int cdgpu_apply_fp32(cdgpu_ctx *ctx, int space_id, int form, const float *h_x, f
  * cells with constant coefficients (CDGPU_ERR_UNSUPPORTED otherwise).  h_x, h_y: host arrays
  * of n_dof doubles. */
 int cdgpu_apply_fp64(cdgpu_ctx *ctx, int space_id, int form, const double *h_x, double *h_y);
+/* The same on device vectors of n_dof doubles, enqueued on the context's stream (no
+ * synchronisation; like cdgpu_spmv_device). */
+int cdgpu_apply_fp64_device(cdgpu_ctx *ctx, int space_id, int form, const double *d_x, double *d_y);
 /* The defect d = f - A x and *h_res = ||d||, like cdgpu_defect, for callers that cannot
  * allocate device memory (for example while another allocator holds the whole device, or
  * where the device synchronisation of cudaFree is not acceptable).  No counterpart in the

@@ -72,6 +72,7 @@ SIGNATURES = {
     "cdgpu_spmv_device": (_I, [_P, _I, _P, _P]),
     "cdgpu_apply_fp32": (_I, [_P, _I, _I, _P, _P]),
     "cdgpu_apply_fp64": (_I, [_P, _I, _I, _P, _P]),
+    "cdgpu_apply_fp64_device": (_I, [_P, _I, _I, _P, _P]),
     "cdgpu_product_tuning": (_I, [_P, _I, C.c_char_p, _I]),
     "cdgpu_defect_noalloc": (_I, [_P, _I, _P, _P, _P, C.POINTER(C.c_double)]),
     "cdgpu_hierarchy": (_I, [_P, _I, _P, _P, C.POINTER(_I)]),

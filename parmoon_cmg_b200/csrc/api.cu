@@ -456,6 +456,15 @@ int cdgpu_spmv(cdgpu_ctx *ctx, int space_id, const double *h_x, double *h_y)
   return rc;
 }
 
+int cdgpu_apply_fp64_device(cdgpu_ctx *ctx, int space_id, int form, const double *d_x, double *d_y)
+{
+  Space *s = get_space(ctx, space_id);
+  if (!s || !s->assembled || !d_x || !d_y || form < 0 || form > 1)
+    return fail(ctx, CDGPU_ERR_INVALID, "apply_fp64: bad argument");
+  cudaSetDevice(ctx->device);
+  return apply_fp64_form(ctx, *s, form, d_x, d_y, false);
+}
+
 int cdgpu_apply_fp64(cdgpu_ctx *ctx, int space_id, int form, const double *h_x, double *h_y)
 {
   Space *s = get_space(ctx, space_id);
@@ -470,7 +479,7 @@ int cdgpu_apply_fp64(cdgpu_ctx *ctx, int space_id, int form, const double *h_x, 
     return rc;
   }
   cudaError_t e = cudaMemcpyAsync(dx, h_x, sizeof(double) * s->n_dof, cudaMemcpyHostToDevice, ctx->stream);
-  rc = e == cudaSuccess ? apply_fp64_form(ctx, *s, form, dx, dy) : cuda_fail(ctx, e, "apply_fp64: copy");
+  rc = e == cudaSuccess ? apply_fp64_form(ctx, *s, form, dx, dy, true) : cuda_fail(ctx, e, "apply_fp64: copy");
   if (!rc)
   {
     e = cudaMemcpyAsync(h_y, dy, sizeof(double) * s->n_dof, cudaMemcpyDeviceToHost, ctx->stream);

@@ -1025,6 +1025,7 @@ int err_flag_status(cdgpu_ctx *ctx)
     if (e == 3) return fail(ctx, CDGPU_ERR_CUDA, "multigrid: a tensor-core product did not complete in time");
     if (e == 4) return fail(ctx, CDGPU_ERR_CUDA, "CSR product: a bulk copy of a matrix tile did not complete in time");
     if (e == 5) return fail(ctx, CDGPU_ERR_CUDA, "assemble: a bulk copy of cell data or tables did not complete in time");
+    if (e == 7) return fail(ctx, CDGPU_ERR_INVALID, "errors: a DOF number outside the space");
     return fail(ctx, CDGPU_ERR_UNSUPPORTED, "assemble: CSR row longer than the kernel's row buffer");
   }
   return CDGPU_OK;
@@ -1034,6 +1035,13 @@ int err_flag_status(cdgpu_ctx *ctx)
 static int ensure_quadtab(cdgpu_ctx *ctx, Space &s)
 {
   if (s.d_quadtab) return CDGPU_OK;
+  // the tables are the space's reference element's: build it first (a space whose errors are
+  // evaluated before any assembly has none yet)
+  if (!s.re_ready)
+  {
+    make_ref_element(s.dim, s.order, s.re);
+    s.re_ready = true;
+  }
   const RefElement &re = s.re;
   std::vector<double> packed;
   packed.insert(packed.end(), re.qx.begin(), re.qx.end());
@@ -1062,7 +1070,8 @@ __global__ void __launch_bounds__(256) errors_sine_kernel(int n_cells, int nbf, 
                                                           const double *__restrict__ qw,
                                                           const double *__restrict__ phi,
                                                           const double *__restrict__ dphi,
-                                                          const double *__restrict__ u, double *__restrict__ partial)
+                                                          const double *__restrict__ u, double *__restrict__ partial,
+                                                          int n_dof, int *__restrict__ err)
 {
   CD_PDL_ENTRY();
   __shared__ double red[2][8];
@@ -1081,7 +1090,14 @@ __global__ void __launch_bounds__(256) errors_sine_kernel(int n_cells, int nbf, 
       {
         const double *gr = dphi + (size_t)(q * nbf + b) * 2;
         const double gx = Ji[0] * gr[0] + Ji[2] * gr[1], gy = Ji[1] * gr[0] + Ji[3] * gr[1];
-        const double ub = u[gn[(size_t)c * nbf + b]];
+        const int gb = gn[(size_t)c * nbf + b];
+        if ((unsigned)gb >= (unsigned)n_dof)
+        {
+          // a DOF number outside the space: flagged, not read
+          atomicExch(err, 7);
+          continue;
+        }
+        const double ub = u[gb];
         uh += ub * phi[q * nbf + b];
         ux += ub * gx;
         uy += ub * gy;
@@ -1126,7 +1142,8 @@ __global__ void __launch_bounds__(256) errors_table_kernel(int dim, int n_cells,
                                                            const double *__restrict__ dphi,
                                                            const double *__restrict__ u,
                                                            const double *__restrict__ ex,
-                                                           double *__restrict__ partial)
+                                                           double *__restrict__ partial, int n_dof,
+                                                           int *__restrict__ err)
 {
   CD_PDL_ENTRY();
   __shared__ double red[2][8];
@@ -1144,7 +1161,14 @@ __global__ void __launch_bounds__(256) errors_table_kernel(int dim, int n_cells,
       for (int b = 0; b < nbf; b++)
       {
         const double *gr = dphi + (size_t)(q * nbf + b) * dim;
-        const double ub = u[gn[(size_t)c * nbf + b]];
+        const int gb = gn[(size_t)c * nbf + b];
+        if ((unsigned)gb >= (unsigned)n_dof)
+        {
+          // a DOF number outside the space: flagged, not read
+          atomicExch(err, 7);
+          continue;
+        }
+        const double ub = u[gb];
         uh += ub * phi[q * nbf + b];
         for (int r = 0; r < dim; r++)
         {
@@ -1189,6 +1213,7 @@ int space_errors_table(cdgpu_ctx *ctx, Space &s, const double *d_u, const double
     make_ref_element(s.dim, s.order, s.re);
     s.re_ready = true;
   }
+  if ((rc = ensure_err_flag(ctx))) return rc;
   if ((rc = ensure_quadtab(ctx, s))) return rc;
   const RefElement &re = s.re;
   const double *qx = s.d_quadtab, *qw = qx + re.qx.size(), *phi = qw + re.qw.size(), *dphi = phi + re.phi.size();
@@ -1197,7 +1222,7 @@ int space_errors_table(cdgpu_ctx *ctx, Space &s, const double *d_u, const double
   if ((rc = dev_alloc(ctx, &d_partial, (size_t)2 * grid))) return rc;
   (void)cd_launch(errors_table_kernel, grid, 256, 0, ctx->stream, s.dim, s.n_cells, s.nbf, re.nq, s.nv,
                   s.all_affine ? 1 : 0, (const double *)s.d_coords, (const int *)s.d_gn, qx, qw, phi, dphi, d_u,
-                  d_ex, d_partial);
+                  d_ex, d_partial, s.n_dof, ctx->d_err);
   cudaError_t e = cudaGetLastError();
   std::vector<double> part((size_t)2 * grid);
   if (e == cudaSuccess)
@@ -1210,7 +1235,7 @@ int space_errors_table(cdgpu_ctx *ctx, Space &s, const double *d_u, const double
   for (int i = 0; i < grid; i++) { a += part[2 * i]; b += part[2 * i + 1]; }
   *l2 = std::sqrt(a);
   *h1semi = std::sqrt(b);
-  return CDGPU_OK;
+  return assemble_check(ctx); // the DOF-number check of the kernel
 }
 
 int space_errors_sine(cdgpu_ctx *ctx, Space &s, const double *d_u, double *l2, double *h1semi)
@@ -1218,6 +1243,7 @@ int space_errors_sine(cdgpu_ctx *ctx, Space &s, const double *d_u, double *l2, d
   if (s.dim != 2 || !s.co_set || s.co.kind != CDGPU_COEFF_SINE)
     return fail(ctx, CDGPU_ERR_UNSUPPORTED, "errors: only 2D spaces with the sine coefficients (SineLaplace) have an exact solution");
   int rc;
+  if ((rc = ensure_err_flag(ctx))) return rc;
   if ((rc = ensure_quadtab(ctx, s))) return rc;
   const RefElement &re = s.re;
   const double *qx = s.d_quadtab, *qw = qx + re.qx.size(), *phi = qw + re.qw.size(), *dphi = phi + re.phi.size();
@@ -1226,7 +1252,7 @@ int space_errors_sine(cdgpu_ctx *ctx, Space &s, const double *d_u, double *l2, d
   if ((rc = dev_alloc(ctx, &d_partial, (size_t)2 * grid))) return rc;
   (void)cd_launch(errors_sine_kernel, grid, 256, 0, ctx->stream, s.n_cells, s.nbf, re.nq, s.nv,
                   s.all_affine ? 1 : 0, (const double *)s.d_coords, (const int *)s.d_gn, qx, qw, phi, dphi, d_u,
-                  d_partial);
+                  d_partial, s.n_dof, ctx->d_err);
   cudaError_t e = cudaGetLastError();
   std::vector<double> part((size_t)2 * grid);
   if (e == cudaSuccess)
@@ -1239,7 +1265,7 @@ int space_errors_sine(cdgpu_ctx *ctx, Space &s, const double *d_u, double *l2, d
   for (int i = 0; i < grid; i++) { a += part[2 * i]; b += part[2 * i + 1]; }
   *l2 = std::sqrt(a);
   *h1semi = std::sqrt(b);
-  return CDGPU_OK;
+  return assemble_check(ctx); // the DOF-number check of the kernel
 }
 
 int assemble_space(cdgpu_ctx *ctx, Space &s, int disctype, const double *h_dir, bool check)

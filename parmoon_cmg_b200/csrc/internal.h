@@ -318,7 +318,7 @@ int setup_hierarchy_buffers(cdgpu_ctx *ctx, Hierarchy &h, int m);
 int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *d_rhs,
               double *d_sol, cdgpu_solve_info *info);
 int apply_fp32_form(cdgpu_ctx *ctx, Space &s, int form, const float *d_x, float *d_y);
-int apply_fp64_form(cdgpu_ctx *ctx, Space &s, int form, const double *d_x, double *d_y);
+int apply_fp64_form(cdgpu_ctx *ctx, Space &s, int form, const double *d_x, double *d_y, bool check);
 // the explicit inverse of the coarsest level's matrix for the exact coarse solve, when its
 // assembly changed since the last inversion (enqueued on ctx->stream)
 int refresh_coarse_inverse(cdgpu_ctx *ctx, Hierarchy &h);

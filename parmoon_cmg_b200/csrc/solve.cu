@@ -1746,14 +1746,15 @@ int run_solve(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const 
 // y = A x with one of the FP64 forms of a space's operator: form 0 the assembled CSR entries,
 // 1 the matrix-free sum-factorised per-cell products the mixed form's FGMRES iteration applies
 // on its finest level.  Dirichlet rows are identity rows in both.  Form 1 needs a Q2
-// hexahedral space assembled by the affine constant-coefficient path.
-int apply_fp64_form(cdgpu_ctx *ctx, Space &s, int form, const double *d_x, double *d_y)
+// hexahedral space assembled by the affine constant-coefficient path.  check: read back the
+// bulk-copy product's wait flag (synchronises).
+int apply_fp64_form(cdgpu_ctx *ctx, Space &s, int form, const double *d_x, double *d_y, bool check)
 {
   if (form == 0)
   {
     csr_spmv<double>(ctx, s, d_x, d_y);
     CD_LAUNCHED(ctx);
-    return ctx->d_err ? assemble_check(ctx) : CDGPU_OK;
+    return check && ctx->d_err ? assemble_check(ctx) : CDGPU_OK;
   }
   if (!use_mf64(s))
     return fail(ctx, CDGPU_ERR_UNSUPPORTED,
