@@ -1546,7 +1546,9 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
           y[a] /= H[(size_t)a * m + a];
           for (int b = a - 1; b >= 0; b--) y[b] -= H[(size_t)b * m + a] * y[a];
         }
-        CD_CUDA(ctx, cudaMemcpyAsync(h.d_ctl + 100, y.data(), sizeof(double) * (i + 1), cudaMemcpyHostToDevice,
+        // staged in the pinned control mirror (positions 100..131), so the copy is asynchronous
+        std::copy(y.begin(), y.begin() + (i + 1), h.h_ctl + 100);
+        CD_CUDA(ctx, cudaMemcpyAsync(h.d_ctl + 100, h.h_ctl + 100, sizeof(double) * (i + 1), cudaMemcpyHostToDevice,
                                      ctx->stream));
         (void)cd_launch(update_kernel, blocks, 256, 0, ctx->stream, n, i + 1, h.d_ctl + 100, h.d_Z, x);
         CD_LAUNCHED(ctx);
@@ -1574,7 +1576,8 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
       y[a] /= H[(size_t)a * m + a];
       for (int b = a - 1; b >= 0; b--) y[b] -= H[(size_t)b * m + a] * y[a];
     }
-    CD_CUDA(ctx, cudaMemcpyAsync(h.d_ctl + 100, y.data(), sizeof(double) * m, cudaMemcpyHostToDevice, ctx->stream));
+    std::copy(y.begin(), y.begin() + m, h.h_ctl + 100);
+    CD_CUDA(ctx, cudaMemcpyAsync(h.d_ctl + 100, h.h_ctl + 100, sizeof(double) * m, cudaMemcpyHostToDevice, ctx->stream));
     (void)cd_launch(update_kernel, blocks, 256, 0, ctx->stream, n, m, h.d_ctl + 100, h.d_Z, x);
     CD_LAUNCHED(ctx);
     if ((rc = finest_defect_norm(ctx, h, x, f, V(0), nrm))) return rc;
