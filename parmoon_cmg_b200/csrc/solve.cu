@@ -261,16 +261,23 @@ __global__ void coarse_smooth_kernel(int n, int n_active, const int *__restrict_
 //   GS_DOTS       partial dots  w . Y_j
 //   GS_AXPY_DOTS  w -= sum_j coef_j Y_j, then partial dots of the new w with every Y_j
 //   GS_AXPY_NORM  w -= sum_j coef_j Y_j, then partial ||w||^2
+//   GS_AXPY_DOTS_NORM  as GS_AXPY_DOTS, and also ||w||^2; the last block then leaves
+//                 ||w - sum_j d_j Y_j||^2 = ||w||^2 - sum_j d_j^2 (Y orthonormal, d = Y^T w) in
+//                 *norm_out, so the second classical Gram-Schmidt pass needs no third pass:
+//                 the next basis vector (w - Y d) / norm is formed by axpy_scale_kernel
 // Every thread keeps the K basis values of its row in registers; per-block partials go to
 // partial[block * 33 + slot] and are summed in block order by the pass's last block.
-enum { GS_DOTS = 0, GS_AXPY_DOTS = 1, GS_AXPY_NORM = 2 };
+enum { GS_DOTS = 0, GS_AXPY_DOTS = 1, GS_AXPY_NORM = 2, GS_AXPY_DOTS_NORM = 3 };
 
 // Block partials of NS sums and their reduction by the last block to arrive (an arrival
 // counter, reset by that block): partial[block * 33 + slot], then out[slot] summed in block
 // order (lanes over blocks, then a fixed warp tree).  Every thread of the block calls it.
+// With norm_out, out[0..NS-1) are dot products d_j of a vector with orthonormal vectors and
+// out[NS-1] the vector's squared norm; the last block also stores max(0, out[NS-1] - sum d_j^2).
 template <int NS>
 __device__ __forceinline__ void gs_reduce(const double (&acc)[NS], double *__restrict__ partial,
-                                          double *__restrict__ out, unsigned *__restrict__ counter)
+                                          double *__restrict__ out, unsigned *__restrict__ counter,
+                                          double *__restrict__ norm_out = nullptr)
 {
   __shared__ double red[kBlock / 32][NS];
   const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
@@ -314,6 +321,16 @@ __device__ __forceinline__ void gs_reduce(const double (&acc)[NS], double *__res
     t = group_sum<32>(t);
     if (lane == 0) out[j] = t;
   }
+  if (norm_out)
+  {
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+      double r = out[NS - 1];
+      for (int j = 0; j < NS - 1; j++) r -= out[j] * out[j];
+      norm_out[0] = r > 0.0 ? r : 0.0;
+    }
+  }
   if (threadIdx.x == 0) *counter = 0u;
 }
 
@@ -322,10 +339,11 @@ __global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, const double *__
                                                          double *__restrict__ w,
                                                          const double *__restrict__ coef,
                                                          double *__restrict__ partial,
-                                                         double *__restrict__ out, unsigned *__restrict__ counter)
+                                                         double *__restrict__ out, unsigned *__restrict__ counter,
+                                                         double *__restrict__ norm_out)
 {
   CD_PDL_ENTRY();
-  constexpr int NS = MODE == GS_AXPY_NORM ? 1 : K;
+  constexpr int NS = MODE == GS_AXPY_NORM ? 1 : MODE == GS_AXPY_DOTS_NORM ? K + 1 : K;
   double acc[NS];
 #pragma unroll
   for (int j = 0; j < NS; j++) acc[j] = 0;
@@ -351,18 +369,19 @@ __global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, const double *__
     {
 #pragma unroll
       for (int j = 0; j < K; j++) acc[j] += wi * y[j];
+      if constexpr (MODE == GS_AXPY_DOTS_NORM) acc[NS - 1] += wi * wi;
     }
   }
-  gs_reduce<NS>(acc, partial, out, counter);
+  gs_reduce<NS>(acc, partial, out, counter, MODE == GS_AXPY_DOTS_NORM ? norm_out : nullptr);
 }
 
 template <int MODE>
 static void launch_gs(int k, int grid, cudaStream_t st, int n, const double *Y, double *w, const double *coef,
-                      double *partial, double *out, unsigned *counter)
+                      double *partial, double *out, unsigned *counter, double *norm_out = nullptr)
 {
   switch (k)
   {
-#define CD_GS_CASE(K) case K: (void)cd_launch(gs_pass_kernel<K, MODE>, grid, kBlock, 0, st, n, Y, w, coef, partial, out, counter); break;
+#define CD_GS_CASE(K) case K: (void)cd_launch(gs_pass_kernel<K, MODE>, grid, kBlock, 0, st, n, Y, w, coef, partial, out, counter, norm_out); break;
     CD_GS_CASE(1) CD_GS_CASE(2) CD_GS_CASE(3) CD_GS_CASE(4) CD_GS_CASE(5) CD_GS_CASE(6) CD_GS_CASE(7)
     CD_GS_CASE(8) CD_GS_CASE(9) CD_GS_CASE(10) CD_GS_CASE(11) CD_GS_CASE(12) CD_GS_CASE(13) CD_GS_CASE(14)
     CD_GS_CASE(15) CD_GS_CASE(16) CD_GS_CASE(17) CD_GS_CASE(18) CD_GS_CASE(19) CD_GS_CASE(20) CD_GS_CASE(21)
@@ -458,6 +477,42 @@ __global__ void scale_norm_kernel(int n, const double *__restrict__ nrm2, const 
   const double hn = sqrt(*nrm2);
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (hn != 0 && i < n) y[i] = (1.0 / hn) * x[i];
+}
+
+// y = (w - sum_j coef_j Y_j) / sqrt(*nrm2) unless *nrm2 == 0: the second Gram-Schmidt pass's
+// update of w (in the order of the GS passes) and the next basis vector in one pass
+template <int K>
+__global__ void __launch_bounds__(256) axpy_scale_kernel(int n, const double *__restrict__ Y,
+                                                         const double *__restrict__ w, const double *__restrict__ coef,
+                                                         const double *__restrict__ nrm2, double *__restrict__ y)
+{
+  CD_PDL_ENTRY();
+  const double hn = sqrt(*nrm2);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (hn == 0 || i >= n) return;
+  double v[K];
+#pragma unroll
+  for (int j = 0; j < K; j++) v[j] = __ldg(Y + (size_t)j * n + i);
+  double wi = w[i];
+#pragma unroll
+  for (int j = 0; j < K; j++) wi -= coef[j] * v[j];
+  y[i] = (1.0 / hn) * wi;
+}
+
+static void launch_axpy_scale(int k, int grid, cudaStream_t st, int n, const double *Y, const double *w,
+                              const double *coef, const double *nrm2, double *y)
+{
+  switch (k)
+  {
+#define CD_AS_CASE(K) case K: (void)cd_launch(axpy_scale_kernel<K>, grid, 256, 0, st, n, Y, w, coef, nrm2, y); break;
+    CD_AS_CASE(1) CD_AS_CASE(2) CD_AS_CASE(3) CD_AS_CASE(4) CD_AS_CASE(5) CD_AS_CASE(6) CD_AS_CASE(7)
+    CD_AS_CASE(8) CD_AS_CASE(9) CD_AS_CASE(10) CD_AS_CASE(11) CD_AS_CASE(12) CD_AS_CASE(13) CD_AS_CASE(14)
+    CD_AS_CASE(15) CD_AS_CASE(16) CD_AS_CASE(17) CD_AS_CASE(18) CD_AS_CASE(19) CD_AS_CASE(20) CD_AS_CASE(21)
+    CD_AS_CASE(22) CD_AS_CASE(23) CD_AS_CASE(24) CD_AS_CASE(25) CD_AS_CASE(26) CD_AS_CASE(27) CD_AS_CASE(28)
+    CD_AS_CASE(29) CD_AS_CASE(30) CD_AS_CASE(31) CD_AS_CASE(32)
+#undef CD_AS_CASE
+    default: break;
+  }
 }
 
 __global__ void set_io_kernel(double **io, const double *r, double *z)
@@ -1465,17 +1520,16 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
       launch_gs<GS_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, nullptr, h.d_partial, c, h.d_gs_count);
       CD_LAUNCHED(ctx);
     }
-    // pass 2: w -= V h1, h2 = V^T w
-    launch_gs<GS_AXPY_DOTS>(k, pb, ctx->stream, n, h.d_V, h.d_w, c, h.d_partial, c + 33, h.d_gs_count);
-    CD_LAUNCHED(ctx);
-    // w -= V h2, ||w||^2
-    launch_gs<GS_AXPY_NORM>(k, pb, ctx->stream, n, h.d_V, h.d_w, c + 33, h.d_partial, c + 66, h.d_gs_count);
+    // pass 2: w -= V h1, h2 = V^T w, and ||w - V h2||^2 = ||w||^2 - ||h2||^2
+    launch_gs<GS_AXPY_DOTS_NORM>(k, pb, ctx->stream, n, h.d_V, h.d_w, c, h.d_partial, c + 33, h.d_gs_count,
+                                 c + 66);
     CD_LAUNCHED(ctx);
     CD_CUDA(ctx, cudaEventRecord(h.ev_ready[i & 1], ctx->stream));
     CD_CUDA(ctx, cudaStreamWaitEvent(h.cstream, h.ev_ready[i & 1], 0));
     CD_CUDA(ctx, cudaMemcpyAsync(h.h_slot + (i & 1) * 80, c, sizeof(double) * 67, cudaMemcpyDeviceToHost, h.cstream));
     CD_CUDA(ctx, cudaEventRecord(h.ev_slot[i & 1], h.cstream));
-    (void)cd_launch(scale_norm_kernel, blocks, 256, 0, ctx->stream, n, c + 66, h.d_w, V(i + 1));
+    // v_{i+1} = (w - V h2) / ||w - V h2||
+    launch_axpy_scale(k, blocks, ctx->stream, n, h.d_V, h.d_w, c + 33, c + 66, V(i + 1));
     CD_LAUNCHED(ctx);
     return CDGPU_OK;
   };
