@@ -470,12 +470,19 @@ __global__ void sum_blocks_kernel(int nblocks, const double *__restrict__ partia
 
 // y = x / sqrt(*nrm2) unless *nrm2 == 0 (the next Arnoldi vector, scaled on the device so that
 // the host need not have read the norm yet)
+// With io, the first thread also sets the multigrid cycle graph's (in, out) slot to (y, z_next):
+// y is the next preconditioner input, so the cycle needs no pointer kernel of its own.
 __global__ void scale_norm_kernel(int n, const double *__restrict__ nrm2, const double *__restrict__ x,
-                                  double *__restrict__ y)
+                                  double *__restrict__ y, double **io, double *z_next)
 {
   CD_PDL_ENTRY();
   const double hn = sqrt(*nrm2);
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (io && i == 0)
+  {
+    io[0] = y;
+    io[1] = z_next;
+  }
   if (hn != 0 && i < n) y[i] = (1.0 / hn) * x[i];
 }
 
@@ -484,11 +491,18 @@ __global__ void scale_norm_kernel(int n, const double *__restrict__ nrm2, const 
 template <int K>
 __global__ void __launch_bounds__(256) axpy_scale_kernel(int n, const double *__restrict__ Y,
                                                          const double *__restrict__ w, const double *__restrict__ coef,
-                                                         const double *__restrict__ nrm2, double *__restrict__ y)
+                                                         const double *__restrict__ nrm2, double *__restrict__ y,
+                                                         double **io, double *z_next)
 {
   CD_PDL_ENTRY();
   const double hn = sqrt(*nrm2);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (io && i == 0)
+  {
+    // the cycle graph's (in, out) slot for the next preconditioner application
+    io[0] = y;
+    io[1] = z_next;
+  }
   if (hn == 0 || i >= n) return;
   double v[K];
 #pragma unroll
@@ -500,11 +514,11 @@ __global__ void __launch_bounds__(256) axpy_scale_kernel(int n, const double *__
 }
 
 static void launch_axpy_scale(int k, int grid, cudaStream_t st, int n, const double *Y, const double *w,
-                              const double *coef, const double *nrm2, double *y)
+                              const double *coef, const double *nrm2, double *y, double **io, double *z_next)
 {
   switch (k)
   {
-#define CD_AS_CASE(K) case K: (void)cd_launch(axpy_scale_kernel<K>, grid, 256, 0, st, n, Y, w, coef, nrm2, y); break;
+#define CD_AS_CASE(K) case K: (void)cd_launch(axpy_scale_kernel<K>, grid, 256, 0, st, n, Y, w, coef, nrm2, y, io, z_next); break;
     CD_AS_CASE(1) CD_AS_CASE(2) CD_AS_CASE(3) CD_AS_CASE(4) CD_AS_CASE(5) CD_AS_CASE(6) CD_AS_CASE(7)
     CD_AS_CASE(8) CD_AS_CASE(9) CD_AS_CASE(10) CD_AS_CASE(11) CD_AS_CASE(12) CD_AS_CASE(13) CD_AS_CASE(14)
     CD_AS_CASE(15) CD_AS_CASE(16) CD_AS_CASE(17) CD_AS_CASE(18) CD_AS_CASE(19) CD_AS_CASE(20) CD_AS_CASE(21)
@@ -929,7 +943,9 @@ static bool same_cycle_params(const cdgpu_solver_params &a, const cdgpu_solver_p
 
 // The whole V/W/F cycle (about 7 kernels per level) is captured once into a CUDA graph
 // and replayed for every basis vector; only the two pointers in h.d_io change.
-static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *r, double *z)
+// io_ready: the kernel before this call already set the graph's (in, out) slot to (r, z)
+static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *r, double *z,
+                    bool io_ready = false)
 {
   const int k = p.precision == 1 ? 1 : 0;
   int rc;
@@ -962,8 +978,11 @@ static int mg_apply(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, 
   // the application's (in, out) pointers into the graph's slot: a one-thread kernel in the
   // stream's launch chain (a host-to-device copy would hold the stream for the copy engine's
   // round trip)
-  (void)cd_launch(set_io_kernel, 1, 1, 0, ctx->stream, h.d_io, r, z);
-  CD_LAUNCHED(ctx);
+  if (!io_ready)
+  {
+    (void)cd_launch(set_io_kernel, 1, 1, 0, ctx->stream, h.d_io, r, z);
+    CD_LAUNCHED(ctx);
+  }
   CD_CUDA(ctx, cudaGraphLaunch(h.gexec[k], ctx->stream));
   ctx->launches += h.graph_nodes[k];
   return CDGPU_OK;
@@ -1426,9 +1445,10 @@ int defect64(cdgpu_ctx *ctx, const Space &s, const double *x, const double *f, d
   return CDGPU_OK;
 }
 
-static int precondition(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *r, double *z)
+static int precondition(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, const double *r, double *z,
+                        bool io_ready = false)
 {
-  return mg_apply(ctx, h, p, r, z);
+  return mg_apply(ctx, h, p, r, z, io_ready);
 }
 
 // the host copy of the FGMRES control block: [0..k) h1, [33..33+k) h2, [66] ||w||^2
@@ -1501,7 +1521,8 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
   // arithmetic.
   auto enqueue = [&](int i) -> int {
     int rc2;
-    if ((rc2 = precondition(ctx, h, p, V(i), Z(i)))) return rc2;
+    // the kernel that formed v_i (scale_norm_kernel or axpy_scale_kernel) set the cycle's slot
+    if ((rc2 = precondition(ctx, h, p, V(i), Z(i), true))) return rc2;
     int k = i + 1, pb = h.partial_blocks;
     double *c = ctl_it(i);
     if (h.mf64 && s.d_inc8)
@@ -1529,13 +1550,14 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
     CD_CUDA(ctx, cudaMemcpyAsync(h.h_slot + (i & 1) * 80, c, sizeof(double) * 67, cudaMemcpyDeviceToHost, h.cstream));
     CD_CUDA(ctx, cudaEventRecord(h.ev_slot[i & 1], h.cstream));
     // v_{i+1} = (w - V h2) / ||w - V h2||
-    launch_axpy_scale(k, blocks, ctx->stream, n, h.d_V, h.d_w, c + 33, c + 66, V(i + 1));
+    launch_axpy_scale(k, blocks, ctx->stream, n, h.d_V, h.d_w, c + 33, c + 66, V(i + 1), h.d_io, Z(i + 1));
     CD_LAUNCHED(ctx);
     return CDGPU_OK;
   };
   // the first restart cycle's v_0 and iteration 0, before ||r0|| is known on the host (if the
   // start already satisfies the stopping test they are discarded: x is not touched)
-  (void)cd_launch(scale_norm_kernel, blocks, 256, 0, ctx->stream, n, (const double *)nrm, V(0), V(0));
+  (void)cd_launch(scale_norm_kernel, blocks, 256, 0, ctx->stream, n, (const double *)nrm, V(0), V(0), h.d_io,
+                  Z(0));
   CD_LAUNCHED(ctx);
   if ((rc = enqueue(0))) return rc;
   CD_CUDA(ctx, cudaEventSynchronize(h.ev_beta));
@@ -1561,7 +1583,8 @@ static int fgmres(cdgpu_ctx *ctx, Hierarchy &h, const cdgpu_solver_params &p, co
   {
     if (!first_cycle)
     {
-      (void)cd_launch(scale_norm_kernel, blocks, 256, 0, ctx->stream, n, (const double *)nrm, V(0), V(0));
+      (void)cd_launch(scale_norm_kernel, blocks, 256, 0, ctx->stream, n, (const double *)nrm, V(0), V(0), h.d_io,
+                  Z(0));
       CD_LAUNCHED(ctx);
     }
     std::fill(sv.begin(), sv.end(), 0.0);

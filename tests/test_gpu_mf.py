@@ -89,6 +89,13 @@ def test_fp64_matrix_free_form(ctx, n, disc):
     assert err_csr <= 1e-14 and err_ref <= 1e-14
     # deterministic: the rows sum their cells in a fixed order
     assert np.array_equal(ctx.apply_fp64(sid, x, 1), y_mf)
+    # the device-vector entry point enqueues the same product
+    import torch
+    dx = torch.from_numpy(x).cuda()
+    dy = torch.zeros_like(dx)
+    ctx.check(ctx.lib.cdgpu_apply_fp64_device(ctx.h, sid, 1, dx.data_ptr(), dy.data_ptr()))
+    torch.cuda.synchronize()
+    assert np.array_equal(dy.cpu().numpy(), y_mf)
 
 
 def test_fp32_operator_forms_unsupported(ctx):
@@ -107,3 +114,27 @@ def test_fp32_operator_forms_unsupported(ctx):
     with pytest.raises(_lib.CdgpuError) as e:
         ctx.apply_fp64(sid, x.astype(np.float64), 1)
     assert e.value.status == _lib.ERR_UNSUPPORTED
+
+
+def test_mixed_solve_with_matrix_free_supg_product(ctx):
+    """A 32^3 Q2 SUPG finest level (32,768 cells, 13 reference tensors): the mixed solve applies
+    its FGMRES product and defect matrix-free in FP64 (the SUPG tensors in the point-wise
+    fluxes) and must land within 1e-8 of the FP64 form's solution, with the same iteration count
+    up to one."""
+    from parmoon_cmg_b200.system import TSystemCD3D, solver_params
+    spaces, parents = mesh.structured_hierarchy(3, 2, 2, 5)
+    S = TSystemCD3D(spaces, parents, disctype=SUPG, ctx=ctx, coarse_disctype=SUPG)
+    S.Init(coeffs(0, eps=1e-2, b=(0.57735026918962573,) * 3, c=0.1, f=1.0, delta0=1.0 / 3.0))
+    rhs = np.zeros(S.N_DOF)
+    sol0 = np.zeros(S.N_DOF)
+    S.Assemble(sol0, rhs)
+    common = dict(coarse_smoother=17, stop_rule=1, red_factor=1e-12, res_norm_min=0.0)
+    x64 = sol0.copy()
+    i64 = S.Solve(x64, rhs, solver_params(precision=0, **common))
+    xm = sol0.copy()
+    im = S.Solve(xm, rhs, solver_params(precision=1, **common))
+    assert i64.status == 0 and im.status == 0
+    err = np.abs(xm - x64).max() / np.abs(x64).max()
+    print(f"SUPG 32^3: FP64 {i64.iterations} its, mixed {im.iterations} its, rel. diff {err:.2e}")
+    assert err <= 1e-8
+    assert abs(im.iterations - i64.iterations) <= 1
