@@ -258,16 +258,15 @@ __global__ void coarse_smooth_kernel(int n, int n_active, const int *__restrict_
 // dense vector kernels for FGMRES (FP64)
 // ---------------------------------------------------------------------------
 // One fused pass of classical Gram-Schmidt over K basis vectors Y[0..K) (row stride n):
-//   GS_DOTS       partial dots  w . Y_j
-//   GS_AXPY_DOTS  w -= sum_j coef_j Y_j, then partial dots of the new w with every Y_j
-//   GS_AXPY_NORM  w -= sum_j coef_j Y_j, then partial ||w||^2
-//   GS_AXPY_DOTS_NORM  as GS_AXPY_DOTS, and also ||w||^2; the last block then leaves
-//                 ||w - sum_j d_j Y_j||^2 = ||w||^2 - sum_j d_j^2 (Y orthonormal, d = Y^T w) in
-//                 *norm_out, so the second classical Gram-Schmidt pass needs no third pass:
-//                 the next basis vector (w - Y d) / norm is formed by axpy_scale_kernel
+//   GS_DOTS            partial dots  w . Y_j
+//   GS_AXPY_DOTS_NORM  w -= sum_j coef_j Y_j, then partial dots d_j of the new w with every
+//                      Y_j and ||w||^2; the last block then leaves ||w - sum_j d_j Y_j||^2 =
+//                      ||w||^2 - sum_j d_j^2 (Y orthonormal, d = Y^T w) in *norm_out, so the
+//                      second classical Gram-Schmidt pass needs no third pass: the next basis
+//                      vector (w - Y d) / norm is formed by axpy_scale_kernel
 // Every thread keeps the K basis values of its row in registers; per-block partials go to
 // partial[block * 33 + slot] and are summed in block order by the pass's last block.
-enum { GS_DOTS = 0, GS_AXPY_DOTS = 1, GS_AXPY_NORM = 2, GS_AXPY_DOTS_NORM = 3 };
+enum { GS_DOTS = 0, GS_AXPY_DOTS_NORM = 1 };
 
 // Block partials of NS sums and their reduction by the last block to arrive (an arrival
 // counter, reset by that block): partial[block * 33 + slot], then out[slot] summed in block
@@ -343,7 +342,7 @@ __global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, const double *__
                                                          double *__restrict__ norm_out)
 {
   CD_PDL_ENTRY();
-  constexpr int NS = MODE == GS_AXPY_NORM ? 1 : MODE == GS_AXPY_DOTS_NORM ? K + 1 : K;
+  constexpr int NS = MODE == GS_AXPY_DOTS_NORM ? K + 1 : K;
   double acc[NS];
 #pragma unroll
   for (int j = 0; j < NS; j++) acc[j] = 0;
@@ -363,14 +362,9 @@ __global__ void __launch_bounds__(kBlock) gs_pass_kernel(int n, const double *__
       for (int j = 0; j < K; j++) wi -= cf[j] * y[j];
       w[i] = wi;
     }
-    if (MODE == GS_AXPY_NORM)
-      acc[0] += wi * wi;
-    else
-    {
 #pragma unroll
-      for (int j = 0; j < K; j++) acc[j] += wi * y[j];
-      if constexpr (MODE == GS_AXPY_DOTS_NORM) acc[NS - 1] += wi * wi;
-    }
+    for (int j = 0; j < K; j++) acc[j] += wi * y[j];
+    if constexpr (MODE == GS_AXPY_DOTS_NORM) acc[NS - 1] += wi * wi;
   }
   gs_reduce<NS>(acc, partial, out, counter, MODE == GS_AXPY_DOTS_NORM ? norm_out : nullptr);
 }
