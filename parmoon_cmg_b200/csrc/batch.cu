@@ -88,6 +88,10 @@ struct BInst
   bool reported = false, tcd = false;
   size_t bytes = 0;
   std::vector<void *> allocs;
+  // one allocation per instance, carved by balloc into its arrays (256-byte aligned); arrays
+  // that do not fit get their own allocation
+  char *arena = nullptr;
+  size_t arena_off = 0, arena_size = 0;
 };
 
 struct Batch
@@ -914,6 +918,14 @@ static int ensure_colors(cdgpu_ctx *ctx, Hierarchy &h)
 template <typename T> static int balloc(cdgpu_ctx *ctx, BInst &in, T **p, size_t n)
 {
   if (n == 0) n = 1;
+  const size_t need = (n * sizeof(T) + 255) & ~(size_t)255;
+  if (in.arena && in.arena_off + need <= in.arena_size)
+  {
+    *p = (T *)(in.arena + in.arena_off);
+    in.arena_off += need;
+    in.bytes += n * sizeof(T);
+    return CDGPU_OK;
+  }
   cudaError_t e = cudaMallocAsync((void **)p, n * sizeof(T), ctx->stream);
   if (e != cudaSuccess)
   {
@@ -1744,6 +1756,21 @@ static int submit_impl(cdgpu_ctx *ctx, Batch &b, int mg_id, const cdgpu_coeffs *
   in.mg = mg_id;
   in.L = L;
   const int m = b.m;
+  {
+    // the instance's arrays in one allocation (the estimate of instance_bytes plus the
+    // alignment of every array); without it, one allocation per array
+    const size_t size = instance_bytes(h, m) + (size_t)(L * 16 + 16) * 256;
+    if (cudaMallocAsync((void **)&in.arena, size, ctx->stream) == cudaSuccess)
+    {
+      in.allocs.push_back(in.arena);
+      in.arena_size = size;
+    }
+    else
+    {
+      cudaGetLastError();
+      in.arena = nullptr;
+    }
+  }
   std::vector<BLevel> lv(kMaxDepth);
   double *tcd_K = nullptr;
   // per level: values, vectors; assemble with this instance's coefficients
