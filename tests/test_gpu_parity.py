@@ -251,6 +251,46 @@ def test_structured_solve_vs_oracle(ctx, oracle_lib, dim, order, n0, L, disc, ep
     assert abs(i1.iterations - its1) <= 2
 
 
+@pytest.mark.parametrize("dim,order,n0,L", [
+    (3, 2, 4, 2),    # 4^3 Q2 coarsest level: 343 active DOFs
+    (2, 1, 16, 2),   # 16^2 Q1 coarsest level: 225 active DOFs
+])
+def test_exact_coarse_solve_large_block_vs_oracle(ctx, oracle_lib, dim, order, n0, L):
+    """Exact coarse solve (SolveExact, MGLevel3D.C:839) on a coarsest level whose active block
+    is too large for the Gauss-Jordan inversion in shared memory (more than 160 rows): the
+    inversion runs in the global buffer; FP64 and mixed solutions against the oracle's, and
+    the iteration counts at the configs' stopping rule."""
+    b = (1.0, 0.5) if dim == 2 else (0.57735026918962573,) * 3
+    co = coeffs(0, eps=1e-1, b=b, f=1.0)
+    spaces, parents, sids, mg = structured_case(ctx, dim, order, n0, L, co, 1)
+    assert spaces[0]["n_active"] > 160
+    levels = []
+    for l, (sp, sid) in enumerate(zip(spaces, sids)):
+        rp, kc = oracle_lib.pattern(sp["global_numbers"], sp["begin_index"], sp["n_dof"], sp["n_active"])
+        ent, rhs = oracle_lib.assemble(dim, order, 1, sp["coords"], sp["global_numbers"],
+                                       sp["begin_index"], sp["n_dof"], sp["n_active"], rp, kc,
+                                       oracle_coeffs(oracle_lib, co))
+        lv = dict(n_dof=sp["n_dof"], n_active=sp["n_active"], row_ptr=rp, kcol=kc, entries=ent)
+        if l > 0:
+            lv["p_row"], lv["p_col"], lv["p_val"] = oracle_lib.prolongation(
+                dim, order, spaces[l - 1], dict(sp), parents[l])
+        levels.append(lv)
+        ctx.assemble(sid, 1, sp["n_dof"], len(kc), want_entries=False)
+    sol0 = np.zeros(spaces[-1]["n_dof"])
+    tight = dict(coarse_smoother=17, red_factor=0.0, res_norm_min=1e-14 * np.linalg.norm(rhs), maxit=3000)
+    x_o, its_o, _, _ = oracle_lib.solve(levels, oracle_lib.solver_params(**tight), rhs, sol0)
+    assert its_o > 0
+    x, info = ctx.solve(mg, solver_params(**tight), rhs, sol0)
+    assert info.status == 0
+    assert rel(x, x_o) <= TOL_SOL, rel(x, x_o)
+    xm, infom = ctx.solve(mg, solver_params(precision=1, **tight), rhs, sol0)
+    assert infom.status == 0
+    assert rel(xm, x_o) <= TOL_MIXED, rel(xm, x_o)
+    _, its1, _, _ = oracle_lib.solve(levels, oracle_lib.solver_params(coarse_smoother=17), rhs, sol0)
+    _, i1 = ctx.solve(mg, solver_params(coarse_smoother=17), rhs, sol0)
+    assert abs(i1.iterations - its1) <= 1, (i1.iterations, its1)
+
+
 @pytest.mark.parametrize("restart,minit", [(4, 0), (5, 9)])
 def test_fgmres_restart_cycles_vs_oracle(ctx, oracle_lib, restart, minit):
     """FGMRES over several restart cycles (FgmresIte.C:536-560) and with a minimum iteration
